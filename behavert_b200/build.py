@@ -1,0 +1,74 @@
+"""Builds libbehavert_b200.so (sm_100a) in-tree with nvcc.
+
+The library is compiled with ``--fmad=false`` and IEEE division / square root
+so that every float operation is one correctly rounded step in source order.
+Usage: ``python -m behavert_b200.build`` (or ``__graft_entry__.build()``).
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+LIB = PKG / "libbehavert_b200.so"
+SOURCES = ["brt_sort.cu", "brt_kernels.cu", "brt_engine.cu"]
+HEADERS = ["brt_internal.cuh", "brt_kernels.cuh", "brt_agent.cuh"]
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-O3", "-lineinfo", "-std=c++17",
+    "--fmad=false", "-prec-div=true", "-prec-sqrt=true",
+    "-Xcompiler", "-fPIC,-O2,-ffp-contract=off",
+    "-shared", "-cudart", "static",
+]
+
+
+def _nvcc() -> str:
+    cand = os.environ.get("NVCC") or "/usr/local/cuda/bin/nvcc"
+    return cand if Path(cand).exists() else "nvcc"
+
+
+def _stale(target: Path, deps) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(Path(d).stat().st_mtime > t for d in deps)
+
+
+def build_library(force: bool = False, verbose: bool = False) -> Path:
+    deps = [CSRC / s for s in SOURCES] + [CSRC / h for h in HEADERS] + [ROOT / "include" / "behavert_b200.h", Path(__file__)]
+    if not force and not _stale(LIB, deps):
+        return LIB
+    cmd = [_nvcc(), *NVCC_FLAGS, "-I", str(ROOT / "include"), "-o", str(LIB), *[str(CSRC / s) for s in SOURCES]]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError("nvcc failed building libbehavert_b200.so")
+    if verbose:
+        sys.stderr.write(res.stderr)
+    return LIB
+
+
+def build_oracle(force: bool = False) -> Path:
+    """Builds the CPU oracle (test infrastructure) under oracle/_build/."""
+    target = ROOT / "oracle" / "_build" / "liboracle_brt.so"
+    deps = [ROOT / "oracle" / "brt_oracle.cpp", ROOT / "include" / "behavert_b200.h"]
+    if not force and not _stale(target, deps):
+        return target
+    res = subprocess.run(["make", "-C", str(ROOT / "oracle")], capture_output=True, text=True)
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError("building the oracle failed")
+    return target
+
+
+if __name__ == "__main__":
+    build_library(force="--force" in sys.argv, verbose="-v" in sys.argv)
+    build_oracle(force="--force" in sys.argv)
+    print(LIB)

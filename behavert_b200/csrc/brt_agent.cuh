@@ -1,0 +1,374 @@
+// brt_agent.cuh -- per-agent device functions shared by the fused pass and
+// the stage-wise kernels, so both produce bit-identical results.
+//
+// Each function cites the reference device code whose operation order it
+// keeps.  Positions live in the periodic cube [0, L)^3; a neighbour reached
+// through a wrapped cell is used at its image position q + s, s in {-L,0,+L}.
+#pragma once
+
+#include "brt_internal.cuh"
+
+namespace brt {
+
+// genericCalcNeighgborhoodD + checkForNeighborsInCell + checkForNeighbor
+// (Proximity3D_kernel.cu:89-125, Proximity3D_resources.cu:59-172), periodic.
+// Visit order x outermost, y, z innermost; within a cell ascending sorted
+// slot; self skipped by slot; accept iff !(sqrtf(d2) > radius), evaluated as
+// d2 <= r2thr (sqrtf is monotone and correctly rounded, r2thr is the largest
+// float whose root does not exceed the radius).  With kNN off the scan stops
+// once M entries are held: later candidates cannot change the list.
+template <bool KNN>
+__device__ __forceinline__ uint32_t buildNeighborList(uint32_t self, f3 p, const FlockDev& fl,
+                                                      const uint32_t* __restrict__ cellStart,
+                                                      const uint32_t* __restrict__ cellEnd,
+                                                      const float4* __restrict__ posS, uint32_t* list,
+                                                      uint32_t ls, float* distList) {
+  const int gx = gridCoord(p.x, fl.cell, fl.G), gy = gridCoord(p.y, fl.cell, fl.G), gz = gridCoord(p.z, fl.cell, fl.G);
+  const uint32_t M = fl.M;
+  uint32_t n = 0;
+  float maxDistValue = 0.0f;
+  for (int ox = -1; ox <= 1; ++ox) {
+    const int cx = wrapCoord(gx + ox, fl.G);
+    const float sx = imageShift(gx, ox, fl.G, fl.L);
+    for (int oy = -1; oy <= 1; ++oy) {
+      const int cy = wrapCoord(gy + oy, fl.G);
+      const float sy = imageShift(gy, oy, fl.G, fl.L);
+      for (int oz = -1; oz <= 1; ++oz) {
+        const int cz = wrapCoord(gz + oz, fl.G);
+        const float sz = imageShift(gz, oz, fl.G, fl.L);
+        const uint32_t h = fl.cellBase + ((uint32_t)cz * fl.G + (uint32_t)cy) * fl.G + (uint32_t)cx;
+        const uint32_t start = __ldg(&cellStart[h]);
+        if (start == kEmpty) continue;
+        uint32_t stop = __ldg(&cellEnd[h]);
+        if (stop <= start) continue;
+        if (fl.maxPerCell && stop - start > fl.maxPerCell) stop = start + fl.maxPerCell;
+        for (uint32_t j = start; j < stop; ++j) {
+          if (j == self) continue;
+          const float4 q = __ldg(&posS[j]);
+          const float dx = (q.x + sx) - p.x, dy = (q.y + sy) - p.y, dz = (q.z + sz) - p.z;
+          const float d2 = dx * dx + dy * dy + dz * dz;
+          if (!KNN) {
+            if (d2 > fl.r2thr) continue;
+            list[(n++) * ls] = j;
+            if (n == M) return n;
+          } else {
+            const float dist = sqrtf(d2);
+            if (dist > fl.radius) continue;
+            if (n < M) {
+              list[n * ls] = j;
+              distList[n] = dist;
+              maxDistValue = fmaxf(maxDistValue, dist);
+              ++n;
+            } else if (dist < maxDistValue) {
+              maxDistValue = distList[0];
+              uint32_t maxIdx = 0;
+              for (uint32_t k = 1; k < n; ++k)
+                if (maxDistValue < distList[k]) { maxDistValue = distList[k]; maxIdx = k; }
+              list[maxIdx * ls] = j;
+              distList[maxIdx] = dist;
+            }
+          }
+        }
+      }
+    }
+  }
+  return n;
+}
+
+// Home-agent context for the steering stages.
+struct AgentCtx {
+  f3 pos, fwd;
+  float speed;
+  int g[3];
+  bool interior;  // no neighbour can need an image shift
+};
+
+__device__ __forceinline__ AgentCtx makeCtx(float4 p4, float4 w4, const FlockDev& fl) {
+  AgentCtx a;
+  a.pos = xyz(p4);
+  a.fwd = xyz(w4);
+  a.speed = w4.w;
+  a.g[0] = gridCoord(a.pos.x, fl.cell, fl.G);
+  a.g[1] = gridCoord(a.pos.y, fl.cell, fl.G);
+  a.g[2] = gridCoord(a.pos.z, fl.cell, fl.G);
+  const int hi = (int)fl.G - 1;
+  a.interior = a.g[0] > 0 && a.g[0] < hi && a.g[1] > 0 && a.g[1] < hi && a.g[2] > 0 && a.g[2] < hi;
+  return a;
+}
+
+__device__ __forceinline__ f3 neighborImage(const AgentCtx& a, float4 q4, const FlockDev& fl) {
+  f3 q = xyz(q4);
+  float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+  if (!a.interior) {
+    sx = imageShiftCells(a.g[0], gridCoord(q.x, fl.cell, fl.G), fl.G, fl.L);
+    sy = imageShiftCells(a.g[1], gridCoord(q.y, fl.cell, fl.G), fl.G, fl.L);
+    sz = imageShiftCells(a.g[2], gridCoord(q.z, fl.cell, fl.G), fl.G, fl.L);
+  }
+  return mk3(q.x + sx, q.y + sy, q.z + sz);
+}
+
+// inBoidNeighborhood (OpenSteerWrapper_resources.cu:67-92) given the shared
+// distance and cosine of the offset.
+__device__ __forceinline__ bool inBoid(float dist, float cosAngle, float minR, float maxR, float cosMax) {
+  if (dist < minR) return true;
+  if (dist > maxR) return false;
+  return cosAngle > cosMax;
+}
+
+// Separation, alignment and cohesion sums over the list in one pass; each sum
+// keeps the sequential order of its own reference loop
+// (calcSeparation :166-211, calcAlignment :253-290, calcCohesion :216-249),
+// and the results are blended in the flocking demo's order
+// (BehaveRT_Flocking.cpp:183-193): steer = ((0 + sep*w) + ali*w) + coh*w.
+__device__ __forceinline__ f3 flockingSteer(const AgentCtx& a, const FlockDev& fl, const uint32_t* list, uint32_t ls,
+                                            uint32_t n, const float4* __restrict__ posS, const float4* __restrict__ fwdS,
+                                            f3 steer, bool SEP, bool ALI, bool COH) {
+  f3 sSep = mk3(0.f, 0.f, 0.f), sAli = mk3(0.f, 0.f, 0.f), sCoh = mk3(0.f, 0.f, 0.f);
+  uint32_t cSep = 0, cAli = 0, cCoh = 0;
+  for (uint32_t k = 0; k < n; ++k) {
+    const uint32_t j = list[k * ls];
+    const f3 other = neighborImage(a, __ldg(&posS[j]), fl);
+    const f3 offset = sub3(other, a.pos);
+    const float d2 = dot3(offset, offset);
+    const float dist = sqrtf(d2);
+    const f3 nrm = mul3(offset, 1.0f / dist);
+    const float cosAngle = dot3(a.fwd, nrm);
+    if (SEP && inBoid(dist, cosAngle, fl.minR, fl.sep[1], fl.sep[2])) {
+      sSep = add3(sSep, div3(offset, -d2));
+      ++cSep;
+    }
+    if (ALI && inBoid(dist, cosAngle, fl.minR, fl.ali[1], fl.ali[2])) {
+      sAli = add3(sAli, xyz(__ldg(&fwdS[j])));
+      ++cAli;
+    }
+    if (COH && inBoid(dist, cosAngle, fl.minR, fl.coh[1], fl.coh[2])) {
+      sCoh = add3(sCoh, other);
+      ++cCoh;
+    }
+  }
+  if (SEP) {
+    if (cSep > 0) sSep = normalize3(div3(sSep, (float)cSep));
+    steer = add3(mul3(sSep, fl.sep[0]), steer);
+  }
+  if (ALI) {
+    if (cAli > 0) sAli = normalize3(sub3(div3(sAli, (float)cAli), a.fwd));
+    steer = add3(mul3(sAli, fl.ali[0]), steer);
+  }
+  if (COH) {
+    if (cCoh > 0) sCoh = normalize3(sub3(div3(sCoh, (float)cCoh), a.pos));
+    steer = add3(mul3(sCoh, fl.coh[0]), steer);
+  }
+  return steer;
+}
+
+// computeSimilarity (BehaviorClustering_resources.cu:156-180); the self norm
+// is the same for every pair and is passed in.
+__device__ __forceinline__ float similarity(const float* fi, float norm1, const float* __restrict__ fj, uint32_t F) {
+  float dot = 0.0f, n2 = 0.0f;
+  for (uint32_t k = 0; k < F; ++k) {
+    const float b = __ldg(&fj[k]);
+    dot += fi[k] * b;
+    n2 += b * b;
+  }
+  n2 = sqrtf(n2);
+  const float s = dot / (norm1 * n2);
+  return (s + 1.0f) / 2.0f;
+}
+__device__ __forceinline__ float selfNorm(const float* fi, uint32_t F) {
+  float n1 = 0.0f;
+  for (uint32_t k = 0; k < F; ++k) n1 += fi[k] * fi[k];
+  return sqrtf(n1);
+}
+
+// BehaviorClustering_resources.cu:61-147
+__device__ __forceinline__ float linInterp(float x, float xa, float ya, float xb, float yb) {
+  return ya * ((x - xb) / (xa - xb)) + yb * ((x - xa) / (xb - xa));
+}
+__device__ __forceinline__ float interpolateSimilarity(float val, float mn, float avg, float mx) {
+  if (val > avg) return clampf(linInterp(val, avg, 0.5f, mx, 1.0f), 0.0f, 1.0f);
+  return clampf(linInterp(val, mn, 0.0f, avg, 0.5f), 0.0f, 1.0f);
+}
+__device__ __forceinline__ float4 updateSimilarityStats(float sim, float4 st, const FlockDev& fl) {
+  float minVal = st.x, avgVal = st.y, maxVal = st.z;
+  const float ctl = fl.avgCtl;
+  const float blend = sim * ctl + ((maxVal + minVal) / 2.0f) * (1.0f - ctl);
+  avgVal += (blend - st.y) * fl.simStats[0];
+  avgVal = clampf(avgVal, 0.0f, 1.0f);
+  if (sim < minVal) {
+    minVal += (sim - minVal) * fl.simStats[1];
+    if (minVal > avgVal) minVal = clampf(minVal, 0.0f, sim);
+  } else if (minVal < avgVal) {
+    minVal += fl.simStats[2];
+  }
+  if (sim > maxVal) {
+    maxVal += (sim - maxVal) * fl.simStats[1];
+    if (maxVal < avgVal) maxVal = clampf(maxVal, sim, 1.0f);
+  } else if (maxVal > avgVal) {
+    maxVal -= fl.simStats[2];
+  }
+  st.x = minVal; st.y = avgVal; st.z = maxVal;
+  return st;
+}
+
+// xxxsteerForSeek / xxxsteerForFlee (OpenSteerWrapper_resources.cu:294-322)
+__device__ __forceinline__ f3 truncateLength(f3 v, float maxLength) {
+  const float len = len3(v);
+  if (len <= maxLength) return v;
+  return mul3(v, maxLength / len);
+}
+
+// BehaviorClustering split path (BehaviorClustering_kernel.cu:306-497,
+// BehaviorClustering_resources.cu:269-384): adaptive similarity per
+// neighbour, then cluster cohesion (seek/flee blend) and cluster alignment,
+// each blended into the steering force.  Similarities are staged in `sims`.
+__device__ __forceinline__ f3 clusteringSteer(const AgentCtx& a, const FlockDev& fl, const uint32_t* list, uint32_t ls, uint32_t n,
+                                              const float4* __restrict__ posS, const float4* __restrict__ fwdS,
+                                              const float* fi, float norm1, const float* __restrict__ featS,
+                                              uint32_t Fs, float4& stats, float* sims, f3 steer) {
+  const bool coh = fl.clus != 0.0f, ali = fl.aclus != 0.0f;
+  for (uint32_t k = 0; k < n; ++k) {
+    const float s = similarity(fi, norm1, featS + (size_t)list[k * ls] * Fs, fl.F);
+    stats = updateSimilarityStats(s, stats, fl);
+    sims[k] = interpolateSimilarity(s, stats.x, stats.y, stats.z);
+  }
+  if (coh) {
+    f3 s = mk3(0.f, 0.f, 0.f);
+    const f3 myVel = mul3(a.fwd, a.speed);
+    for (uint32_t k = 0; k < n; ++k) {
+      const float sim = sims[k];
+      const f3 other = neighborImage(a, __ldg(&posS[list[k * ls]]), fl);
+      const f3 seek = sub3(truncateLength(sub3(other, a.pos), fl.maxSpeed), myVel);
+      const f3 flee = sub3(truncateLength(sub3(a.pos, other), fl.maxSpeed), myVel);
+      const float om = 1.0f - sim;
+      s = add3(s, add3(mul3(seek, sim), mul3(flee, om)));
+    }
+    if (n > 0) s = mul3(normalize3(div3(s, (float)n)), fl.clus);
+    steer = add3(s, steer);
+  }
+  if (ali) {
+    f3 s = mk3(0.f, 0.f, 0.f);
+    for (uint32_t k = 0; k < n; ++k) s = add3(s, mul3(xyz(__ldg(&fwdS[list[k * ls]])), sims[k]));
+    if (n > 0) s = mul3(normalize3(sub3(div3(s, (float)n), a.fwd)), fl.aclus);
+    steer = add3(s, steer);
+  }
+  return steer;
+}
+
+// Static sphere obstacles: flee every sphere whose centre is closer than
+// radius + commonSearchRadius (minimum-image offset), linear falloff to zero
+// at that distance, weight obstacleAvoidanceWeight.  No reference counterpart
+// (nearest analogue moveAwayFromTarget_kernel, OpenSteerWrapper_kernel.cu:185-212).
+__device__ __forceinline__ f3 obstacleSteer(const AgentCtx& a, const FlockDev& fl, const float4* __restrict__ obstacles, f3 steer) {
+  f3 s = mk3(0.f, 0.f, 0.f);
+  const float L = fl.L, hL = 0.5f * fl.L;
+  for (uint32_t o = 0; o < fl.numObstacles; ++o) {
+    const float4 c = __ldg(&obstacles[fl.obsBase + o]);
+    f3 off = sub3(a.pos, xyz(c));
+    if (off.x > hL) off.x = off.x - L; else if (off.x < -hL) off.x = off.x + L;
+    if (off.y > hL) off.y = off.y - L; else if (off.y < -hL) off.y = off.y + L;
+    if (off.z > hL) off.z = off.z - L; else if (off.z < -hL) off.z = off.z + L;
+    const float d = len3(off);
+    const float reach = c.w + fl.radius;
+    if (d < reach && d > 0.0f) {
+      const float t = 1.0f - d / reach;
+      s = add3(s, mul3(off, t / d));
+    }
+  }
+  return add3(mul3(s, fl.obsW), steer);
+}
+
+// Feature relaxation toward the similarity-weighted neighbour mean (no
+// reference counterpart; the similarity is the reference's computeSimilarity).
+__device__ __forceinline__ void relaxFeatures(const FlockDev& fl, const uint32_t* list, uint32_t ls, uint32_t n, const float* fi,
+                                              float norm1, const float* __restrict__ featS, uint32_t Fs, float* fo) {
+  for (uint32_t k = 0; k < fl.F; ++k) fo[k] = fi[k];
+  if (fl.relax == 0.0f || fl.F == 0 || n == 0) return;
+  float acc[BRT_MAX_FEATUREDIM];
+  float sumS = 0.0f;
+  for (uint32_t k = 0; k < fl.F; ++k) acc[k] = 0.0f;
+  for (uint32_t m = 0; m < n; ++m) {
+    const float* fj = featS + (size_t)list[m * ls] * Fs;
+    const float s = similarity(fi, norm1, fj, fl.F);
+    sumS += s;
+    for (uint32_t k = 0; k < fl.F; ++k) acc[k] += s * __ldg(&fj[k]);
+  }
+  if (sumS > 0.0f) {
+    for (uint32_t k = 0; k < fl.F; ++k) {
+      const float mean = acc[k] / sumS;
+      fo[k] = fi[k] + fl.relax * (mean - fi[k]);
+    }
+  }
+}
+
+// genericApplySteeringForceD / applySteeringForceSingle
+// (OpenSteerWrapper_kernel.cu:265-333, OpenSteerWrapper_resources.cu:326-379,
+// Core/common_resources.cu:158-271), then wrap into [0, L).
+struct Integrated {
+  float4 pos, fwd, acc;
+};
+__device__ __forceinline__ f3 vecLimitDeviationAngle(f3 source, float cosineOfConeAngle, f3 basis) {
+  const float sourceLength = len3(source);
+  if (sourceLength == 0.0f) return source;
+  const f3 direction = div3(source, sourceLength);
+  const float cosineOfSourceAngle = dot3(direction, basis);
+  if (cosineOfSourceAngle >= cosineOfConeAngle) return source;
+  const float projection = dot3(source, basis);
+  const f3 perp = sub3(source, mul3(basis, projection));
+  const f3 unitPerp = normalize3(perp);
+  const float perpDist = sqrtf(1.0f - (cosineOfConeAngle * cosineOfConeAngle));
+  const f3 c0 = mul3(basis, cosineOfConeAngle);
+  const f3 c1 = mul3(unitPerp, perpDist);
+  return mul3(add3(c0, c1), sourceLength);
+}
+__device__ __forceinline__ f3 adjustRawSteeringForce(f3 force, float speed, f3 forward, float maxSpeed) {
+  const float maxAdjustedSpeed = 0.2f * maxSpeed;
+  if ((speed > maxAdjustedSpeed) || (force.x == 0.0f && force.y == 0.0f && force.z == 0.0f)) return force;
+  const float range = speed / maxAdjustedSpeed;
+  const float p = powf(range, 20.0f);
+  const float cosine = 1.0f + ((-1.0f - 1.0f) * p);
+  return vecLimitDeviationAngle(force, cosine, forward);
+}
+__device__ __forceinline__ float wrapPeriodic(float x, float L) {
+  if (x >= L) return x - L;
+  if (x < 0.0f) {
+    x = x + L;
+    if (x >= L) x = 0.0f;
+  }
+  return x;
+}
+__device__ __forceinline__ Integrated integrate(const AgentCtx& a, float4 acc4, f3 steer, float dt, const FlockDev& fl) {
+  Integrated r;
+  if (a.speed < 0.0f) {
+    // The agent does not move; the reference writes the steering force into
+    // forward (OpenSteerWrapper_kernel.cu:286-294).
+    r.pos = make_float4(a.pos.x, a.pos.y, a.pos.z, 1.0f);
+    r.acc = acc4;
+    r.fwd = make_float4(steer.x, steer.y, steer.z, 0.0f);
+    return r;
+  }
+  f3 force = steer;
+  if (fl.use2D) force.y = 0.0f;
+  f3 position = a.pos, forward = a.fwd, smoothed = xyz(acc4);
+  float speed = a.speed;
+  const f3 adjusted = adjustRawSteeringForce(force, speed, forward, fl.maxSpeed);
+  const f3 clipped = truncateLength(adjusted, fl.maxForce);
+  const f3 newAccel = div3(clipped, fl.mass);
+  if (dt > 0.0f) {
+    const float smoothRate = clampf(9.0f * dt, 0.15f, 0.4f);
+    const float alpha = clampf(smoothRate, 0.0f, 1.0f);
+    smoothed = add3(smoothed, mul3(sub3(newAccel, smoothed), alpha));
+  }
+  f3 v = add3(mul3(forward, speed), mul3(smoothed, dt));
+  v = truncateLength(v, fl.maxSpeed);
+  speed = len3(v);
+  position = add3(position, mul3(v, dt));
+  if (fl.use2D) v.y = 0.0f;
+  forward = normalize3(v);
+  if (fl.use2D) position.y = 0.5f;
+  r.pos = make_float4(wrapPeriodic(position.x, fl.L), wrapPeriodic(position.y, fl.L), wrapPeriodic(position.z, fl.L), 1.0f);
+  r.acc = make_float4(smoothed.x, smoothed.y, smoothed.z, acc4.w);
+  r.fwd = make_float4(forward.x, forward.y, forward.z, speed);
+  return r;
+}
+
+}  // namespace brt

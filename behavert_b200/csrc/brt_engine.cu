@@ -1,0 +1,792 @@
+// brt_engine.cu -- host side of the C-ABI: engine lifetime, feature I/O,
+// the fused step (optionally as one CUDA graph of many steps) and the
+// stage-wise functionalities of the reference's plugin chain.
+#include "brt_internal.cuh"
+#include "brt_kernels.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+namespace brt {
+
+static thread_local std::string tlsLastError;
+void setLastError(const std::string& msg) { tlsLastError = msg; }
+
+// Largest float x with !(sqrtf(x) > r): the neighbour predicate
+// !(sqrtf(d2) > r) of checkForNeighbor (Proximity3D_resources.cu:66-69) is
+// then exactly d2 <= x, because sqrtf is monotone and correctly rounded on
+// both host and device.
+static float radiusThreshold(float r) {
+  if (!(r >= 0.0f)) return -1.0f;
+  if (std::isinf(r)) return INFINITY;
+  float x = r * r;
+  if (std::isinf(x)) x = 3.0e38f;
+  while (!(std::sqrt(std::nextafter(x, INFINITY)) > r) && !std::isinf(std::nextafter(x, INFINITY))) x = std::nextafter(x, INFINITY);
+  while (x > 0.0f && std::sqrt(x) > r) x = std::nextafter(x, 0.0f);
+  return x;
+}
+
+static int validateParams(const brt_params& p, uint32_t& G) {
+  if (p.disableSorting) { setLastError("disableSorting is not supported"); return BRT_ERR_CONFIG; }
+  if (!(p.cellSize > 0.0f) || !(p.worldSize > 0.0f)) { setLastError("worldSize and cellSize must be positive"); return BRT_ERR_CONFIG; }
+  double g = (double)p.worldSize / (double)p.cellSize;
+  G = (uint32_t)std::llround(g);
+  if (G < 3 || (float)G * p.cellSize != p.worldSize) {
+    setLastError("worldSize must be gridSize * cellSize with gridSize >= 3");
+    return BRT_ERR_CONFIG;
+  }
+  if ((double)G * G * G > (double)(1u << 30)) { setLastError("too many cells"); return BRT_ERR_CAPACITY; }
+  if (p.maxNeighbors < 1 || p.maxNeighbors > BRT_MAX_NEIGHBORS) { setLastError("maxNeighbors must be in [1, 128]"); return BRT_ERR_CONFIG; }
+  if (p.featuresCount > BRT_MAX_FEATUREDIM) { setLastError("featuresCount must be <= 32"); return BRT_ERR_CONFIG; }
+  if (p.numObstacles > BRT_MAX_OBSTACLES) { setLastError("numObstacles must be <= 64"); return BRT_ERR_CONFIG; }
+  if (!(p.commonMass != 0.0f)) { setLastError("commonMass must be nonzero"); return BRT_ERR_CONFIG; }
+  return BRT_OK;
+}
+
+static FlockDev toDev(const brt_params& p, uint32_t G) {
+  FlockDev d;
+  std::memset(&d, 0, sizeof(d));
+  d.G = G;
+  d.C = G * G * G;
+  d.n = p.numBodies;
+  d.L = p.worldSize;
+  d.cell = p.cellSize;
+  d.radius = p.commonSearchRadius;
+  d.r2thr = radiusThreshold(p.commonSearchRadius);
+  d.M = p.maxNeighbors;
+  d.maxPerCell = p.maxBodiesPerCell;
+  d.useKnn = p.useKnn;
+  d.maxSpeed = p.commonMaxSpeed;
+  d.maxForce = p.commonMaxForce;
+  d.mass = p.commonMass;
+  d.minR = p.commonSensingMinRadius;
+  for (int k = 0; k < 3; ++k) { d.sep[k] = p.separationParams[k]; d.ali[k] = p.alignmentParams[k]; d.coh[k] = p.cohesionParams[k]; }
+  d.use2D = p.use2DProjection;
+  d.F = p.featuresCount;
+  d.relax = p.featureRelaxRate;
+  d.clus = p.clusteringForceParams[0];
+  d.aclus = p.alignmentClusteringForceParams[0];
+  for (int k = 0; k < 3; ++k) d.simStats[k] = p.similarityStatsParams[k];
+  d.avgCtl = p.avgSimilarityController;
+  d.numObstacles = p.numObstacles;
+  d.obsW = p.obstacleAvoidanceWeight;
+  return d;
+}
+
+}  // namespace brt
+
+using namespace brt;
+
+struct brt_engine {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  uint32_t nflocks = 0, N = 0, C = 0, Cpad = 0, Mmax = 0, Fmax = 0, Fs = 0;
+  std::vector<brt_params> params;
+  std::vector<FlockDev> flocksHost;
+  FlockDev* flocks = nullptr;
+  uint32_t* agentBase = nullptr;
+  float4* obstacles = nullptr;
+  bool anyKnn = false;
+  // state
+  float4 *posA = nullptr, *fwdA = nullptr, *accA = nullptr, *posS = nullptr, *fwdS = nullptr, *accS = nullptr;
+  float *featA = nullptr, *featS = nullptr;
+  uint32_t *idA = nullptr, *idS = nullptr;
+  float4* statsById = nullptr;
+  float4* steer = nullptr;
+  uint32_t* lists = nullptr;
+  uint32_t listStride = 0;
+  uint2* pairs[2] = {nullptr, nullptr};
+  uint32_t *cellStart = nullptr, *cellEnd = nullptr;
+  SortPlan plan;
+  void* sortMem = nullptr;
+  SortScratch ss;
+  uint32_t* errWord = nullptr;
+  float4* stage4 = nullptr;  // id-order staging (N float4)
+  float* stageF = nullptr;   // id-order staging (N * Fmax)
+  // pipeline state
+  bool reordered = false, listsValid = false, recordLists = false;
+  uint32_t finalPairs = 0;
+  uint32_t paramsVersion = 0;
+  std::map<std::tuple<uint32_t, uint32_t, bool, uint32_t>, cudaGraphExec_t> graphs;
+  uint32_t smCount = 148;
+  // per-stage timing: a ring of event sets, drained into totals
+  static constexpr int kRing = 32;
+  bool timing = false, capturing = false;
+  cudaEvent_t ev[kRing][5] = {};
+  bool pending[kRing] = {};
+  int ringPos = 0;
+  double stageMs[4] = {0, 0, 0, 0};
+  uint64_t timedSteps = 0;
+};
+
+namespace {
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+template <class T>
+int devAlloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) return BRT_OK;
+  BRT_CUDA_TRY(cudaMalloc((void**)p, count * sizeof(T)));
+  return BRT_OK;
+}
+
+void freeAll(brt_engine* e) {
+  for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second);
+  e->graphs.clear();
+  for (int r = 0; r < brt_engine::kRing; ++r)
+    for (int k = 0; k < 5; ++k)
+      if (e->ev[r][k]) cudaEventDestroy(e->ev[r][k]);
+  void* ptrs[] = {e->flocks, e->agentBase, e->obstacles, e->posA, e->fwdA, e->accA, e->posS, e->fwdS, e->accS,
+                  e->featA, e->featS, e->idA, e->idS, e->statsById, e->steer, e->lists, e->pairs[0], e->pairs[1],
+                  e->cellStart, e->cellEnd, e->sortMem, e->errWord, e->stage4, e->stageF};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (e->stream) cudaStreamDestroy(e->stream);
+}
+
+HashArgs hashArgs(brt_engine* e) {
+  HashArgs A;
+  std::memset(&A, 0, sizeof(A));
+  A.pos = e->posA; A.id = e->idA; A.pairs = e->pairs[0];
+  A.flocks = e->flocks; A.agentBase = e->agentBase; A.nflocks = e->nflocks; A.n = e->N;
+  A.passes = e->plan.passes; A.bins = e->plan.bins;
+  for (uint32_t k = 0; k < e->plan.passes; ++k) { A.shift[k] = e->plan.shift[k]; A.mask[k] = sortPassMask(e->plan, k); }
+  A.hist = e->ss.hist;
+  A.cellStart = e->cellStart; A.cellEnd = e->cellEnd; A.cellWords4 = e->Cpad / 4;
+  A.status = e->ss.status; A.statusWords = e->plan.passes * std::max(1u, e->plan.tiles) * e->plan.bins;
+  A.counters = e->ss.counters;
+  return A;
+}
+
+StageArgs stageArgs(brt_engine* e) {
+  StageArgs A;
+  std::memset(&A, 0, sizeof(A));
+  A.posS = e->posS; A.fwdS = e->fwdS; A.accS = e->accS; A.featS = e->featS; A.idS = e->idS;
+  A.posA = e->posA; A.fwdA = e->fwdA; A.accA = e->accA; A.featA = e->featA; A.idA = e->idA;
+  A.statsById = e->statsById; A.steer = e->steer;
+  A.cellStart = e->cellStart; A.cellEnd = e->cellEnd;
+  A.flocks = e->flocks; A.agentBase = e->agentBase; A.obstacles = e->obstacles;
+  A.lists = e->lists; A.listStride = e->listStride;
+  A.nflocks = e->nflocks; A.n = e->N; A.Fs = e->Fs;
+  return A;
+}
+
+// Drains one ring slot of stage events into the totals.
+int drainSlot(brt_engine* e, int r) {
+  if (!e->pending[r]) return BRT_OK;
+  BRT_CUDA_TRY(cudaEventSynchronize(e->ev[r][4]));
+  for (int k = 0; k < 4; ++k) {
+    float ms = 0.0f;
+    BRT_CUDA_TRY(cudaEventElapsedTime(&ms, e->ev[r][k], e->ev[r][k + 1]));
+    e->stageMs[k] += ms;
+  }
+  e->timedSteps++;
+  e->pending[r] = false;
+  return BRT_OK;
+}
+
+// Records stage boundary k of the current timed step.
+int stageMark(brt_engine* e, int k) {
+  if (!e->timing || e->capturing) return BRT_OK;
+  BRT_CUDA_TRY(cudaEventRecord(e->ev[e->ringPos][k], e->stream));
+  return BRT_OK;
+}
+
+// hash -> sort -> reorder + cell ranges
+int enqueueReorder(brt_engine* e) {
+  cudaStream_t st = e->stream;
+  int rc = stageMark(e, 0);
+  if (rc) return rc;
+  BRT_CUDA_TRY(launchHash(hashArgs(e), e->smCount * 8, st));
+  if ((rc = stageMark(e, 1))) return rc;
+  for (uint32_t k = 0; k < e->plan.passes; ++k)
+    BRT_CUDA_TRY(launchOnesweepPass(e->plan, k, e->pairs[k & 1], e->pairs[(k + 1) & 1], e->ss, e->errWord, st));
+  if ((rc = stageMark(e, 2))) return rc;
+  e->finalPairs = e->plan.passes & 1;
+  ReorderArgs R;
+  std::memset(&R, 0, sizeof(R));
+  R.pairs = e->pairs[e->finalPairs];
+  R.posA = e->posA; R.fwdA = e->fwdA; R.accA = e->accA; R.featA = e->featA; R.idA = e->idA;
+  R.posS = e->posS; R.fwdS = e->fwdS; R.accS = e->accS; R.featS = e->featS; R.idS = e->idS;
+  R.fs4 = e->Fs / 4;
+  R.cellStart = e->cellStart; R.cellEnd = e->cellEnd;
+  R.hist = e->ss.hist; R.histWords = e->plan.passes * e->plan.bins;
+  R.n = e->N; R.numCells = e->C; R.errWord = e->errWord;
+  BRT_CUDA_TRY(launchReorder(R, st));
+  return stageMark(e, 3);
+}
+
+int enqueueStep(brt_engine* e, float dt, bool record) {
+  const bool timed = e->timing && !e->capturing;
+  if (timed) {
+    int rc = drainSlot(e, e->ringPos);
+    if (rc) return rc;
+  }
+  int rc = enqueueReorder(e);
+  if (rc) return rc;
+  FusedArgs F;
+  std::memset(&F, 0, sizeof(F));
+  F.posS = e->posS; F.fwdS = e->fwdS; F.accS = e->accS; F.featS = e->featS; F.idS = e->idS;
+  F.posA = e->posA; F.fwdA = e->fwdA; F.accA = e->accA; F.featA = e->featA; F.idA = e->idA;
+  F.statsById = e->statsById;
+  F.cellStart = e->cellStart; F.cellEnd = e->cellEnd;
+  F.flocks = e->flocks; F.agentBase = e->agentBase; F.obstacles = e->obstacles;
+  F.lists = record ? e->lists : nullptr; F.listStride = e->listStride;
+  F.nflocks = e->nflocks; F.n = e->N; F.Mmax = e->Mmax; F.Fs = e->Fs; F.dt = dt;
+  BRT_CUDA_TRY(launchFused(F, e->anyKnn, e->stream));
+  if (timed) {
+    if ((rc = stageMark(e, 4))) return rc;
+    e->pending[e->ringPos] = true;
+    e->ringPos = (e->ringPos + 1) % brt_engine::kRing;
+  }
+  return BRT_OK;
+}
+
+// Captures the nsteps-step graph (cached by dt, nsteps, recording, params).
+int getGraph(brt_engine* e, float dt, uint32_t nsteps, bool record, cudaGraphExec_t* out) {
+  uint32_t dtBits;
+  std::memcpy(&dtBits, &dt, 4);
+  auto key = std::make_tuple(nsteps, dtBits, record, e->paramsVersion);
+  auto it = e->graphs.find(key);
+  if (it == e->graphs.end()) {
+    if (e->graphs.size() >= 8) {
+      for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second);
+      e->graphs.clear();
+    }
+    cudaGraph_t g = nullptr;
+    BRT_CUDA_TRY(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    e->capturing = true;
+    int rc = BRT_OK;
+    for (uint32_t s = 0; s < nsteps && !rc; ++s) rc = enqueueStep(e, dt, record);
+    cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+    e->capturing = false;
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    if (ce != cudaSuccess) { setLastError(std::string("graph capture: ") + cudaGetErrorString(ce)); return BRT_ERR_CUDA; }
+    cudaGraphExec_t ge = nullptr;
+    ce = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) { setLastError(std::string("graph instantiate: ") + cudaGetErrorString(ce)); return BRT_ERR_CUDA; }
+    it = e->graphs.emplace(key, ge).first;
+  }
+  *out = it->second;
+  return BRT_OK;
+}
+
+int checkDeviceError(brt_engine* e, bool clear) {
+  uint32_t w = 0;
+  BRT_CUDA_TRY(cudaMemcpyAsync(&w, e->errWord, 4, cudaMemcpyDeviceToHost, e->stream));
+  BRT_CUDA_TRY(cudaStreamSynchronize(e->stream));
+  if (w && clear) BRT_CUDA_TRY(cudaMemsetAsync(e->errWord, 0, 4, e->stream));
+  if (w & kDevErrLookback) { setLastError("onesweep look-back spin limit reached"); return BRT_ERR_TIMEOUT; }
+  if (w) { setLastError("device-side pipeline check failed"); return BRT_ERR_STATE; }
+  return BRT_OK;
+}
+
+int syncAndCheck(brt_engine* e) { return checkDeviceError(e, true); }
+
+int configureKernels(brt_engine* e);
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* brt_version(void) { return "behavert_b200 0.1 (sm_100a)"; }
+
+const char* brt_error_string(int status) {
+  switch (status) {
+    case BRT_OK: return "ok";
+    case BRT_ERR_CUDA: return "CUDA error";
+    case BRT_ERR_CONFIG: return "invalid configuration";
+    case BRT_ERR_CAPACITY: return "capacity exceeded";
+    case BRT_ERR_TIMEOUT: return "device wait timed out";
+    case BRT_ERR_ARG: return "invalid argument";
+    case BRT_ERR_STATE: return "invalid call order";
+    case BRT_ERR_NODEVICE: return "no CUDA device";
+    default: return "unknown status";
+  }
+}
+
+const char* brt_last_error(void) { return tlsLastError.c_str(); }
+
+int brt_device_count(int* count) {
+  if (!count) return BRT_ERR_ARG;
+  *count = 0;
+  cudaError_t err = cudaGetDeviceCount(count);
+  if (err != cudaSuccess) { *count = 0; cudaGetLastError(); }
+  return BRT_OK;
+}
+
+int brt_params_default(brt_params* p) {
+  if (!p) return BRT_ERR_ARG;
+  std::memset(p, 0, sizeof(*p));
+  p->numBodies = 4096;
+  p->commonRadius = 1.0f;
+  p->worldSize = 64.0f;
+  p->cellSize = 4.0f;
+  p->maxBodiesPerCell = 0;
+  p->maxNeighbors = 16;
+  p->useKnn = 0;
+  p->commonSearchRadius = 4.0f;
+  p->commonMaxSpeed = 1.0f;
+  p->commonMaxForce = 0.1f;
+  p->commonMass = 1.0f;
+  p->commonSensingMinRadius = 0.0f;
+  p->separationParams[0] = 1.5f; p->separationParams[1] = 4.0f; p->separationParams[2] = -2.0f;
+  p->alignmentParams[0] = 1.0f; p->alignmentParams[1] = 4.0f; p->alignmentParams[2] = -2.0f;
+  p->cohesionParams[0] = 1.0f; p->cohesionParams[1] = 4.0f; p->cohesionParams[2] = -2.0f;
+  p->featuresCount = 0;
+  p->similarityStatsParams[0] = 0.01f; p->similarityStatsParams[1] = 0.1f; p->similarityStatsParams[2] = 0.001f;
+  p->avgSimilarityController = 1.0f;
+  p->featureRelaxRate = 0.0f;
+  return BRT_OK;
+}
+
+int brt_engine_create(const brt_params* flocks, uint32_t num_flocks, int device, brt_engine** out) {
+  if (!flocks || !out || num_flocks == 0) { setLastError("brt_engine_create: bad arguments"); return BRT_ERR_ARG; }
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); setLastError("no CUDA device"); return BRT_ERR_NODEVICE; }
+  if (device < 0 || device >= ndev) { setLastError("bad device index"); return BRT_ERR_ARG; }
+  DeviceGuard guard(device);
+  brt_engine* e = new brt_engine();
+  e->device = device;
+  e->nflocks = num_flocks;
+  e->params.assign(flocks, flocks + num_flocks);
+  std::vector<uint32_t> agentBase(num_flocks + 1, 0);
+  std::vector<float4> obs;
+  uint64_t N = 0, C = 0;
+  for (uint32_t f = 0; f < num_flocks; ++f) {
+    uint32_t G = 0;
+    int rc = validateParams(flocks[f], G);
+    if (rc) { delete e; return rc; }
+    FlockDev d = toDev(flocks[f], G);
+    d.cellBase = (uint32_t)C;
+    d.agentBase = (uint32_t)N;
+    d.obsBase = (uint32_t)obs.size();
+    for (uint32_t o = 0; o < flocks[f].numObstacles; ++o)
+      obs.push_back(make_float4(flocks[f].obstacles[o][0], flocks[f].obstacles[o][1], flocks[f].obstacles[o][2], flocks[f].obstacles[o][3]));
+    agentBase[f] = (uint32_t)N;
+    N += flocks[f].numBodies;
+    C += d.C;
+    e->Mmax = std::max(e->Mmax, d.M);
+    e->Fmax = std::max(e->Fmax, d.F);
+    e->anyKnn = e->anyKnn || d.useKnn;
+    e->flocksHost.push_back(d);
+  }
+  if (N >= (1ull << 30) || C >= (1ull << 30)) { delete e; setLastError("too many agents or cells"); return BRT_ERR_CAPACITY; }
+  agentBase[num_flocks] = (uint32_t)N;
+  e->N = (uint32_t)N;
+  e->C = (uint32_t)C;
+  e->Cpad = (e->C + 3) & ~3u;
+  e->Fs = (e->Fmax + 3) & ~3u;
+  e->listStride = e->Mmax + 1;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) e->smCount = prop.multiProcessorCount;
+  uint32_t bits = 1;
+  while ((1ull << bits) < C) ++bits;
+  e->plan = makeSortPlan(e->N, bits, 8);
+  int rc = BRT_OK;
+  auto chk = [&](int r) { if (r && !rc) rc = r; };
+  if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) { delete e; setLastError("stream creation failed"); return BRT_ERR_CUDA; }
+  const size_t n = e->N;
+  chk(devAlloc(&e->flocks, num_flocks));
+  chk(devAlloc(&e->agentBase, num_flocks + 1));
+  chk(devAlloc(&e->obstacles, std::max<size_t>(1, obs.size())));
+  chk(devAlloc(&e->posA, n)); chk(devAlloc(&e->fwdA, n)); chk(devAlloc(&e->accA, n));
+  chk(devAlloc(&e->posS, n)); chk(devAlloc(&e->fwdS, n)); chk(devAlloc(&e->accS, n));
+  chk(devAlloc(&e->featA, n * e->Fs)); chk(devAlloc(&e->featS, n * e->Fs));
+  chk(devAlloc(&e->idA, n)); chk(devAlloc(&e->idS, n));
+  chk(devAlloc(&e->statsById, n));
+  chk(devAlloc(&e->steer, n));
+  chk(devAlloc(&e->lists, n * e->listStride));
+  chk(devAlloc(&e->pairs[0], n)); chk(devAlloc(&e->pairs[1], n));
+  chk(devAlloc(&e->cellStart, e->Cpad)); chk(devAlloc(&e->cellEnd, e->Cpad));
+  chk(devAlloc(&e->errWord, 1));
+  chk(devAlloc(&e->stage4, n));
+  chk(devAlloc(&e->stageF, std::max<size_t>(1, n * e->Fmax)));
+  const size_t sortBytes = sortScratchBytes(e->plan, false);
+  if (!rc && cudaMalloc(&e->sortMem, sortBytes) != cudaSuccess) { setLastError("sort scratch allocation failed"); rc = BRT_ERR_CUDA; }
+  if (rc) { freeAll(e); delete e; return rc; }
+  e->ss = carveSortScratch(e->plan, e->sortMem, false);
+  cudaStream_t st = e->stream;
+  BRT_CUDA_TRY(cudaMemcpyAsync(e->flocks, e->flocksHost.data(), sizeof(FlockDev) * num_flocks, cudaMemcpyHostToDevice, st));
+  BRT_CUDA_TRY(cudaMemcpyAsync(e->agentBase, agentBase.data(), 4 * (num_flocks + 1), cudaMemcpyHostToDevice, st));
+  if (!obs.empty()) BRT_CUDA_TRY(cudaMemcpyAsync(e->obstacles, obs.data(), sizeof(float4) * obs.size(), cudaMemcpyHostToDevice, st));
+  BRT_CUDA_TRY(cudaMemsetAsync(e->sortMem, 0, sortBytes, st));
+  BRT_CUDA_TRY(cudaMemsetAsync(e->errWord, 0, 4, st));
+  if (n) {
+    BRT_CUDA_TRY(cudaMemsetAsync(e->posA, 0, n * 16, st));
+    BRT_CUDA_TRY(cudaMemsetAsync(e->fwdA, 0, n * 16, st));
+    BRT_CUDA_TRY(cudaMemsetAsync(e->accA, 0, n * 16, st));
+    BRT_CUDA_TRY(cudaMemsetAsync(e->statsById, 0, n * 16, st));
+    BRT_CUDA_TRY(cudaMemsetAsync(e->steer, 0, n * 16, st));
+    if (e->Fs) BRT_CUDA_TRY(cudaMemsetAsync(e->featA, 0, n * e->Fs * 4, st));
+    // identity slot order
+    std::vector<uint32_t> iota(n);
+    for (size_t i = 0; i < n; ++i) iota[i] = (uint32_t)i;
+    BRT_CUDA_TRY(cudaMemcpyAsync(e->idA, iota.data(), 4 * n, cudaMemcpyHostToDevice, st));
+    BRT_CUDA_TRY(cudaStreamSynchronize(st));
+  }
+  rc = configureKernels(e);
+  if (rc) { freeAll(e); delete e; return rc; }
+  BRT_CUDA_TRY(cudaStreamSynchronize(st));
+  *out = e;
+  return BRT_OK;
+}
+
+int brt_engine_destroy(brt_engine* e) {
+  if (!e) return BRT_ERR_ARG;
+  DeviceGuard guard(e->device);
+  cudaStreamSynchronize(e->stream);
+  freeAll(e);
+  delete e;
+  return BRT_OK;
+}
+
+int brt_engine_num_agents(const brt_engine* e, uint32_t* n) {
+  if (!e || !n) return BRT_ERR_ARG;
+  *n = e->N;
+  return BRT_OK;
+}
+int brt_engine_num_cells(const brt_engine* e, uint32_t* c) {
+  if (!e || !c) return BRT_ERR_ARG;
+  *c = e->C;
+  return BRT_OK;
+}
+int brt_neighbor_list_stride(const brt_engine* e, uint32_t* stride) {
+  if (!e || !stride) return BRT_ERR_ARG;
+  *stride = e->listStride;
+  return BRT_OK;
+}
+
+int brt_engine_set_params(brt_engine* e, uint32_t flock, const brt_params* p) {
+  if (!e || !p || flock >= e->nflocks) { setLastError("brt_engine_set_params: bad arguments"); return BRT_ERR_ARG; }
+  const brt_params& o = e->params[flock];
+  if (p->numBodies != o.numBodies || p->worldSize != o.worldSize || p->cellSize != o.cellSize ||
+      p->maxNeighbors != o.maxNeighbors || p->featuresCount != o.featuresCount || p->numObstacles != o.numObstacles ||
+      (p->useKnn != 0) != (o.useKnn != 0)) {
+    setLastError("brt_engine_set_params: geometry fields cannot change");
+    return BRT_ERR_CONFIG;
+  }
+  uint32_t G = 0;
+  int rc = validateParams(*p, G);
+  if (rc) return rc;
+  DeviceGuard guard(e->device);
+  FlockDev d = toDev(*p, G);
+  const FlockDev& old = e->flocksHost[flock];
+  d.cellBase = old.cellBase;
+  d.agentBase = old.agentBase;
+  d.obsBase = old.obsBase;
+  e->flocksHost[flock] = d;
+  e->params[flock] = *p;
+  BRT_CUDA_TRY(cudaMemcpyAsync(e->flocks + flock, &e->flocksHost[flock], sizeof(FlockDev), cudaMemcpyHostToDevice, e->stream));
+  std::vector<float4> obs;
+  for (uint32_t k = 0; k < p->numObstacles; ++k)
+    obs.push_back(make_float4(p->obstacles[k][0], p->obstacles[k][1], p->obstacles[k][2], p->obstacles[k][3]));
+  if (!obs.empty())
+    BRT_CUDA_TRY(cudaMemcpyAsync(e->obstacles + d.obsBase, obs.data(), sizeof(float4) * obs.size(), cudaMemcpyHostToDevice, e->stream));
+  BRT_CUDA_TRY(cudaStreamSynchronize(e->stream));
+  for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second);
+  e->graphs.clear();
+  e->paramsVersion++;
+  return BRT_OK;
+}
+
+int brt_engine_stream(brt_engine* e, void** stream) {
+  if (!e || !stream) return BRT_ERR_ARG;
+  *stream = (void*)e->stream;
+  return BRT_OK;
+}
+
+int brt_sync(brt_engine* e) {
+  if (!e) return BRT_ERR_ARG;
+  DeviceGuard guard(e->device);
+  return syncAndCheck(e);
+}
+
+int brt_engine_record_lists(brt_engine* e, int enable) {
+  if (!e) return BRT_ERR_ARG;
+  e->recordLists = enable != 0;
+  return BRT_OK;
+}
+
+int brt_engine_check_device_error(brt_engine* e, uint32_t* word) {
+  if (!e || !word) return BRT_ERR_ARG;
+  DeviceGuard guard(e->device);
+  BRT_CUDA_TRY(cudaMemcpyAsync(word, e->errWord, 4, cudaMemcpyDeviceToHost, e->stream));
+  BRT_CUDA_TRY(cudaStreamSynchronize(e->stream));
+  BRT_CUDA_TRY(cudaMemsetAsync(e->errWord, 0, 4, e->stream));
+  BRT_CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return BRT_OK;
+}
+
+// ---- feature I/O ------------------------------------------------------------
+
+int brt_set_state(brt_engine* e, const float* pos4, const float* fwd4, const float* acc4, const float* features, int where) {
+  if (!e) return BRT_ERR_ARG;
+  if (where != BRT_MEM_HOST && where != BRT_MEM_DEVICE) return BRT_ERR_ARG;
+  DeviceGuard guard(e->device);
+  cudaStream_t st = e->stream;
+  const size_t n = e->N;
+  auto stage4 = [&](const float* src) -> const float4* {
+    if (where == BRT_MEM_DEVICE) return (const float4*)src;
+    cudaMemcpyAsync(e->stage4, src, n * 16, cudaMemcpyHostToDevice, st);
+    return e->stage4;
+  };
+  if (n == 0) return BRT_OK;
+  // Inputs are in agent-id order; the canonical arrays are in slot order.
+  if (pos4) { const float4* s = stage4(pos4); BRT_CUDA_TRY(launchGatherFromId(s, e->idA, e->posA, e->N, true, st)); }
+  if (fwd4) { const float4* s = stage4(fwd4); BRT_CUDA_TRY(launchGatherFromId(s, e->idA, e->fwdA, e->N, false, st)); }
+  if (acc4) { const float4* s = stage4(acc4); BRT_CUDA_TRY(launchGatherFromId(s, e->idA, e->accA, e->N, false, st)); }
+  if (features && e->Fmax) {
+    const float* s = features;
+    if (where == BRT_MEM_HOST) {
+      BRT_CUDA_TRY(cudaMemcpyAsync(e->stageF, features, n * e->Fmax * 4, cudaMemcpyHostToDevice, st));
+      s = e->stageF;
+    }
+    BRT_CUDA_TRY(launchGatherFeatFromId(s, e->Fmax, e->idA, e->featA, e->Fs, e->N, st));
+  }
+  e->reordered = false;
+  e->listsValid = false;
+  if (where == BRT_MEM_HOST) BRT_CUDA_TRY(cudaStreamSynchronize(st));
+  return BRT_OK;
+}
+
+int brt_get_state(brt_engine* e, float* pos4, float* fwd4, float* acc4, float* features, int where) {
+  if (!e) return BRT_ERR_ARG;
+  if (where != BRT_MEM_HOST && where != BRT_MEM_DEVICE) return BRT_ERR_ARG;
+  DeviceGuard guard(e->device);
+  cudaStream_t st = e->stream;
+  const size_t n = e->N;
+  if (n == 0) return BRT_OK;
+  float4* srcs[3] = {e->posA, e->fwdA, e->accA};
+  float* dsts[3] = {pos4, fwd4, acc4};
+  for (int k = 0; k < 3; ++k) {
+    if (!dsts[k]) continue;
+    if (where == BRT_MEM_DEVICE) {
+      BRT_CUDA_TRY(launchScatterToId(srcs[k], e->idA, (float4*)dsts[k], e->N, st));
+    } else {
+      BRT_CUDA_TRY(launchScatterToId(srcs[k], e->idA, e->stage4, e->N, st));
+      BRT_CUDA_TRY(cudaMemcpyAsync(dsts[k], e->stage4, n * 16, cudaMemcpyDeviceToHost, st));
+    }
+  }
+  if (features && e->Fmax) {
+    if (where == BRT_MEM_DEVICE) {
+      BRT_CUDA_TRY(launchScatterFeatToId(e->featA, e->Fs, e->idA, features, e->Fmax, e->N, st));
+    } else {
+      BRT_CUDA_TRY(launchScatterFeatToId(e->featA, e->Fs, e->idA, e->stageF, e->Fmax, e->N, st));
+      BRT_CUDA_TRY(cudaMemcpyAsync(features, e->stageF, n * e->Fmax * 4, cudaMemcpyDeviceToHost, st));
+    }
+  }
+  if (where == BRT_MEM_HOST) return syncAndCheck(e);
+  return BRT_OK;
+}
+
+int brt_set_similarity_stats(brt_engine* e, const float* stats4, int where) {
+  if (!e || !stats4) return BRT_ERR_ARG;
+  DeviceGuard guard(e->device);
+  BRT_CUDA_TRY(cudaMemcpyAsync(e->statsById, stats4, (size_t)e->N * 16,
+                               where == BRT_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, e->stream));
+  if (where == BRT_MEM_HOST) BRT_CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return BRT_OK;
+}
+
+int brt_get_similarity_stats(brt_engine* e, float* stats4, int where) {
+  if (!e || !stats4) return BRT_ERR_ARG;
+  DeviceGuard guard(e->device);
+  BRT_CUDA_TRY(cudaMemcpyAsync(stats4, e->statsById, (size_t)e->N * 16,
+                               where == BRT_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, e->stream));
+  if (where == BRT_MEM_HOST) return syncAndCheck(e);
+  return BRT_OK;
+}
+
+// ---- fused step --------------------------------------------------------------
+
+int brt_step(brt_engine* e, float elapsedTime, uint32_t nsteps) {
+  if (!e) return BRT_ERR_ARG;
+  if (nsteps == 0 || e->N == 0) return BRT_OK;
+  DeviceGuard guard(e->device);
+  const bool record = e->recordLists;
+  if (nsteps == 1) {
+    int rc = enqueueStep(e, elapsedTime, record);
+    if (rc) return rc;
+  } else {
+    cudaGraphExec_t ge = nullptr;
+    int rc = getGraph(e, elapsedTime, nsteps, record, &ge);
+    if (rc) return rc;
+    BRT_CUDA_TRY(cudaGraphLaunch(ge, e->stream));
+  }
+  e->reordered = true;
+  e->listsValid = record;
+  return BRT_OK;
+}
+
+int brt_step_prepare(brt_engine* e, float elapsedTime, uint32_t nsteps) {
+  if (!e) return BRT_ERR_ARG;
+  if (nsteps < 2 || e->N == 0) return BRT_OK;
+  DeviceGuard guard(e->device);
+  cudaGraphExec_t ge = nullptr;
+  return getGraph(e, elapsedTime, nsteps, e->recordLists, &ge);
+}
+
+int brt_engine_stage_timing(brt_engine* e, int enable) {
+  if (!e) return BRT_ERR_ARG;
+  DeviceGuard guard(e->device);
+  if (enable && !e->ev[0][0]) {
+    for (int r = 0; r < brt_engine::kRing; ++r)
+      for (int k = 0; k < 5; ++k) BRT_CUDA_TRY(cudaEventCreate(&e->ev[r][k]));
+  }
+  if (!enable) {
+    for (int r = 0; r < brt_engine::kRing; ++r) {
+      int rc = drainSlot(e, r);
+      if (rc) return rc;
+    }
+  }
+  e->timing = enable != 0;
+  return BRT_OK;
+}
+
+int brt_engine_stage_times(brt_engine* e, double* ms4, uint64_t* steps, uint32_t* launches_per_step) {
+  if (!e) return BRT_ERR_ARG;
+  DeviceGuard guard(e->device);
+  for (int r = 0; r < brt_engine::kRing; ++r) {
+    int rc = drainSlot(e, (e->ringPos + r) % brt_engine::kRing);
+    if (rc) return rc;
+  }
+  if (ms4) for (int k = 0; k < 4; ++k) ms4[k] = e->stageMs[k];
+  if (steps) *steps = e->timedSteps;
+  if (launches_per_step) *launches_per_step = 3 + e->plan.passes;
+  e->stageMs[0] = e->stageMs[1] = e->stageMs[2] = e->stageMs[3] = 0;
+  e->timedSteps = 0;
+  return BRT_OK;
+}
+
+// ---- stage-wise functionalities ------------------------------------------------
+
+int brt_reorder_sim_data(brt_engine* e) {
+  if (!e) return BRT_ERR_ARG;
+  DeviceGuard guard(e->device);
+  if (e->N == 0) return BRT_OK;
+  int rc = enqueueReorder(e);
+  if (rc) return rc;
+  e->reordered = true;
+  e->listsValid = false;
+  return BRT_OK;
+}
+
+int brt_compute_neighborhoods(brt_engine* e) {
+  if (!e) return BRT_ERR_ARG;
+  if (!e->reordered) { setLastError("computeNeighborhoods before reorderSimData"); return BRT_ERR_STATE; }
+  DeviceGuard guard(e->device);
+  BRT_CUDA_TRY(launchLists(stageArgs(e), e->anyKnn, e->stream));
+  e->listsValid = true;
+  return BRT_OK;
+}
+
+int brt_reset_steer_force(brt_engine* e) {
+  if (!e) return BRT_ERR_ARG;
+  DeviceGuard guard(e->device);
+  if (e->N) BRT_CUDA_TRY(cudaMemsetAsync(e->steer, 0, (size_t)e->N * 16, e->stream));
+  return BRT_OK;
+}
+
+static int steerStage(brt_engine* e, int which) {
+  if (!e) return BRT_ERR_ARG;
+  if (!e->reordered || !e->listsValid) { setLastError("steering stage before computeNeighborhoods"); return BRT_ERR_STATE; }
+  DeviceGuard guard(e->device);
+  BRT_CUDA_TRY(launchSteerStage(stageArgs(e), which, e->stream));
+  return BRT_OK;
+}
+
+int brt_compute_separations(brt_engine* e) { return steerStage(e, 0); }
+int brt_compute_alignments(brt_engine* e) { return steerStage(e, 1); }
+int brt_compute_cohesions(brt_engine* e) { return steerStage(e, 2); }
+int brt_steer_for_clustering(brt_engine* e) { return steerStage(e, 3); }
+// In the periodic world every position is inside the world box, so the
+// reference's seek-to-centre force is zero (OpenSteerWrapper_kernel.cu:236-246);
+// this stage applies the static obstacle field of the EnvGrid3D grid instead.
+int brt_compute_seekings_world_center(brt_engine* e) { return steerStage(e, 4); }
+
+int brt_apply_steering_forces(brt_engine* e, float elapsedTime) {
+  if (!e) return BRT_ERR_ARG;
+  if (!e->reordered || !e->listsValid) { setLastError("applySteeringForces before computeNeighborhoods"); return BRT_ERR_STATE; }
+  DeviceGuard guard(e->device);
+  BRT_CUDA_TRY(launchIntegrateStage(stageArgs(e), elapsedTime, e->stream));
+  return BRT_OK;
+}
+
+// ---- getters -------------------------------------------------------------------
+
+static cudaMemcpyKind kindOut(int where) { return where == BRT_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice; }
+
+int brt_get_hash(brt_engine* e, uint32_t* keys, uint32_t* ids, int where) {
+  if (!e) return BRT_ERR_ARG;
+  if (!e->reordered) { setLastError("getHash before reorderSimData"); return BRT_ERR_STATE; }
+  DeviceGuard guard(e->device);
+  const size_t n = e->N;
+  if (n == 0) return BRT_OK;
+  if (where == BRT_MEM_DEVICE) {
+    BRT_CUDA_TRY(launchHashPairsOut(e->pairs[e->finalPairs], e->idS, keys, ids, e->N, e->stream));
+    return BRT_OK;
+  }
+  uint32_t* tk = (uint32_t*)e->stage4;
+  uint32_t* ti = tk + n;
+  BRT_CUDA_TRY(launchHashPairsOut(e->pairs[e->finalPairs], e->idS, tk, ti, e->N, e->stream));
+  if (keys) BRT_CUDA_TRY(cudaMemcpyAsync(keys, tk, n * 4, cudaMemcpyDeviceToHost, e->stream));
+  if (ids) BRT_CUDA_TRY(cudaMemcpyAsync(ids, ti, n * 4, cudaMemcpyDeviceToHost, e->stream));
+  return syncAndCheck(e);
+}
+
+int brt_get_cell_ranges(brt_engine* e, uint32_t* cell_start, uint32_t* cell_end, int where) {
+  if (!e) return BRT_ERR_ARG;
+  if (!e->reordered) { setLastError("getCellStart before reorderSimData"); return BRT_ERR_STATE; }
+  DeviceGuard guard(e->device);
+  if (cell_start) BRT_CUDA_TRY(cudaMemcpyAsync(cell_start, e->cellStart, (size_t)e->C * 4, kindOut(where), e->stream));
+  if (cell_end) BRT_CUDA_TRY(cudaMemcpyAsync(cell_end, e->cellEnd, (size_t)e->C * 4, kindOut(where), e->stream));
+  if (where == BRT_MEM_HOST) return syncAndCheck(e);
+  return BRT_OK;
+}
+
+int brt_get_neighbor_lists(brt_engine* e, uint32_t* lists, int where) {
+  if (!e || !lists) return BRT_ERR_ARG;
+  if (!e->listsValid) { setLastError("neighbour lists not computed (computeNeighborhoods or record_lists)"); return BRT_ERR_STATE; }
+  DeviceGuard guard(e->device);
+  BRT_CUDA_TRY(cudaMemcpyAsync(lists, e->lists, (size_t)e->N * e->listStride * 4, kindOut(where), e->stream));
+  if (where == BRT_MEM_HOST) return syncAndCheck(e);
+  return BRT_OK;
+}
+
+int brt_get_steer_force(brt_engine* e, float* steer4, int where) {
+  if (!e || !steer4) return BRT_ERR_ARG;
+  DeviceGuard guard(e->device);
+  BRT_CUDA_TRY(cudaMemcpyAsync(steer4, e->steer, (size_t)e->N * 16, kindOut(where), e->stream));
+  if (where == BRT_MEM_HOST) return syncAndCheck(e);
+  return BRT_OK;
+}
+
+}  // extern "C"
+
+namespace {
+int configureKernels(brt_engine* e) {
+  BRT_CUDA_TRY(configureFusedKernels(e->Mmax));
+  return BRT_OK;
+}
+}  // namespace

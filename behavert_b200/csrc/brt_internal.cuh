@@ -1,0 +1,139 @@
+// brt_internal.cuh -- shared declarations of the CUDA library (not installed).
+//
+// The whole library is compiled with --fmad=false and IEEE division / square
+// root, so every float + - * / sqrt below is one correctly rounded operation
+// in the order written.  That is the same operation sequence the reference's
+// device functions spell out (Core/common_resources.cu, the *_resources.cu
+// files of the plugins), so results are reproducible bit for bit by a host
+// build of the same sequence.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include "../../include/behavert_b200.h"
+
+namespace brt {
+
+constexpr uint32_t kEmpty = 0xFFFFFFFFu;
+
+// Device error word bits (set by kernels, read by brt_engine_check_device_error).
+constexpr uint32_t kDevErrLookback = 1u;   // onesweep look-back spin limit hit
+constexpr uint32_t kDevErrCapacity = 2u;   // a per-kernel capacity check fired
+constexpr uint32_t kDevErrOrder = 4u;      // pipeline invariant violated
+
+// Per-flock parameters as the kernels read them (one entry per flock).
+struct FlockDev {
+  // geometry: periodic cube [0, L)^3, G cells per side of size cell
+  uint32_t G, C, cellBase, agentBase, n;
+  float L, cell;
+  // Proximity3D
+  float radius;
+  float r2thr;          // d2 <= r2thr  <=>  !(sqrtf(d2) > radius)
+  uint32_t M, maxPerCell;
+  int32_t useKnn;
+  // OpenSteerWrapper
+  float maxSpeed, maxForce, mass, minR;
+  float sep[3], ali[3], coh[3];
+  int32_t use2D;
+  // BehaviorClustering
+  uint32_t F;
+  float relax;
+  float clus, aclus;
+  float simStats[3];
+  float avgCtl;
+  // obstacles
+  uint32_t numObstacles;
+  float obsW;
+  uint32_t obsBase;     // first entry in the engine-wide obstacle table
+  uint32_t pad;
+};
+
+// ---------------------------------------------------------------------------
+// float3 helpers in the reference's operation order (cutil_math semantics,
+// normalize = v * (1 / sqrtf(dot(v, v)))).
+struct f3 { float x, y, z; };
+__host__ __device__ __forceinline__ f3 mk3(float x, float y, float z) { f3 r; r.x = x; r.y = y; r.z = z; return r; }
+__host__ __device__ __forceinline__ f3 add3(f3 a, f3 b) { return mk3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__host__ __device__ __forceinline__ f3 sub3(f3 a, f3 b) { return mk3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__host__ __device__ __forceinline__ f3 mul3(f3 a, float s) { return mk3(a.x * s, a.y * s, a.z * s); }
+__host__ __device__ __forceinline__ f3 div3(f3 a, float s) { return mk3(a.x / s, a.y / s, a.z / s); }
+__host__ __device__ __forceinline__ float dot3(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__host__ __device__ __forceinline__ float len3(f3 a) { return sqrtf(dot3(a, a)); }
+__host__ __device__ __forceinline__ f3 normalize3(f3 v) { float inv = 1.0f / sqrtf(dot3(v, v)); return mul3(v, inv); }
+__host__ __device__ __forceinline__ float clampf(float f, float a, float b) { return fmaxf(a, fminf(f, b)); }
+__host__ __device__ __forceinline__ f3 xyz(float4 v) { return mk3(v.x, v.y, v.z); }
+
+// envgrid3d_resources.cu:60-84 with origin 0 and clamping to the grid.
+__device__ __forceinline__ int gridCoord(float x, float cell, uint32_t G) {
+  int g = (int)floorf(x / cell);
+  return max(0, min(g, (int)G - 1));
+}
+
+// Neighbour cell through offset o from home coordinate g, with its image shift.
+__device__ __forceinline__ int wrapCoord(int c, uint32_t G) {
+  return c < 0 ? c + (int)G : (c >= (int)G ? c - (int)G : c);
+}
+__device__ __forceinline__ float imageShift(int g, int o, uint32_t G, float L) {
+  return (o < 0 && g == 0) ? -L : ((o > 0 && g == (int)G - 1) ? L : 0.0f);
+}
+
+// Image shift of a listed neighbour from the two cell coordinates.
+__device__ __forceinline__ float imageShiftCells(int gi, int gj, uint32_t G, float L) {
+  return (gi == 0 && gj == (int)G - 1) ? -L : ((gi == (int)G - 1 && gj == 0) ? L : 0.0f);
+}
+
+// Flock of a sorted slot (flocks own contiguous slot ranges).
+__device__ __forceinline__ uint32_t flockOfSlot(const uint32_t* __restrict__ agentBase, uint32_t nflocks, uint32_t slot) {
+  uint32_t lo = 0, hi = nflocks;  // agentBase has nflocks+1 entries
+  while (hi - lo > 1) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(&agentBase[mid]) <= slot) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// ---------------------------------------------------------------------------
+// Sort plan shared by the engine and the standalone entry point.
+struct SortPlan {
+  uint32_t n = 0, bits = 0, passes = 0, digitBits = 0, bins = 0, tiles = 0;
+  uint32_t shift[4] = {0, 0, 0, 0};
+};
+constexpr uint32_t kSortThreads = 256;
+constexpr uint32_t kSortItems = 8;
+constexpr uint32_t kSortTile = kSortThreads * kSortItems;
+
+SortPlan makeSortPlan(uint32_t n, uint32_t bits, uint32_t maxDigitBits);
+// Scratch layout inside one allocation.
+struct SortScratch {
+  uint32_t* hist;      // passes * bins
+  uint32_t* counters;  // passes (tile counters)
+  uint32_t* status;    // passes * tiles * bins
+  uint2* tmp;          // n pairs (ping-pong), may be null for the engine
+  size_t bytes;
+};
+size_t sortScratchBytes(const SortPlan& p, bool withTmp);
+SortScratch carveSortScratch(const SortPlan& p, void* base, bool withTmp);
+
+// Launch one onesweep pass.
+cudaError_t launchOnesweepPass(const SortPlan& p, uint32_t pass, const uint2* in, uint2* out,
+                               const SortScratch& s, uint32_t* errWord, cudaStream_t st);
+// Histogram of all passes' digits (standalone sort only; the engine fuses it
+// into the hash kernel).
+cudaError_t launchSortHistogram(const SortPlan& p, const uint2* in, const SortScratch& s, cudaStream_t st);
+
+// Thread-local error message.
+void setLastError(const std::string& msg);
+
+}  // namespace brt
+
+#define BRT_CUDA_TRY(expr)                                                              \
+  do {                                                                                  \
+    cudaError_t _e = (expr);                                                            \
+    if (_e != cudaSuccess) {                                                            \
+      ::brt::setLastError(std::string(#expr) + ": " + cudaGetErrorString(_e));          \
+      return BRT_ERR_CUDA;                                                              \
+    }                                                                                   \
+  } while (0)

@@ -1,0 +1,84 @@
+// brt_kernels.cuh -- argument blocks and launchers of the pipeline kernels.
+#pragma once
+
+#include "brt_internal.cuh"
+
+namespace brt {
+
+constexpr uint32_t kFusedThreads = 128;
+
+struct HashArgs {
+  const float4* pos;           // canonical slot order
+  const uint32_t* id;          // agent id per canonical slot
+  uint2* pairs;                // out, agent-id order: (key, slot)
+  const FlockDev* flocks;
+  const uint32_t* agentBase;   // nflocks + 1
+  uint32_t nflocks, n;
+  uint32_t passes, bins;
+  uint32_t shift[4], mask[4];
+  uint32_t* hist;              // passes * bins, accumulated with atomics
+  uint32_t* cellStart;
+  uint32_t* cellEnd;
+  uint32_t cellWords4;         // cell words / 4 (arrays padded to 4)
+  uint32_t* status;            // sort look-back state to clear
+  uint32_t statusWords;
+  uint32_t* counters;          // sort tile counters to clear
+};
+
+struct ReorderArgs {
+  const uint2* pairs;          // sorted (key, previous slot)
+  const float4* posA; const float4* fwdA; const float4* accA;
+  const float* featA; const uint32_t* idA;
+  float4* posS; float4* fwdS; float4* accS; float* featS; uint32_t* idS;
+  uint32_t fs4;                // feature float4s per agent
+  uint32_t* cellStart; uint32_t* cellEnd;
+  uint32_t* hist; uint32_t histWords;
+  uint32_t n, numCells;
+  uint32_t* errWord;
+};
+
+struct FusedArgs {
+  const float4* posS; const float4* fwdS; const float4* accS;
+  const float* featS; const uint32_t* idS;
+  float4* posA; float4* fwdA; float4* accA; float* featA; uint32_t* idA;
+  float4* statsById;
+  const uint32_t* cellStart; const uint32_t* cellEnd;
+  const FlockDev* flocks; const uint32_t* agentBase;
+  const float4* obstacles;
+  uint32_t* lists;             // optional, stride listStride
+  uint32_t listStride;
+  uint32_t nflocks, n, Mmax, Fs;
+  float dt;
+};
+
+struct StageArgs {
+  const float4* posS; const float4* fwdS; const float4* accS;
+  const float* featS; const uint32_t* idS;
+  float4* posA; float4* fwdA; float4* accA; float* featA; uint32_t* idA;
+  float4* statsById;
+  float4* steer;
+  const uint32_t* cellStart; const uint32_t* cellEnd;
+  const FlockDev* flocks; const uint32_t* agentBase;
+  const float4* obstacles;
+  uint32_t* lists;
+  uint32_t listStride;
+  uint32_t nflocks, n, Fs;
+};
+
+cudaError_t launchHash(const HashArgs& A, uint32_t maxBlocks, cudaStream_t st);
+cudaError_t launchReorder(const ReorderArgs& A, cudaStream_t st);
+cudaError_t launchFused(const FusedArgs& A, bool knn, cudaStream_t st);
+cudaError_t launchLists(const StageArgs& A, bool knn, cudaStream_t st);
+cudaError_t launchSteerStage(const StageArgs& A, int which, cudaStream_t st);
+cudaError_t launchIntegrateStage(const StageArgs& A, float dt, cudaStream_t st);
+cudaError_t launchScatterToId(const float4* src, const uint32_t* id, float4* dst, uint32_t n, cudaStream_t st);
+cudaError_t launchScatterFeatToId(const float* src, uint32_t Fs, const uint32_t* id, float* dst, uint32_t F, uint32_t n, cudaStream_t st);
+cudaError_t launchLoadFeat(const float* src, uint32_t F, float* dst, uint32_t Fs, uint32_t n, cudaStream_t st);
+cudaError_t launchGatherFromId(const float4* src, const uint32_t* id, float4* dst, uint32_t n, bool forceW1, cudaStream_t st);
+cudaError_t configureFusedKernels(uint32_t Mmax);
+cudaError_t launchGatherFeatFromId(const float* src, uint32_t F, const uint32_t* id, float* dst, uint32_t Fs, uint32_t n, cudaStream_t st);
+cudaError_t launchHashPairsOut(const uint2* pairs, const uint32_t* idS, uint32_t* keys, uint32_t* ids, uint32_t n, cudaStream_t st);
+
+uint32_t sortPassMask(const SortPlan& p, uint32_t pass);
+
+}  // namespace brt

@@ -1,0 +1,207 @@
+"""Python mirror of the reference's engine functionalities over the C-ABI.
+
+`Engine` exposes the plugin chain's per-frame methods under the reference's
+names (EnvGrid3DPlugIn::reorderSimData, Proximity3DPlugIn::computeNeighborhoods,
+OpenSteerWrapperPlugIn::computeSeparations ... applySteeringForces,
+BehaviorClusteringPlugIn::steerForClustering) and the getters of the features
+they produce (getPos, getForward, getHash, getCellStart, neighbour lists).
+Every call goes through libbehavert_b200.so; nothing here computes.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional, Sequence
+
+import numpy as np
+
+from ._abi import (BRT_MEM_DEVICE, BRT_MEM_HOST, BrtParams, check, lib, ptr)
+
+
+class Engine:
+    """One or many flocks simulated on one GPU (a `brt_engine`)."""
+
+    def __init__(self, flocks: Sequence[BrtParams] | BrtParams, device: int = 0):
+        if isinstance(flocks, BrtParams):
+            flocks = [flocks]
+        arr = (BrtParams * len(flocks))(*flocks)
+        h = C.c_void_p()
+        check(lib().brt_engine_create(arr, len(flocks), device, C.byref(h)), "brt_engine_create")
+        self._h = h
+        self.flocks = [f.copy() for f in flocks]
+        n = C.c_uint32()
+        check(lib().brt_engine_num_agents(h, C.byref(n)), "num_agents")
+        self.num_agents = n.value
+        check(lib().brt_engine_num_cells(h, C.byref(n)), "num_cells")
+        self.num_cells = n.value
+        check(lib().brt_neighbor_list_stride(h, C.byref(n)), "list_stride")
+        self.list_stride = n.value
+        self.features_count = max(int(f.featuresCount) for f in flocks)
+
+    # -- lifetime -------------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            check(lib().brt_engine_destroy(self._h), "brt_engine_destroy")
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def set_params(self, flock: int, p: BrtParams) -> None:
+        check(lib().brt_engine_set_params(self._h, flock, C.byref(p)), "brt_engine_set_params")
+        self.flocks[flock] = p.copy()
+
+    def sync(self) -> None:
+        check(lib().brt_sync(self._h), "brt_sync")
+
+    def record_lists(self, enable: bool = True) -> None:
+        check(lib().brt_engine_record_lists(self._h, int(enable)), "record_lists")
+
+    def stream_handle(self) -> int:
+        s = C.c_void_p()
+        check(lib().brt_engine_stream(self._h, C.byref(s)), "brt_engine_stream")
+        return s.value or 0
+
+    def device_error(self) -> int:
+        w = C.c_uint32()
+        check(lib().brt_engine_check_device_error(self._h, C.byref(w)), "check_device_error")
+        return w.value
+
+    # -- features ---------------------------------------------------------------
+    @staticmethod
+    def _where(a) -> int:
+        if a is None or isinstance(a, np.ndarray):
+            return BRT_MEM_HOST
+        return BRT_MEM_DEVICE if getattr(a, "is_cuda", False) else BRT_MEM_HOST
+
+    def set_state(self, pos4=None, fwd4=None, acc4=None, features=None) -> None:
+        arrays = [a for a in (pos4, fwd4, acc4, features) if a is not None]
+        where = self._where(arrays[0]) if arrays else BRT_MEM_HOST
+        check(lib().brt_set_state(self._h, ptr(pos4), ptr(fwd4), ptr(acc4), ptr(features), where), "brt_set_state")
+
+    def get_state(self, features: bool = True):
+        n = self.num_agents
+        pos = np.empty((n, 4), np.float32)
+        fwd = np.empty((n, 4), np.float32)
+        acc = np.empty((n, 4), np.float32)
+        feat = np.empty((n, self.features_count), np.float32) if (features and self.features_count) else None
+        check(lib().brt_get_state(self._h, ptr(pos), ptr(fwd), ptr(acc), ptr(feat), BRT_MEM_HOST), "brt_get_state")
+        return pos, fwd, acc, feat
+
+    def get_state_into(self, pos4=None, fwd4=None, acc4=None, features=None) -> None:
+        arrays = [a for a in (pos4, fwd4, acc4, features) if a is not None]
+        where = self._where(arrays[0]) if arrays else BRT_MEM_HOST
+        check(lib().brt_get_state(self._h, ptr(pos4), ptr(fwd4), ptr(acc4), ptr(features), where), "brt_get_state")
+
+    def set_similarity_stats(self, stats4) -> None:
+        check(lib().brt_set_similarity_stats(self._h, ptr(stats4), self._where(stats4)), "set_similarity_stats")
+
+    def get_similarity_stats(self) -> np.ndarray:
+        out = np.empty((self.num_agents, 4), np.float32)
+        check(lib().brt_get_similarity_stats(self._h, ptr(out), BRT_MEM_HOST), "get_similarity_stats")
+        return out
+
+    # -- the fused step ---------------------------------------------------------------
+    def step(self, dt: float, nsteps: int = 1) -> None:
+        check(lib().brt_step(self._h, dt, nsteps), "brt_step")
+
+    def step_prepare(self, dt: float, nsteps: int) -> None:
+        check(lib().brt_step_prepare(self._h, dt, nsteps), "brt_step_prepare")
+
+    def stage_timing(self, enable: bool = True) -> None:
+        check(lib().brt_engine_stage_timing(self._h, int(enable)), "brt_engine_stage_timing")
+
+    def stage_times(self):
+        """(ms per stage [hash, sort, reorder, fused] summed, timed steps, launches per step)."""
+        ms = (C.c_double * 4)()
+        steps = C.c_uint64()
+        launches = C.c_uint32()
+        check(lib().brt_engine_stage_times(self._h, ms, C.byref(steps), C.byref(launches)), "brt_engine_stage_times")
+        return list(ms), steps.value, launches.value
+
+    # -- stage-wise functionalities (reference names) --------------------------------------
+    def reorderSimData(self) -> None:
+        check(lib().brt_reorder_sim_data(self._h), "reorderSimData")
+
+    def computeNeighborhoods(self) -> None:
+        check(lib().brt_compute_neighborhoods(self._h), "computeNeighborhoods")
+
+    def resetSteerForce(self) -> None:
+        check(lib().brt_reset_steer_force(self._h), "resetSteerForce")
+
+    def computeSeparations(self) -> None:
+        check(lib().brt_compute_separations(self._h), "computeSeparations")
+
+    def computeAlignments(self) -> None:
+        check(lib().brt_compute_alignments(self._h), "computeAlignments")
+
+    def computeCohesions(self) -> None:
+        check(lib().brt_compute_cohesions(self._h), "computeCohesions")
+
+    def steerForClustering(self) -> None:
+        check(lib().brt_steer_for_clustering(self._h), "steerForClustering")
+
+    def computeSeekingsWorldCenter(self) -> None:
+        check(lib().brt_compute_seekings_world_center(self._h), "computeSeekingsWorldCenter")
+
+    def applySteeringForces(self, dt: float) -> None:
+        check(lib().brt_apply_steering_forces(self._h, dt), "applySteeringForces")
+
+    def update_stagewise(self, dt: float) -> None:
+        """The BehaveRT_Clustering per-frame sequence, stage by stage."""
+        self.reorderSimData()
+        self.computeNeighborhoods()
+        self.resetSteerForce()
+        self.computeSeparations()
+        self.computeAlignments()
+        self.computeCohesions()
+        self.steerForClustering()
+        self.computeSeekingsWorldCenter()
+        self.applySteeringForces(dt)
+
+    # -- getters ------------------------------------------------------------------------------
+    def getHash(self):
+        n = self.num_agents
+        keys = np.empty(n, np.uint32)
+        ids = np.empty(n, np.uint32)
+        check(lib().brt_get_hash(self._h, ptr(keys), ptr(ids), BRT_MEM_HOST), "getHash")
+        return keys, ids
+
+    def getCellRanges(self):
+        cs = np.empty(self.num_cells, np.uint32)
+        ce = np.empty(self.num_cells, np.uint32)
+        check(lib().brt_get_cell_ranges(self._h, ptr(cs), ptr(ce), BRT_MEM_HOST), "getCellStart")
+        return cs, ce
+
+    def getNeighborLists(self) -> np.ndarray:
+        out = np.empty((self.num_agents, self.list_stride), np.uint32)
+        check(lib().brt_get_neighbor_lists(self._h, ptr(out), BRT_MEM_HOST), "neighbor lists")
+        return out
+
+    def getSteerForce(self) -> np.ndarray:
+        out = np.empty((self.num_agents, 4), np.float32)
+        check(lib().brt_get_steer_force(self._h, ptr(out), BRT_MEM_HOST), "getSteerForce")
+        return out
+
+
+def radix_sort_pairs(pairs_in, pairs_out, n: int, bits: int, scratch, stream: Optional[int] = None) -> None:
+    """Standalone onesweep sort of uint2 (key, value) pairs on device memory."""
+    nbytes = scratch.numel() * scratch.element_size() if hasattr(scratch, "numel") else scratch.nbytes
+    check(lib().brt_radix_sort_pairs(ptr(pairs_in), ptr(pairs_out), n, bits, ptr(scratch), nbytes,
+                                     C.c_void_p(stream) if stream else None), "brt_radix_sort_pairs")
+
+
+def radix_sort_scratch_bytes(n: int, bits: int) -> int:
+    return int(lib().brt_radix_sort_scratch_bytes(n, bits))

@@ -1,0 +1,228 @@
+/*
+ * behavert_b200.h -- C-ABI of the B200-native BehaveRT per-step agent pipeline.
+ *
+ * One shared library (libbehavert_b200.so) exports these functions.  The
+ * signatures use plain C types only (no CUDA or torch types): pointers, sizes
+ * and status codes.  Every function returns an int status (BRT_OK == 0) and
+ * never exits the process; brt_last_error() returns a message for the last
+ * failing call made on the calling thread.
+ *
+ * Reference interfaces replaced (paths are inside the BehaveRT project):
+ *   - The plugin functionalities of the mixin engine
+ *       EnvGrid3DPlugIn::reorderSimData        PlugIns/EnvGrid3D/include/EnvGrid3DPlugIn.h:293-415
+ *       Proximity3DPlugIn::computeNeighborhoods PlugIns/Proximity3D/include/Proximity3DPlugIn.h:261-308
+ *       OpenSteerWrapperPlugIn::{resetSteerForce, computeSeparations,
+ *         computeAlignments, computeCohesions, computeSeekingsWorldCenter,
+ *         applySteeringForces}                   PlugIns/OpenSteerWrapper/include/OpenSteerWrapperPlugIn.h:288-424
+ *       BehaviorClusteringPlugIn::steerForClustering
+ *                                                PlugIns/BehaviorClustering/include/BehaviorClusteringPlugIn.h:740-822
+ *   - The feature arrays (DeviceArrayWrapper<T>, Core/include/DeviceArrayWrapper.h:58-192):
+ *       position / forward / smoothAccel (float4), featuresVector (float x F),
+ *       similarityStats (float4), agentHash (uint2), cellStart (uint),
+ *       neighList (uint, stride maxNeighbors+1).
+ *   - The parameter structs hBody3DParams, hEnvGrid3DParams, hProximity3DParams,
+ *       hOpenSteerWrapperParams, hBehaviorClusteringParams (field names kept).
+ *   - BehaveRT::RadixSort(KeyValuePair*, KeyValuePair*, elements, bits)
+ *       PlugIns/EnvGrid3D/radixsort.cu:50-80
+ *
+ * Layout conventions
+ *   - All per-agent arrays handed across this boundary are in AGENT-ID order,
+ *     like the reference's id-ordered features after applySteeringForces
+ *     (OpenSteerWrapper_kernel.cu:324-331).  float4 arrays are 4 floats per
+ *     agent; features are featuresCount floats per agent.
+ *   - Sorted-order outputs (hash pairs, cell ranges, neighbour lists, steering
+ *     forces) use SORTED SLOTS, exactly like the reference's getHash(),
+ *     getCellStart() and neighList.
+ *   - `where` selects host (BRT_MEM_HOST) or device (BRT_MEM_DEVICE) pointers.
+ *
+ * Threading: one engine per host thread.  Work is enqueued on the engine's own
+ * CUDA stream; host-buffer getters synchronise that stream.
+ */
+#ifndef BEHAVERT_B200_H
+#define BEHAVERT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BRT_ABI_VERSION 1
+
+/* status codes */
+#define BRT_OK            0
+#define BRT_ERR_CUDA      1  /* a CUDA runtime call failed                     */
+#define BRT_ERR_CONFIG    2  /* invalid parameters (grid < 3 cells, M > 128 ...) */
+#define BRT_ERR_CAPACITY  3  /* a size limit was exceeded                      */
+#define BRT_ERR_TIMEOUT   4  /* a bounded device spin-wait gave up             */
+#define BRT_ERR_ARG       5  /* null pointer / bad argument                    */
+#define BRT_ERR_STATE     6  /* call order violated (e.g. lists not computed)  */
+#define BRT_ERR_NODEVICE  7  /* no CUDA device                                 */
+
+#define BRT_MEM_HOST   0
+#define BRT_MEM_DEVICE 1
+
+#define BRT_MAX_NEIGHBORS   128  /* Proximity3d_MAX_NEIGHBORS, Proximity3D_kernel.cuh:37        */
+#define BRT_MAX_FEATUREDIM   32  /* BehaviorClustering_MAX_FEATUREDIM, BehaviorClustering_kernel.cuh:39 */
+#define BRT_MAX_OBSTACLES    64  /* per flock                                                     */
+
+/*
+ * Parameters of one flock (one independent simulation).  Field names follow
+ * the reference's host parameter structs; the world is the periodic cube
+ * [0, worldSize)^3 split into gridSize^3 cells of side cellSize
+ * (worldSize == gridSize * cellSize, gridSize >= 3).
+ */
+typedef struct brt_params {
+    /* Body3DParams (PlugIns/Body/include/body3d_kernel.cuh:39-58) */
+    uint32_t numBodies;
+    float    commonRadius;
+    int32_t  use2DProjection;
+
+    /* EnvGrid3DParams (PlugIns/EnvGrid3D/include/envgrid3d_kernel.cuh:38-65),
+       periodic cube instead of the reference's padded clamped box */
+    float    worldSize;
+    float    cellSize;
+    uint32_t maxBodiesPerCell;     /* 0 = unbounded (per-cell scan cap)      */
+    int32_t  disableSorting;       /* accepted for drop-in, must be 0        */
+
+    /* Proximity3DParams (PlugIns/Proximity3D/include/Proximity3D_kernel.cuh:40-73) */
+    uint32_t maxNeighbors;         /* 1..BRT_MAX_NEIGHBORS                   */
+    int32_t  useKnn;               /* replace-farthest when the list is full */
+    float    commonSearchRadius;
+
+    /* OpenSteerWrapperParams (PlugIns/OpenSteerWrapper/include/OpenSteerWrapper_kernel.cuh:36-55) */
+    float    commonMaxSpeed;
+    float    commonMaxForce;
+    float    commonMass;
+    float    commonSensingMinRadius;
+    float    separationParams[3];  /* weight, radius, cosMaxAngle            */
+    float    cohesionParams[3];
+    float    alignmentParams[3];
+
+    /* BehaviorClusteringParams (PlugIns/BehaviorClustering/include/BehaviorClustering_kernel.cuh:41-60) */
+    uint32_t featuresCount;        /* 0..BRT_MAX_FEATUREDIM                  */
+    float    clusteringForceParams[3];          /* .x = weight               */
+    float    alignmentClusteringForceParams[3]; /* .x = weight               */
+    float    similarityStatsParams[3];          /* avg rate, min/max rate, memory */
+    float    avgSimilarityController;
+    /* Feature relaxation toward the similarity-weighted neighbour mean
+       (rate per step; 0 disables).  No reference counterpart. */
+    float    featureRelaxRate;
+
+    /* Static sphere obstacles on the EnvGrid3D grid (no reference counterpart;
+       nearest analogue moveAwayFromTarget_kernel, OpenSteerWrapper_kernel.cu:185-212) */
+    uint32_t numObstacles;         /* 0..BRT_MAX_OBSTACLES                    */
+    float    obstacleAvoidanceWeight;
+    float    obstacles[BRT_MAX_OBSTACLES][4]; /* centre xyz, radius            */
+} brt_params;
+
+/* Fills *p with the reference defaults used by the flocking demo and the
+   unspecified constants fixed by this library (commonMass 1, sensing min
+   radius 0, cosMaxAngle -2, unbounded maxBodiesPerCell, clustering steering
+   off). */
+int brt_params_default(brt_params* p);
+
+typedef struct brt_engine brt_engine;
+
+/* ---- library ---------------------------------------------------------- */
+const char* brt_version(void);
+const char* brt_error_string(int status);
+const char* brt_last_error(void);
+int brt_device_count(int* count);
+
+/* ---- engine lifetime (CommonResources + plugin install chain,
+        Core/src/CommonResources.cpp:49-92, Core/src/SimEnginePlugIn.cpp:45-56).
+   A single engine may hold many flocks; agent ids of flock f are
+   [sum_{g<f} numBodies_g, sum_{g<=f} numBodies_g). ---------------------- */
+int brt_engine_create(const brt_params* flocks, uint32_t num_flocks, int device, brt_engine** out);
+int brt_engine_destroy(brt_engine* e);
+int brt_engine_num_agents(const brt_engine* e, uint32_t* num_agents);
+int brt_engine_num_cells(const brt_engine* e, uint32_t* num_cells);
+/* Replace the parameters of one flock; geometry fields (numBodies,
+   worldSize, cellSize, maxNeighbors, featuresCount) must not change. */
+int brt_engine_set_params(brt_engine* e, uint32_t flock, const brt_params* p);
+/* The engine's CUDA stream (a cudaStream_t), for callers that enqueue their
+   own work around the engine's. */
+int brt_engine_stream(brt_engine* e, void** stream);
+int brt_sync(brt_engine* e);
+
+/* ---- feature arrays (DeviceArrayWrapper::copyArrayToDevice /
+        copyArrayFromDevice, Core/include/DeviceArrayWrapper.h:345-386) ---- */
+/* Any pointer may be NULL to leave that feature unchanged / not read.
+   pos4.w is ignored on input (the reference keeps w = 1); fwd4.w = speed. */
+int brt_set_state(brt_engine* e, const float* pos4, const float* fwd4,
+                  const float* acc4, const float* features, int where);
+int brt_get_state(brt_engine* e, float* pos4, float* fwd4,
+                  float* acc4, float* features, int where);
+/* similarityStats (float4 per agent: min, avg, max, unused) of BehaviorClustering */
+int brt_set_similarity_stats(brt_engine* e, const float* stats4, int where);
+int brt_get_similarity_stats(brt_engine* e, float* stats4, int where);
+
+/* ---- the fused per-step pipeline ------------------------------------------
+   hash -> onesweep sort -> reorder + cell ranges -> fused neighbour search +
+   steering + integration + clustering update, nsteps times.  nsteps > 1 runs
+   a CUDA graph of the whole loop.  Replaces the BehaveRT_Flocking update
+   sequence, Samples/OpensteerDemo/plugins/BehaveRT_Flocking.cpp:177-199. */
+int brt_step(brt_engine* e, float elapsedTime, uint32_t nsteps);
+/* Capture and instantiate the CUDA graph that brt_step(e, elapsedTime,
+   nsteps > 1) launches, without running it (so a timed loop excludes capture). */
+int brt_step_prepare(brt_engine* e, float elapsedTime, uint32_t nsteps);
+/* Per-stage CUDA-event timing of single-step brt_step calls (not graphs):
+   when enabled, events are recorded on the engine stream after the hash,
+   sort, reorder and fused stages of every step.  brt_engine_stage_times
+   synchronises and returns the accumulated milliseconds per stage
+   (ms[0] hash, ms[1] all sort passes, ms[2] reorder + cell ranges, ms[3]
+   fused pass), the number of timed steps and the kernel launches per step. */
+int brt_engine_stage_timing(brt_engine* e, int enable);
+int brt_engine_stage_times(brt_engine* e, double* ms4, uint64_t* steps, uint32_t* launches_per_step);
+
+/* ---- stage-wise functionalities (same names and order as the reference) -- */
+int brt_reorder_sim_data(brt_engine* e);              /* EnvGrid3DPlugIn.h:293-415          */
+int brt_compute_neighborhoods(brt_engine* e);         /* Proximity3DPlugIn.h:261-308        */
+int brt_reset_steer_force(brt_engine* e);             /* OpenSteerWrapperPlugIn.h:421-424   */
+int brt_compute_separations(brt_engine* e);           /* OpenSteerWrapperPlugIn.h:288-302   */
+int brt_compute_alignments(brt_engine* e);            /* OpenSteerWrapperPlugIn.h:326-344   */
+int brt_compute_cohesions(brt_engine* e);             /* OpenSteerWrapperPlugIn.h:350-366   */
+int brt_steer_for_clustering(brt_engine* e);          /* BehaviorClusteringPlugIn.h:740-822 */
+int brt_compute_seekings_world_center(brt_engine* e); /* OpenSteerWrapperPlugIn.h:380-393   */
+int brt_apply_steering_forces(brt_engine* e, float elapsedTime); /* OpenSteerWrapperPlugIn.h:400-418 */
+
+/* ---- getters of the intermediate features --------------------------------- */
+/* Sorted (cell hash, agent id) pairs as uint2, like getHash() after
+   reorderSimData (EnvGrid3DPlugIn.h:101-105).  keys/ids may be NULL. */
+int brt_get_hash(brt_engine* e, uint32_t* keys, uint32_t* ids, int where);
+/* cellStart / cellEnd per global cell; 0xFFFFFFFF for empty cells
+   (Proximity3D_kernel.cu:54-84 writes cellStart only). */
+int brt_get_cell_ranges(brt_engine* e, uint32_t* cell_start, uint32_t* cell_end, int where);
+/* Neighbour lists of the last computeNeighborhoods (or of the last fused step
+   when brt_engine_record_lists is on): numAgents * (maxNeighbors+1) uint32,
+   [count, slot_0, ..., slot_{count-1}, unused...] per sorted slot
+   (Proximity3D_kernel.cu:117-124).  Flocks with different maxNeighbors use
+   the engine-wide maximum as stride. */
+int brt_get_neighbor_lists(brt_engine* e, uint32_t* lists, int where);
+int brt_neighbor_list_stride(const brt_engine* e, uint32_t* stride);
+/* Steering force accumulated by the stage-wise calls, per sorted slot (float4). */
+int brt_get_steer_force(brt_engine* e, float* steer4, int where);
+/* Make brt_step also write the neighbour lists of every step (off by default:
+   the timed pipeline does not materialise them). */
+int brt_engine_record_lists(brt_engine* e, int enable);
+/* Device error word: nonzero after a bounded spin gave up or a capacity check
+   fired inside a kernel; cleared by this call. */
+int brt_engine_check_device_error(brt_engine* e, uint32_t* word);
+
+/* ---- standalone key/value radix sort (BehaveRT::RadixSort replacement) ----
+   Stable LSD onesweep sort with decoupled look-back of `n` (key, value) pairs
+   (uint2: key in .x, value in .y) on the low `bits` bits of the key.
+   pairs_in is not modified; the result goes to pairs_out.  `scratch` is
+   device memory of at least brt_radix_sort_scratch_bytes(n, bits) bytes;
+   `stream` is a cudaStream_t (NULL = default stream). */
+size_t brt_radix_sort_scratch_bytes(uint32_t n, uint32_t bits);
+int brt_radix_sort_pairs(const uint32_t* pairs_in, uint32_t* pairs_out, uint32_t n,
+                         uint32_t bits, void* scratch, size_t scratch_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BEHAVERT_B200_H */
