@@ -111,7 +111,7 @@ class ClockSampler:
         sm = [float(r[1]) for r in inside if r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in inside if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in inside for k in range(4) if "Active" in r[5 + k]})
+        reasons = sorted({names[k] for r in inside for k in range(4) if r[5 + k].strip() == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(inside)}
 
