@@ -120,6 +120,8 @@ _SIGS = {
     "brt_engine_check_device_error": (C.c_int, [_vp, _u32p]),
     "brt_radix_sort_scratch_bytes": (C.c_size_t, [C.c_uint32, C.c_uint32]),
     "brt_radix_sort_pairs": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, _vp, C.c_size_t, _vp]),
+    "brt_radix_sort_noalloc_max_pairs": (C.c_size_t, []),
+    "brt_radix_sort_pairs_noalloc": (C.c_int, [_vp, _vp, C.c_uint32, C.c_uint32, _vp]),
 }
 
 # Every symbol the public header declares (checked by the CPU tests).

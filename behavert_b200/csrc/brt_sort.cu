@@ -19,6 +19,8 @@
 #include "brt_internal.cuh"
 
 #include <algorithm>
+#include <mutex>
+#include <string>
 
 namespace brt {
 namespace {
@@ -346,5 +348,101 @@ extern "C" int brt_radix_sort_pairs(const uint32_t* pairs_in, uint32_t* pairs_ou
   BRT_CUDA_TRY(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, st));
   BRT_CUDA_TRY(cudaStreamSynchronize(st));
   if (herr) { brt::setLastError("brt_radix_sort_pairs: look-back spin limit reached"); return BRT_ERR_TIMEOUT; }
+  return BRT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the standalone sort.
+//
+// Some callers cannot call cudaMalloc: a frame loop or game-engine plugin
+// that must not stall (cudaFree synchronises the whole device), code that runs
+// under another framework's caching allocator which owns all device memory,
+// and hosts that fix their GPU memory budget at start-up.  For them the sort
+// scratch lives in one file-scope device array of a fixed size, sized for at
+// most kNoAllocMaxPairs pairs.  Every GPU that loads this library holds the
+// array (about 10 MiB) until the process exits.
+namespace {
+
+constexpr uint32_t kNoAllocMaxPairs = 1u << 20;
+constexpr size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
+// Worst case for n <= kNoAllocMaxPairs with 8-bit digits: 4 passes, 256 bins,
+// ceil(2^20 / tile) tiles; plus the ping-pong pairs and the error word.
+constexpr size_t kNoAllocTiles = (kNoAllocMaxPairs + brt::kSortTile - 1) / brt::kSortTile;
+constexpr size_t kNoAllocScratchBytes = a256(4 * 256 * 4) + a256(4 * 4) + a256(4 * kNoAllocTiles * 256 * 4) +
+                                        a256((size_t)kNoAllocMaxPairs * 8) + 256;
+
+static __device__ __align__(256) unsigned char g_noAllocSortScratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noAllocMutex;
+void* g_noAllocAddress[kNoAllocMaxDevices] = {};
+
+// The array's name is a host-side stand-in in host code, not a device
+// address: resolve the real address once per device, with that device current.
+int noAllocScratchAddress(void** out) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
+    brt::setLastError("brt_radix_sort_pairs_noalloc: no usable current device");
+    return BRT_ERR_NODEVICE;
+  }
+  std::lock_guard<std::mutex> lock(g_noAllocMutex);
+  if (!g_noAllocAddress[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noAllocSortScratch);
+    if (e != cudaSuccess || !p) {
+      brt::setLastError(std::string("brt_radix_sort_pairs_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+      return BRT_ERR_CUDA;
+    }
+    g_noAllocAddress[dev] = p;
+  }
+  *out = g_noAllocAddress[dev];
+  return BRT_OK;
+}
+
+}  // namespace
+
+extern "C" size_t brt_radix_sort_noalloc_max_pairs(void) { return kNoAllocMaxPairs; }
+
+extern "C" int brt_radix_sort_pairs_noalloc(const uint32_t* pairs_in, uint32_t* pairs_out, uint32_t n, uint32_t bits,
+                                            void* stream) {
+  if (n == 0) return BRT_OK;
+  if (!pairs_in || !pairs_out) { brt::setLastError("brt_radix_sort_pairs_noalloc: null pointer"); return BRT_ERR_ARG; }
+  if ((const void*)pairs_in == (const void*)pairs_out) {
+    brt::setLastError("brt_radix_sort_pairs_noalloc: in and out must differ");
+    return BRT_ERR_ARG;
+  }
+  if (n > kNoAllocMaxPairs) {
+    brt::setLastError("brt_radix_sort_pairs_noalloc: n exceeds the 1,048,576-pair limit of the static scratch; "
+                      "use brt_radix_sort_pairs with caller-allocated scratch");
+    return BRT_ERR_CAPACITY;
+  }
+  brt::SortPlan p = brt::makeSortPlan(n, bits, 8);
+  if (brt::sortScratchBytes(p, true) + 256 > kNoAllocScratchBytes) {
+    brt::setLastError("brt_radix_sort_pairs_noalloc: plan exceeds the static scratch");
+    return BRT_ERR_CAPACITY;
+  }
+  void* base = nullptr;
+  int rc = noAllocScratchAddress(&base);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  brt::SortScratch s = brt::carveSortScratch(p, base, true);
+  uint32_t* err = (uint32_t*)((char*)base + s.bytes);
+  // The array keeps the previous call's contents: clear the histogram, tile
+  // counters, look-back status and error word (the ping-pong half is fully
+  // overwritten before it is read).
+  BRT_CUDA_TRY(cudaMemsetAsync(base, 0, (size_t)((char*)s.tmp - (char*)base), st));
+  BRT_CUDA_TRY(cudaMemsetAsync(err, 0, 4, st));
+  BRT_CUDA_TRY(brt::launchSortHistogram(p, (const uint2*)pairs_in, s, st));
+  const uint2* src = (const uint2*)pairs_in;
+  for (uint32_t k = 0; k < p.passes; ++k) {
+    uint2* dst = (((p.passes - 1 - k) & 1u) == 0u) ? (uint2*)pairs_out : s.tmp;
+    BRT_CUDA_TRY(brt::launchOnesweepPass(p, k, src, dst, s, err, st));
+    src = dst;
+  }
+  uint32_t herr = 0;
+  BRT_CUDA_TRY(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, st));
+  BRT_CUDA_TRY(cudaStreamSynchronize(st));
+  if (herr) { brt::setLastError("brt_radix_sort_pairs_noalloc: look-back spin limit reached"); return BRT_ERR_TIMEOUT; }
   return BRT_OK;
 }

@@ -221,6 +221,27 @@ size_t brt_radix_sort_scratch_bytes(uint32_t n, uint32_t bits);
 int brt_radix_sort_pairs(const uint32_t* pairs_in, uint32_t* pairs_out, uint32_t n,
                          uint32_t bits, void* scratch, size_t scratch_bytes, void* stream);
 
+/* ---- the same sort without any allocation ------------------------------------
+   No counterpart in the reference.  For callers that cannot call cudaMalloc:
+   frame loops and engine plugins that must not stall the device (cudaFree
+   synchronises it), code running under another framework's caching allocator
+   that owns all device memory, and hosts that fix their GPU memory budget at
+   start-up.  The scratch is one static device array inside this library
+   (about 10 MiB on every GPU that loads it, held until the process exits), so:
+     - n is limited to brt_radix_sort_noalloc_max_pairs() (1,048,576) pairs;
+       larger n returns BRT_ERR_CAPACITY;
+     - the first call on a device looks up the array's device address for the
+       current device; make that first call before any stream capture;
+     - every call clears the parts of the array that must start at zero, but
+       all calls share the array: calls that overlap on the GPU (other
+       streams, other host threads) race and must be serialised by the caller;
+     - it allocates nothing: no cudaMalloc, cudaFree or allocating library call.
+   Results are identical to brt_radix_sort_pairs; the call synchronises
+   `stream` to read the device error word. */
+size_t brt_radix_sort_noalloc_max_pairs(void);
+int brt_radix_sort_pairs_noalloc(const uint32_t* pairs_in, uint32_t* pairs_out, uint32_t n,
+                                 uint32_t bits, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
