@@ -92,6 +92,7 @@ _SIGS = {
     "brt_engine_num_agents": (C.c_int, [_vp, _u32p]),
     "brt_engine_num_cells": (C.c_int, [_vp, _u32p]),
     "brt_engine_set_params": (C.c_int, [_vp, C.c_uint32, C.POINTER(BrtParams)]),
+    "brt_engine_set_option": (C.c_int, [_vp, C.c_char_p, C.c_int64]),
     "brt_engine_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
     "brt_sync": (C.c_int, [_vp]),
     "brt_set_state": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int]),

@@ -15,7 +15,7 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libbehavert_b200.so"
-SOURCES = ["brt_sort.cu", "brt_kernels.cu", "brt_engine.cu"]
+SOURCES = ["brt_sort.cu", "brt_kernels.cu", "brt_fused.cu", "brt_engine.cu"]
 HEADERS = ["brt_internal.cuh", "brt_kernels.cuh", "brt_agent.cuh"]
 
 NVCC_FLAGS = [

@@ -75,6 +75,58 @@ __device__ __forceinline__ uint32_t buildNeighborList(uint32_t self, f3 p, const
   return n;
 }
 
+// The same list as buildNeighborList<false>, walked as one flat loop over the
+// concatenated candidates of the 27 cells (same visit order).  Lanes of a
+// warp whose home cells differ then run the candidate loop in lockstep
+// instead of diverging on every cell's own trip count.
+__device__ __forceinline__ uint32_t scanNeighborsFlat(uint32_t self, f3 p, const FlockDev& fl,
+                                                      const uint32_t* __restrict__ cellStart,
+                                                      const uint32_t* __restrict__ cellEnd,
+                                                      const float4* __restrict__ posS, uint32_t* list,
+                                                      uint32_t ls) {
+  const int gx = gridCoord(p.x, fl.cell, fl.G), gy = gridCoord(p.y, fl.cell, fl.G), gz = gridCoord(p.z, fl.cell, fl.G);
+  const uint32_t M = fl.M;
+  const float thr = fl.r2thr;
+  uint32_t n = 0;
+  int c = -1;
+  uint32_t j = 0, stop = 0;
+  float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+  for (;;) {
+    if (j >= stop) {
+      bool found = false;
+      while (++c < 27) {
+        const int ox = c / 9 - 1, oy = (c / 3) % 3 - 1, oz = c % 3 - 1;
+        const int cx = wrapCoord(gx + ox, fl.G), cy = wrapCoord(gy + oy, fl.G), cz = wrapCoord(gz + oz, fl.G);
+        const uint32_t h = fl.cellBase + ((uint32_t)cz * fl.G + (uint32_t)cy) * fl.G + (uint32_t)cx;
+        const uint32_t start = __ldg(&cellStart[h]);
+        if (start == kEmpty) continue;
+        uint32_t end = __ldg(&cellEnd[h]);
+        if (end <= start) continue;
+        if (fl.maxPerCell && end - start > fl.maxPerCell) end = start + fl.maxPerCell;
+        j = start;
+        stop = end;
+        sx = imageShift(gx, ox, fl.G, fl.L);
+        sy = imageShift(gy, oy, fl.G, fl.L);
+        sz = imageShift(gz, oz, fl.G, fl.L);
+        found = true;
+        break;
+      }
+      if (!found) break;
+    }
+    if (j != self) {
+      const float4 q = __ldg(&posS[j]);
+      const float dx = (q.x + sx) - p.x, dy = (q.y + sy) - p.y, dz = (q.z + sz) - p.z;
+      const float d2 = dx * dx + dy * dy + dz * dz;
+      if (!(d2 > thr)) {
+        list[(n++) * ls] = j;
+        if (n == M) break;
+      }
+    }
+    ++j;
+  }
+  return n;
+}
+
 // Home-agent context for the steering stages.
 struct AgentCtx {
   f3 pos, fwd;

@@ -31,6 +31,18 @@ static float radiusThreshold(float r) {
   return x;
 }
 
+// Smallest float x >= 0 with sqrtf(x) >= r, so that sqrtf(d2) < r is exactly
+// d2 < x (0 when r <= 0: the test never holds).
+static float lowerRadiusThreshold(float r) {
+  if (!(r > 0.0f)) return 0.0f;
+  if (std::isinf(r)) return INFINITY;
+  float x = r * r;
+  if (std::isinf(x)) return INFINITY;
+  while (x > 0.0f && std::sqrt(std::nextafter(x, 0.0f)) >= r) x = std::nextafter(x, 0.0f);
+  while (std::sqrt(x) < r) x = std::nextafter(x, INFINITY);
+  return x;
+}
+
 static int validateParams(const brt_params& p, uint32_t& G) {
   if (p.disableSorting) { setLastError("disableSorting is not supported"); return BRT_ERR_CONFIG; }
   if (!(p.cellSize > 0.0f) || !(p.worldSize > 0.0f)) { setLastError("worldSize and cellSize must be positive"); return BRT_ERR_CONFIG; }
@@ -75,6 +87,14 @@ static FlockDev toDev(const brt_params& p, uint32_t G) {
   d.avgCtl = p.avgSimilarityController;
   d.numObstacles = p.numObstacles;
   d.obsW = p.obstacleAvoidanceWeight;
+  d.minT = lowerRadiusThreshold(p.commonSensingMinRadius);
+  d.sepT = radiusThreshold(p.separationParams[1]);
+  d.aliT = radiusThreshold(p.alignmentParams[1]);
+  d.cohT = radiusThreshold(p.cohesionParams[1]);
+  {
+    const float mc = std::max(p.separationParams[2], std::max(p.alignmentParams[2], p.cohesionParams[2]));
+    d.cosBound2 = (mc < -1.0f) ? mc * mc : 0.0f;
+  }
   return d;
 }
 
@@ -92,9 +112,11 @@ struct brt_engine {
   uint32_t* agentBase = nullptr;
   float4* obstacles = nullptr;
   bool anyKnn = false;
+  bool forceTwoPass = false;  // option "two_pass": run the list-first kernel even when not needed
+  int flockOccupancy = 1;     // option "flock_occupancy": register cap for 8 blocks per SM
   // state
   float4 *posA = nullptr, *fwdA = nullptr, *accA = nullptr, *posS = nullptr, *fwdS = nullptr, *accS = nullptr;
-  float *featA = nullptr, *featS = nullptr;
+  float *featA = nullptr, *featS = nullptr, *featNormS = nullptr;
   uint32_t *idA = nullptr, *idS = nullptr;
   float4* statsById = nullptr;
   float4* steer = nullptr;
@@ -154,7 +176,7 @@ void freeAll(brt_engine* e) {
     for (int k = 0; k < 5; ++k)
       if (e->ev[r][k]) cudaEventDestroy(e->ev[r][k]);
   void* ptrs[] = {e->flocks, e->agentBase, e->obstacles, e->posA, e->fwdA, e->accA, e->posS, e->fwdS, e->accS,
-                  e->featA, e->featS, e->idA, e->idS, e->statsById, e->steer, e->lists, e->pairs[0], e->pairs[1],
+                  e->featA, e->featS, e->featNormS, e->idA, e->idS, e->statsById, e->steer, e->lists, e->pairs[0], e->pairs[1],
                   e->cellStart, e->cellEnd, e->sortMem, e->errWord, e->stage4, e->stageF};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -225,6 +247,7 @@ int enqueueReorder(brt_engine* e) {
   R.pairs = e->pairs[e->finalPairs];
   R.posA = e->posA; R.fwdA = e->fwdA; R.accA = e->accA; R.featA = e->featA; R.idA = e->idA;
   R.posS = e->posS; R.fwdS = e->fwdS; R.accS = e->accS; R.featS = e->featS; R.idS = e->idS;
+  R.featNormS = e->featNormS;
   R.fs4 = e->Fs / 4;
   R.cellStart = e->cellStart; R.cellEnd = e->cellEnd;
   R.hist = e->ss.hist; R.histWords = e->plan.passes * e->plan.bins;
@@ -244,13 +267,19 @@ int enqueueStep(brt_engine* e, float dt, bool record) {
   FusedArgs F;
   std::memset(&F, 0, sizeof(F));
   F.posS = e->posS; F.fwdS = e->fwdS; F.accS = e->accS; F.featS = e->featS; F.idS = e->idS;
+  F.featNormS = e->featNormS;
   F.posA = e->posA; F.fwdA = e->fwdA; F.accA = e->accA; F.featA = e->featA; F.idA = e->idA;
   F.statsById = e->statsById;
   F.cellStart = e->cellStart; F.cellEnd = e->cellEnd;
   F.flocks = e->flocks; F.agentBase = e->agentBase; F.obstacles = e->obstacles;
   F.lists = record ? e->lists : nullptr; F.listStride = e->listStride;
   F.nflocks = e->nflocks; F.n = e->N; F.Mmax = e->Mmax; F.Fs = e->Fs; F.dt = dt;
-  BRT_CUDA_TRY(launchFused(F, e->anyKnn, e->stream));
+  // The single-pass kernel covers every flock unless one needs kNN
+  // replacement or clustering steering (both need the whole list first).
+  bool twoPass = e->anyKnn || e->forceTwoPass;
+  for (const FlockDev& d : e->flocksHost) twoPass = twoPass || (d.F > 0 && (d.clus != 0.0f || d.aclus != 0.0f));
+  if (twoPass) BRT_CUDA_TRY(launchFused(F, e->anyKnn, e->stream));
+  else BRT_CUDA_TRY(launchFlock(F, e->flockOccupancy, e->stream));
   if (timed) {
     if ((rc = stageMark(e, 4))) return rc;
     e->pending[e->ringPos] = true;
@@ -391,7 +420,12 @@ int brt_engine_create(const brt_params* flocks, uint32_t num_flocks, int device,
     e->anyKnn = e->anyKnn || d.useKnn;
     e->flocksHost.push_back(d);
   }
-  if (N >= (1ull << 30) || C >= (1ull << 30)) { delete e; setLastError("too many agents or cells"); return BRT_ERR_CAPACITY; }
+  // Neighbour-list entries hold a 26-bit sorted slot (brt_fused.cu).
+  if (N >= (1ull << 26) || C >= (1ull << 30)) {
+    delete e;
+    setLastError("too many agents (at most 2^26 - 1) or cells (at most 2^30 - 1) in one engine");
+    return BRT_ERR_CAPACITY;
+  }
   agentBase[num_flocks] = (uint32_t)N;
   e->N = (uint32_t)N;
   e->C = (uint32_t)C;
@@ -413,6 +447,7 @@ int brt_engine_create(const brt_params* flocks, uint32_t num_flocks, int device,
   chk(devAlloc(&e->posA, n)); chk(devAlloc(&e->fwdA, n)); chk(devAlloc(&e->accA, n));
   chk(devAlloc(&e->posS, n)); chk(devAlloc(&e->fwdS, n)); chk(devAlloc(&e->accS, n));
   chk(devAlloc(&e->featA, n * e->Fs)); chk(devAlloc(&e->featS, n * e->Fs));
+  if (e->Fs) chk(devAlloc(&e->featNormS, n));
   chk(devAlloc(&e->idA, n)); chk(devAlloc(&e->idS, n));
   chk(devAlloc(&e->statsById, n));
   chk(devAlloc(&e->steer, n));
@@ -504,6 +539,38 @@ int brt_engine_set_params(brt_engine* e, uint32_t flock, const brt_params* p) {
   if (!obs.empty())
     BRT_CUDA_TRY(cudaMemcpyAsync(e->obstacles + d.obsBase, obs.data(), sizeof(float4) * obs.size(), cudaMemcpyHostToDevice, e->stream));
   BRT_CUDA_TRY(cudaStreamSynchronize(e->stream));
+  for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second);
+  e->graphs.clear();
+  e->paramsVersion++;
+  return BRT_OK;
+}
+
+int brt_engine_set_option(brt_engine* e, const char* key, int64_t value) {
+  if (!e || !key) return BRT_ERR_ARG;
+  DeviceGuard guard(e->device);
+  const std::string k(key);
+  if (k == "two_pass") {
+    e->forceTwoPass = value != 0;
+  } else if (k == "flock_occupancy") {
+    e->flockOccupancy = value != 0 ? 1 : 0;
+  } else if (k == "sort_digit_bits") {
+    if (value < 4 || value > 9) { setLastError("sort_digit_bits must be in [4, 9]"); return BRT_ERR_ARG; }
+    BRT_CUDA_TRY(cudaStreamSynchronize(e->stream));
+    SortPlan plan = makeSortPlan(e->N, e->plan.bits, (uint32_t)value);
+    const size_t bytes = sortScratchBytes(plan, false);
+    void* mem = nullptr;
+    BRT_CUDA_TRY(cudaMalloc(&mem, bytes));
+    BRT_CUDA_TRY(cudaMemset(mem, 0, bytes));
+    if (e->sortMem) cudaFree(e->sortMem);
+    e->sortMem = mem;
+    e->plan = plan;
+    e->ss = carveSortScratch(plan, mem, false);
+    e->reordered = false;
+    e->listsValid = false;
+  } else {
+    setLastError("unknown option " + k);
+    return BRT_ERR_ARG;
+  }
   for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second);
   e->graphs.clear();
   e->paramsVersion++;
@@ -787,6 +854,7 @@ int brt_get_steer_force(brt_engine* e, float* steer4, int where) {
 namespace {
 int configureKernels(brt_engine* e) {
   BRT_CUDA_TRY(configureFusedKernels(e->Mmax));
+  BRT_CUDA_TRY(configureFlockKernels(e->Mmax));
   return BRT_OK;
 }
 }  // namespace

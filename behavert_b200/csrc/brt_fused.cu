@@ -1,0 +1,214 @@
+// brt_fused.cu -- the fused flocking kernel for flocks without kNN
+// replacement or clustering steering (those use fusedKernel, brt_kernels.cu).
+//
+// One thread per sorted slot.  Phase 1 scans the 27 neighbour cells in the
+// reference's visit order (Proximity3D_kernel.cu:108-115) into a shared-memory
+// list; phase 2 walks the list once, in list order, accumulating separation,
+// alignment, cohesion (OpenSteerWrapper_resources.cu:166-290) and the
+// feature-relaxation sums with the features held in registers and each
+// neighbour's feature norm precomputed by the reorder kernel.  (Folding the
+// sums into the scan itself makes every scan iteration pay for the warp's
+// accepting lanes, which measured slower.)
+//
+// inBoidNeighborhood (OpenSteerWrapper_resources.cu:67-92) is evaluated with
+// exact squared-distance thresholds (sqrtf is monotone and correctly rounded):
+//   dist < minR <=> d2 < minT,  dist > maxR <=> d2 > maxT.
+// When every cosMaxAngle is below -1 and |forward| is small enough, the angle
+// test can only reject a NaN cosine; that needs d2 == 0 (or d2 so small that
+// the normalised offset may lose its unit length), so those rare candidates,
+// and every candidate when the angle test matters, take the exact path.
+#include "brt_agent.cuh"
+#include "brt_kernels.cuh"
+
+namespace brt {
+
+// List entries carry the neighbour's image shift in their top bits:
+// 2 bits per axis (0: none, 1: -L, 2: +L) above a 26-bit sorted slot.
+constexpr uint32_t kSlotBits = 26;
+constexpr uint32_t kSlotMask = (1u << kSlotBits) - 1u;
+
+__device__ __forceinline__ uint32_t shiftCode(int g, int o, uint32_t G) {
+  return (o < 0 && g == 0) ? 1u : ((o > 0 && g == (int)G - 1) ? 2u : 0u);
+}
+__device__ __forceinline__ float shiftOf(uint32_t code, float L) {
+  return code == 1u ? -L : (code == 2u ? L : 0.0f);
+}
+
+template <int FP, int MINB>
+__global__ void __launch_bounds__(kFusedThreads, MINB) flockKernel(FusedArgs A) {
+  extern __shared__ uint32_t sList[];
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.n) return;
+  const uint32_t f = A.nflocks == 1 ? 0u : flockOfSlot(A.agentBase, A.nflocks, i);
+  const FlockDev& fl = A.flocks[f];
+  const float4 p4 = __ldg(&A.posS[i]);
+  const f3 p = xyz(p4);
+  const uint32_t G = fl.G;
+  const int gx = gridCoord(p.x, fl.cell, G), gy = gridCoord(p.y, fl.cell, G), gz = gridCoord(p.z, fl.cell, G);
+  const int hi = (int)G - 1;
+  const bool interior = gx > 0 && gx < hi && gy > 0 && gy < hi && gz > 0 && gz < hi;
+  const uint32_t M = fl.M;
+  uint32_t* list = sList + threadIdx.x;
+  const uint32_t ls = blockDim.x;
+
+  // Phase 1: the neighbour list in the reference's visit order.
+  (void)M;
+  const uint32_t n = scanNeighborsFlat(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls);
+  if (A.lists) {
+    uint32_t* out = A.lists + (size_t)i * A.listStride;
+    out[0] = n;
+    for (uint32_t k = 0; k < n; ++k) out[1 + k] = list[k * ls] & kSlotMask;
+  }
+
+  // Phase 2: steering and feature sums over the list, in list order.
+  const float4 w4 = __ldg(&A.fwdS[i]);
+  const float4 a4 = __ldg(&A.accS[i]);
+  const f3 fwd = xyz(w4);
+  const bool cosFree = dot3(fwd, fwd) * 1.002f < fl.cosBound2;
+  const bool sepOn = fl.sep[0] != 0.0f, aliOn = fl.ali[0] != 0.0f, cohOn = fl.coh[0] != 0.0f;
+  const uint32_t F = fl.F;
+  const bool relaxOn = FP > 0 && fl.relax != 0.0f && F > 0;
+  const uint32_t fs4 = A.Fs / 4;
+  float fi[FP > 0 ? FP : 1];
+  float facc[FP > 0 ? FP : 1];
+  float n1 = 0.0f, sumS = 0.0f;
+  if (FP > 0) {
+    const float4* src = reinterpret_cast<const float4*>(A.featS) + (size_t)i * fs4;
+#pragma unroll
+    for (int q = 0; q < FP / 4; ++q) {
+      const float4 v = (uint32_t)q < fs4 ? __ldg(&src[q]) : make_float4(0.f, 0.f, 0.f, 0.f);
+      fi[4 * q + 0] = v.x; fi[4 * q + 1] = v.y; fi[4 * q + 2] = v.z; fi[4 * q + 3] = v.w;
+    }
+#pragma unroll
+    for (int k = 0; k < FP; ++k) facc[k] = 0.0f;
+    n1 = __ldg(&A.featNormS[i]);
+  }
+  f3 sSep = mk3(0.f, 0.f, 0.f), sAli = mk3(0.f, 0.f, 0.f), sCoh = mk3(0.f, 0.f, 0.f);
+  uint32_t cSep = 0, cAli = 0, cCoh = 0;
+  const AgentCtx a = makeCtx(p4, w4, fl);
+  (void)interior;
+  for (uint32_t k = 0; k < n; ++k) {
+    const uint32_t e = list[k * ls];
+    const uint32_t j = e & kSlotMask;
+    const f3 img = neighborImage(a, __ldg(&A.posS[j]), fl);
+    const float qx = img.x, qy = img.y, qz = img.z;
+    const float dx = qx - p.x, dy = qy - p.y, dz = qz - p.z;
+    const float d2 = dx * dx + dy * dy + dz * dz;
+    bool inS, inA, inC;
+    if (cosFree && d2 >= 1e-30f) {
+      const bool lo = d2 < fl.minT;
+      inS = lo || !(d2 > fl.sepT);
+      inA = lo || !(d2 > fl.aliT);
+      inC = lo || !(d2 > fl.cohT);
+    } else {
+      const float dist = sqrtf(d2);
+      const f3 nrm = mul3(mk3(dx, dy, dz), 1.0f / dist);
+      const float cosA = dot3(fwd, nrm);
+      inS = inBoid(dist, cosA, fl.minR, fl.sep[1], fl.sep[2]);
+      inA = inBoid(dist, cosA, fl.minR, fl.ali[1], fl.ali[2]);
+      inC = inBoid(dist, cosA, fl.minR, fl.coh[1], fl.coh[2]);
+    }
+    if (sepOn && inS) {
+      const float nd2 = -d2;
+      sSep = add3(sSep, mk3(dx / nd2, dy / nd2, dz / nd2));
+      ++cSep;
+    }
+    if (aliOn && inA) {
+      sAli = add3(sAli, xyz(__ldg(&A.fwdS[j])));
+      ++cAli;
+    }
+    if (cohOn && inC) {
+      sCoh = add3(sCoh, mk3(qx, qy, qz));
+      ++cCoh;
+    }
+    if (relaxOn) {
+      float fj[FP > 0 ? FP : 1];
+      const float4* src = reinterpret_cast<const float4*>(A.featS) + (size_t)j * fs4;
+#pragma unroll
+      for (int qq = 0; qq < FP / 4; ++qq) {
+        const float4 v = (uint32_t)qq < fs4 ? __ldg(&src[qq]) : make_float4(0.f, 0.f, 0.f, 0.f);
+        fj[4 * qq + 0] = v.x; fj[4 * qq + 1] = v.y; fj[4 * qq + 2] = v.z; fj[4 * qq + 3] = v.w;
+      }
+      float dot = 0.0f;
+#pragma unroll
+      for (int kk = 0; kk < FP; ++kk) dot += fi[kk] * fj[kk];
+      const float s = (dot / (n1 * __ldg(&A.featNormS[j])) + 1.0f) / 2.0f;
+      sumS += s;
+#pragma unroll
+      for (int kk = 0; kk < FP; ++kk) facc[kk] += s * fj[kk];
+    }
+  }
+  f3 steer = mk3(0.f, 0.f, 0.f);
+  if (sepOn) {
+    if (cSep > 0) sSep = normalize3(div3(sSep, (float)cSep));
+    steer = add3(mul3(sSep, fl.sep[0]), steer);
+  }
+  if (aliOn) {
+    if (cAli > 0) sAli = normalize3(sub3(div3(sAli, (float)cAli), fwd));
+    steer = add3(mul3(sAli, fl.ali[0]), steer);
+  }
+  if (cohOn) {
+    if (cCoh > 0) sCoh = normalize3(sub3(div3(sCoh, (float)cCoh), p));
+    steer = add3(mul3(sCoh, fl.coh[0]), steer);
+  }
+  if (fl.numObstacles && fl.obsW != 0.0f) steer = obstacleSteer(a, fl, A.obstacles, steer);
+  if (FP > 0) {
+    if (relaxOn && n > 0 && sumS > 0.0f) {
+#pragma unroll
+      for (int k = 0; k < FP; ++k)
+        if ((uint32_t)k < F) {
+          const float mean = facc[k] / sumS;
+          fi[k] = fi[k] + fl.relax * (mean - fi[k]);
+        }
+    }
+    float4* dst = reinterpret_cast<float4*>(A.featA) + (size_t)i * fs4;
+#pragma unroll
+    for (int q = 0; q < FP / 4; ++q)
+      if ((uint32_t)q < fs4) dst[q] = make_float4(fi[4 * q], fi[4 * q + 1], fi[4 * q + 2], fi[4 * q + 3]);
+  }
+  const Integrated r = integrate(a, a4, steer, A.dt, fl);
+  A.posA[i] = r.pos;
+  A.fwdA[i] = r.fwd;
+  A.accA[i] = r.acc;
+  A.idA[i] = __ldg(&A.idS[i]);
+}
+
+namespace {
+template <int FP>
+cudaError_t launchFlockFP(const FusedArgs& A, uint32_t blocks, size_t smem, int occupancy, cudaStream_t st) {
+  if (occupancy) flockKernel<FP, 8><<<blocks, kFusedThreads, smem, st>>>(A);
+  else flockKernel<FP, 1><<<blocks, kFusedThreads, smem, st>>>(A);
+  return cudaGetLastError();
+}
+template <int FP>
+cudaError_t configureFlockFP(int smem) {
+  cudaError_t e = cudaFuncSetAttribute(flockKernel<FP, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(flockKernel<FP, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+}
+}  // namespace
+
+// occupancy != 0 caps registers so that 8 blocks of 128 threads fit per SM.
+cudaError_t launchFlock(const FusedArgs& A, int occupancy, cudaStream_t st) {
+  if (A.n == 0) return cudaSuccess;
+  const uint32_t blocks = (A.n + kFusedThreads - 1) / kFusedThreads;
+  const uint32_t fp = A.Fs;
+  const size_t smem = (size_t)kFusedThreads * A.Mmax * 4;
+  if (fp == 0) return launchFlockFP<0>(A, blocks, smem, occupancy, st);
+  if (fp <= 4) return launchFlockFP<4>(A, blocks, smem, occupancy, st);
+  if (fp <= 8) return launchFlockFP<8>(A, blocks, smem, occupancy, st);
+  if (fp <= 16) return launchFlockFP<16>(A, blocks, smem, occupancy, st);
+  return launchFlockFP<32>(A, blocks, smem, occupancy, st);
+}
+
+cudaError_t configureFlockKernels(uint32_t Mmax) {
+  const int smem = (int)((size_t)kFusedThreads * Mmax * 4);
+  cudaError_t e = cudaSuccess;
+  if ((e = configureFlockFP<0>(smem))) return e;
+  if ((e = configureFlockFP<4>(smem))) return e;
+  if ((e = configureFlockFP<8>(smem))) return e;
+  if ((e = configureFlockFP<16>(smem))) return e;
+  return configureFlockFP<32>(smem);
+}
+
+}  // namespace brt

@@ -49,6 +49,13 @@ struct FlockDev {
   float obsW;
   uint32_t obsBase;     // first entry in the engine-wide obstacle table
   uint32_t pad;
+  // inBoidNeighborhood as exact squared-distance tests:
+  //   dist < minR  <=>  d2 < minT,   dist > maxR_b  <=>  d2 > maxT_b
+  float minT, sepT, aliT, cohT;
+  // Square of -max(cosMaxAngle) when every cosMaxAngle < -1, else 0: for an
+  // agent with |forward|^2 * 1.002 below it, every finite cosine passes the
+  // angle test, which then only rejects NaN (a zero offset).
+  float cosBound2;
 };
 
 // ---------------------------------------------------------------------------

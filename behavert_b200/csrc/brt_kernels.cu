@@ -73,9 +73,21 @@ __global__ void __launch_bounds__(256) reorderKernel(ReorderArgs A) {
     A.accS[i] = __ldg(&A.accA[ps]);
     A.idS[i] = __ldg(&A.idA[ps]);
     if (A.fs4) {
+      // The feature norm sqrtf(sum f^2) (computeSimilarity's norma,
+      // BehaviorClustering_resources.cu:164-175) is the same for every pair
+      // an agent takes part in: compute it once here, in the same order.
       const float4* src = reinterpret_cast<const float4*>(A.featA) + (size_t)ps * A.fs4;
       float4* dst = reinterpret_cast<float4*>(A.featS) + (size_t)i * A.fs4;
-      for (uint32_t q = 0; q < A.fs4; ++q) dst[q] = __ldg(&src[q]);
+      float nn = 0.0f;
+      for (uint32_t q = 0; q < A.fs4; ++q) {
+        const float4 v = __ldg(&src[q]);
+        dst[q] = v;
+        nn += v.x * v.x;
+        nn += v.y * v.y;
+        nn += v.z * v.z;
+        nn += v.w * v.w;
+      }
+      if (A.featNormS) A.featNormS[i] = sqrtf(nn);
     }
     if (key != prev) A.cellStart[key] = i;
     if (key != next) A.cellEnd[key] = i + 1;

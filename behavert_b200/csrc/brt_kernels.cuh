@@ -30,6 +30,7 @@ struct ReorderArgs {
   const float4* posA; const float4* fwdA; const float4* accA;
   const float* featA; const uint32_t* idA;
   float4* posS; float4* fwdS; float4* accS; float* featS; uint32_t* idS;
+  float* featNormS;            // sqrtf(sum f^2) per sorted slot (optional)
   uint32_t fs4;                // feature float4s per agent
   uint32_t* cellStart; uint32_t* cellEnd;
   uint32_t* hist; uint32_t histWords;
@@ -40,6 +41,7 @@ struct ReorderArgs {
 struct FusedArgs {
   const float4* posS; const float4* fwdS; const float4* accS;
   const float* featS; const uint32_t* idS;
+  const float* featNormS;
   float4* posA; float4* fwdA; float4* accA; float* featA; uint32_t* idA;
   float4* statsById;
   const uint32_t* cellStart; const uint32_t* cellEnd;
@@ -68,6 +70,7 @@ struct StageArgs {
 cudaError_t launchHash(const HashArgs& A, uint32_t maxBlocks, cudaStream_t st);
 cudaError_t launchReorder(const ReorderArgs& A, cudaStream_t st);
 cudaError_t launchFused(const FusedArgs& A, bool knn, cudaStream_t st);
+cudaError_t launchFlock(const FusedArgs& A, int occupancy, cudaStream_t st);
 cudaError_t launchLists(const StageArgs& A, bool knn, cudaStream_t st);
 cudaError_t launchSteerStage(const StageArgs& A, int which, cudaStream_t st);
 cudaError_t launchIntegrateStage(const StageArgs& A, float dt, cudaStream_t st);
@@ -76,6 +79,7 @@ cudaError_t launchScatterFeatToId(const float* src, uint32_t Fs, const uint32_t*
 cudaError_t launchLoadFeat(const float* src, uint32_t F, float* dst, uint32_t Fs, uint32_t n, cudaStream_t st);
 cudaError_t launchGatherFromId(const float4* src, const uint32_t* id, float4* dst, uint32_t n, bool forceW1, cudaStream_t st);
 cudaError_t configureFusedKernels(uint32_t Mmax);
+cudaError_t configureFlockKernels(uint32_t Mmax);
 cudaError_t launchGatherFeatFromId(const float* src, uint32_t F, const uint32_t* id, float* dst, uint32_t Fs, uint32_t n, cudaStream_t st);
 cudaError_t launchHashPairsOut(const uint2* pairs, const uint32_t* idS, uint32_t* keys, uint32_t* ids, uint32_t n, cudaStream_t st);
 

@@ -63,6 +63,9 @@ class Engine:
         check(lib().brt_engine_set_params(self._h, flock, C.byref(p)), "brt_engine_set_params")
         self.flocks[flock] = p.copy()
 
+    def set_option(self, key: str, value: int) -> None:
+        check(lib().brt_engine_set_option(self._h, key.encode(), int(value)), "brt_engine_set_option")
+
     def sync(self) -> None:
         check(lib().brt_sync(self._h), "brt_sync")
 

@@ -142,6 +142,13 @@ int brt_engine_num_cells(const brt_engine* e, uint32_t* num_cells);
 /* Replace the parameters of one flock; geometry fields (numBodies,
    worldSize, cellSize, maxNeighbors, featuresCount) must not change. */
 int brt_engine_set_params(brt_engine* e, uint32_t flock, const brt_params* p);
+/* Tuning options (the reference's DeviceInterface BlockDim / commonBlockDim
+   knobs, Core/src/CommonResources.cpp:78-82, generalised):
+     "sort_digit_bits"  4..9  radix digit width of the onesweep passes (default 8)
+     "two_pass"         0/1   build each neighbour list before steering even
+                              when the single-pass kernel applies (default 0)
+   Unknown keys return BRT_ERR_ARG. */
+int brt_engine_set_option(brt_engine* e, const char* key, int64_t value);
 /* The engine's CUDA stream (a cudaStream_t), for callers that enqueue their
    own work around the engine's. */
 int brt_engine_stream(brt_engine* e, void** stream);

@@ -169,6 +169,31 @@ def test_stagewise_equals_fused():
             assert np.array_equal(x, y)
 
 
+def test_single_pass_equals_two_pass():
+    """The single-pass fused kernel and the list-first kernel agree bit for bit."""
+    w = workloads.large(n=40000)
+    with make_engine(w) as a, make_engine(w) as b:
+        b.set_option("two_pass", 1)
+        for eng in (a, b):
+            eng.record_lists(True)
+            eng.step(0.1, 3)
+        assert np.array_equal(a.getNeighborLists(), b.getNeighborLists())
+        for x, y in zip(a.get_state(), b.get_state()):
+            assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("bits", [5, 7, 9])
+def test_sort_digit_width_option(bits):
+    w = workloads.large(n=30000)
+    with make_engine(w) as a, make_engine(w) as b:
+        b.set_option("sort_digit_bits", bits)
+        a.step(0.1, 2)
+        b.step(0.1, 2)
+        for x, y in zip(a.get_state(), b.get_state()):
+            assert np.array_equal(x, y)
+        assert np.array_equal(a.getHash()[1], b.getHash()[1])
+
+
 def test_graph_equals_single_steps():
     w = workloads.plain(n=8192, L=80.0)
     with make_engine(w) as a, make_engine(w) as b:
