@@ -127,6 +127,88 @@ __device__ __forceinline__ uint32_t scanNeighborsFlat(uint32_t self, f3 p, const
   return n;
 }
 
+// The same list as buildNeighborList<false> (same visit order, same test),
+// written for memory-level parallelism: for each (x, y) row the three z
+// cells' ranges are fetched together, and candidate positions are loaded
+// UNROLL at a time before they are tested in order.
+//
+// With CULL, a neighbour cell is skipped when its box is provably farther
+// than the search radius: the distance from p to the shared face is exact
+// (p - g*cell and (g+1)*cell - p are Sterbenz-exact for g >= 1, within an ulp
+// of 4 otherwise) and any candidate of that cell lies beyond the face up to
+// the rounding of its own coordinate, so a margin of 0.01 on d^2 cannot drop a
+// candidate that would pass the exact test.  Skipping such a cell therefore
+// leaves the list unchanged.
+template <int UNROLL, bool CULL>
+__device__ __forceinline__ uint32_t scanNeighborsPipelined(uint32_t self, f3 p, const FlockDev& fl,
+                                                           const uint32_t* __restrict__ cellStart,
+                                                           const uint32_t* __restrict__ cellEnd,
+                                                           const float4* __restrict__ posS, uint32_t* list,
+                                                           uint32_t ls) {
+  const int gx = gridCoord(p.x, fl.cell, fl.G), gy = gridCoord(p.y, fl.cell, fl.G), gz = gridCoord(p.z, fl.cell, fl.G);
+  const uint32_t M = fl.M;
+  const float thr = fl.r2thr;
+  // squared distances to the lower / upper faces of the home cell
+  float lo2[3], hi2[3];
+  if (CULL) {
+    const float cl = fl.cell;
+    const float lx = p.x - (float)gx * cl, ly = p.y - (float)gy * cl, lz = p.z - (float)gz * cl;
+    const float ux = (float)(gx + 1) * cl - p.x, uy = (float)(gy + 1) * cl - p.y, uz = (float)(gz + 1) * cl - p.z;
+    lo2[0] = lx * lx; lo2[1] = ly * ly; lo2[2] = lz * lz;
+    hi2[0] = ux * ux; hi2[1] = uy * uy; hi2[2] = uz * uz;
+  }
+  // The candidate-coordinate rounding grows with the world size (ulp of L).
+  const float cullThr = thr + 0.01f + 1e-6f * fl.cell * fl.L;
+  uint32_t n = 0;
+  for (int ox = -1; ox <= 1; ++ox) {
+    const int cx = wrapCoord(gx + ox, fl.G);
+    const float sx = imageShift(gx, ox, fl.G, fl.L);
+    const float bx = CULL ? (ox < 0 ? lo2[0] : (ox > 0 ? hi2[0] : 0.0f)) : 0.0f;
+    for (int oy = -1; oy <= 1; ++oy) {
+      const int cy = wrapCoord(gy + oy, fl.G);
+      const float sy = imageShift(gy, oy, fl.G, fl.L);
+      const float bxy = CULL ? bx + (oy < 0 ? lo2[1] : (oy > 0 ? hi2[1] : 0.0f)) : 0.0f;
+      if (CULL && bxy > cullThr) continue;
+      uint32_t st[3], en[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const int cz = wrapCoord(gz + k - 1, fl.G);
+        const uint32_t h = fl.cellBase + ((uint32_t)cz * fl.G + (uint32_t)cy) * fl.G + (uint32_t)cx;
+        st[k] = __ldg(&cellStart[h]);
+        en[k] = __ldg(&cellEnd[h]);
+      }
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const uint32_t start = st[k];
+        uint32_t stop = en[k];
+        if (start == kEmpty || stop <= start) continue;
+        if (CULL && bxy + (k == 0 ? lo2[2] : (k == 2 ? hi2[2] : 0.0f)) > cullThr) continue;
+        if (fl.maxPerCell && stop - start > fl.maxPerCell) stop = start + fl.maxPerCell;
+        const float sz = imageShift(gz, k - 1, fl.G, fl.L);
+        for (uint32_t j = start; j < stop; j += UNROLL) {
+          float4 q[UNROLL];
+#pragma unroll
+          for (int u = 0; u < UNROLL; ++u)
+            q[u] = (j + u < stop) ? __ldg(&posS[j + u]) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+          for (int u = 0; u < UNROLL; ++u) {
+            const uint32_t jj = j + u;
+            if (jj < stop && jj != self) {
+              const float dx = (q[u].x + sx) - p.x, dy = (q[u].y + sy) - p.y, dz = (q[u].z + sz) - p.z;
+              const float d2 = dx * dx + dy * dy + dz * dz;
+              if (!(d2 > thr)) {
+                list[(n++) * ls] = jj;
+                if (n == M) return n;
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+  return n;
+}
+
 // Home-agent context for the steering stages.
 struct AgentCtx {
   f3 pos, fwd;

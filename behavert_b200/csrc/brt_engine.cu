@@ -113,7 +113,8 @@ struct brt_engine {
   float4* obstacles = nullptr;
   bool anyKnn = false;
   bool forceTwoPass = false;  // option "two_pass": run the list-first kernel even when not needed
-  int flockOccupancy = 1;     // option "flock_occupancy": register cap for 8 blocks per SM
+  int phase2Variant = 0;      // option "phase2_variant": list walk one or two neighbours at a time
+  int scanVariant = 0;        // option "scan_variant": neighbour-scan loop shape
   // state
   float4 *posA = nullptr, *fwdA = nullptr, *accA = nullptr, *posS = nullptr, *fwdS = nullptr, *accS = nullptr;
   float *featA = nullptr, *featS = nullptr, *featNormS = nullptr;
@@ -274,12 +275,13 @@ int enqueueStep(brt_engine* e, float dt, bool record) {
   F.flocks = e->flocks; F.agentBase = e->agentBase; F.obstacles = e->obstacles;
   F.lists = record ? e->lists : nullptr; F.listStride = e->listStride;
   F.nflocks = e->nflocks; F.n = e->N; F.Mmax = e->Mmax; F.Fs = e->Fs; F.dt = dt;
+  F.scanVariant = e->scanVariant;
   // The single-pass kernel covers every flock unless one needs kNN
   // replacement or clustering steering (both need the whole list first).
   bool twoPass = e->anyKnn || e->forceTwoPass;
   for (const FlockDev& d : e->flocksHost) twoPass = twoPass || (d.F > 0 && (d.clus != 0.0f || d.aclus != 0.0f));
   if (twoPass) BRT_CUDA_TRY(launchFused(F, e->anyKnn, e->stream));
-  else BRT_CUDA_TRY(launchFlock(F, e->flockOccupancy, e->stream));
+  else BRT_CUDA_TRY(launchFlock(F, e->phase2Variant, e->stream));
   if (timed) {
     if ((rc = stageMark(e, 4))) return rc;
     e->pending[e->ringPos] = true;
@@ -551,8 +553,11 @@ int brt_engine_set_option(brt_engine* e, const char* key, int64_t value) {
   const std::string k(key);
   if (k == "two_pass") {
     e->forceTwoPass = value != 0;
-  } else if (k == "flock_occupancy") {
-    e->flockOccupancy = value != 0 ? 1 : 0;
+  } else if (k == "phase2_variant") {
+    e->phase2Variant = value != 0 ? 1 : 0;
+  } else if (k == "scan_variant") {
+    if (value < 0 || value > 3) { setLastError("scan_variant must be in [0, 3]"); return BRT_ERR_ARG; }
+    e->scanVariant = (int)value;
   } else if (k == "sort_digit_bits") {
     if (value < 4 || value > 9) { setLastError("sort_digit_bits must be in [4, 9]"); return BRT_ERR_ARG; }
     BRT_CUDA_TRY(cudaStreamSynchronize(e->stream));

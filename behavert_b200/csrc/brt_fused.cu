@@ -34,8 +34,8 @@ __device__ __forceinline__ float shiftOf(uint32_t code, float L) {
   return code == 1u ? -L : (code == 2u ? L : 0.0f);
 }
 
-template <int FP, int MINB>
-__global__ void __launch_bounds__(kFusedThreads, MINB) flockKernel(FusedArgs A) {
+template <int FP, int P2>
+__global__ void __launch_bounds__(kFusedThreads, 8) flockKernel(FusedArgs A) {
   extern __shared__ uint32_t sList[];
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.n) return;
@@ -53,7 +53,11 @@ __global__ void __launch_bounds__(kFusedThreads, MINB) flockKernel(FusedArgs A) 
 
   // Phase 1: the neighbour list in the reference's visit order.
   (void)M;
-  const uint32_t n = scanNeighborsFlat(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls);
+  const uint32_t n =
+      A.scanVariant == 0 ? scanNeighborsPipelined<4, true>(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls)
+    : A.scanVariant == 1 ? scanNeighborsPipelined<2, true>(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls)
+    : A.scanVariant == 2 ? scanNeighborsPipelined<4, false>(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls)
+                         : scanNeighborsFlat(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls);
   if (A.lists) {
     uint32_t* out = A.lists + (size_t)i * A.listStride;
     out[0] = n;
@@ -87,10 +91,10 @@ __global__ void __launch_bounds__(kFusedThreads, MINB) flockKernel(FusedArgs A) 
   uint32_t cSep = 0, cAli = 0, cCoh = 0;
   const AgentCtx a = makeCtx(p4, w4, fl);
   (void)interior;
-  for (uint32_t k = 0; k < n; ++k) {
-    const uint32_t e = list[k * ls];
-    const uint32_t j = e & kSlotMask;
-    const f3 img = neighborImage(a, __ldg(&A.posS[j]), fl);
+  // One listed neighbour: its image position, forward and features are
+  // loaded by the caller so that several neighbours' loads can be in flight.
+  auto visit = [&](const float4 q4, const float4 wj, const float* fj, float n2) {
+    const f3 img = neighborImage(a, q4, fl);
     const float qx = img.x, qy = img.y, qz = img.z;
     const float dx = qx - p.x, dy = qy - p.y, dz = qz - p.z;
     const float d2 = dx * dx + dy * dy + dz * dz;
@@ -114,7 +118,7 @@ __global__ void __launch_bounds__(kFusedThreads, MINB) flockKernel(FusedArgs A) 
       ++cSep;
     }
     if (aliOn && inA) {
-      sAli = add3(sAli, xyz(__ldg(&A.fwdS[j])));
+      sAli = add3(sAli, xyz(wj));
       ++cAli;
     }
     if (cohOn && inC) {
@@ -122,20 +126,50 @@ __global__ void __launch_bounds__(kFusedThreads, MINB) flockKernel(FusedArgs A) 
       ++cCoh;
     }
     if (relaxOn) {
-      float fj[FP > 0 ? FP : 1];
+      // computeSimilarity's dot product, then acc += s * f_j, in the
+      // reference's sequential order.
+      float dot = 0.0f;
+#pragma unroll
+      for (int kk = 0; kk < FP; ++kk) dot += fi[kk] * fj[kk];
+      const float s = (dot / (n1 * n2) + 1.0f) / 2.0f;
+      sumS += s;
+#pragma unroll
+      for (int kk = 0; kk < FP; ++kk) facc[kk] += s * fj[kk];
+    }
+  };
+  auto loadFeat = [&](uint32_t j, float* fj, float& n2) {
+    if (relaxOn) {
       const float4* src = reinterpret_cast<const float4*>(A.featS) + (size_t)j * fs4;
 #pragma unroll
       for (int qq = 0; qq < FP / 4; ++qq) {
         const float4 v = (uint32_t)qq < fs4 ? __ldg(&src[qq]) : make_float4(0.f, 0.f, 0.f, 0.f);
         fj[4 * qq + 0] = v.x; fj[4 * qq + 1] = v.y; fj[4 * qq + 2] = v.z; fj[4 * qq + 3] = v.w;
       }
-      float dot = 0.0f;
-#pragma unroll
-      for (int kk = 0; kk < FP; ++kk) dot += fi[kk] * fj[kk];
-      const float s = (dot / (n1 * __ldg(&A.featNormS[j])) + 1.0f) / 2.0f;
-      sumS += s;
-#pragma unroll
-      for (int kk = 0; kk < FP; ++kk) facc[kk] += s * fj[kk];
+      n2 = __ldg(&A.featNormS[j]);
+    }
+  };
+  const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (P2 == 0) {
+    for (uint32_t k = 0; k < n; ++k) {
+      const uint32_t j = list[k * ls] & kSlotMask;
+      float fj[FP > 0 ? FP : 1];
+      float n2 = 0.0f;
+      loadFeat(j, fj, n2);
+      visit(__ldg(&A.posS[j]), aliOn ? __ldg(&A.fwdS[j]) : zero4, fj, n2);
+    }
+  } else {
+    for (uint32_t k = 0; k < n; k += 2) {
+      const bool two = k + 1 < n;
+      const uint32_t j0 = list[k * ls] & kSlotMask;
+      const uint32_t j1 = two ? (list[(k + 1) * ls] & kSlotMask) : j0;
+      const float4 q0 = __ldg(&A.posS[j0]), q1 = __ldg(&A.posS[j1]);
+      const float4 w0 = aliOn ? __ldg(&A.fwdS[j0]) : zero4, w1 = aliOn ? __ldg(&A.fwdS[j1]) : zero4;
+      float f0[FP > 0 ? FP : 1], f1[FP > 0 ? FP : 1];
+      float n20 = 0.0f, n21 = 0.0f;
+      loadFeat(j0, f0, n20);
+      loadFeat(j1, f1, n21);
+      visit(q0, w0, f0, n20);
+      if (two) visit(q1, w1, f1, n21);
     }
   }
   f3 steer = mk3(0.f, 0.f, 0.f);
@@ -175,30 +209,31 @@ __global__ void __launch_bounds__(kFusedThreads, MINB) flockKernel(FusedArgs A) 
 
 namespace {
 template <int FP>
-cudaError_t launchFlockFP(const FusedArgs& A, uint32_t blocks, size_t smem, int occupancy, cudaStream_t st) {
-  if (occupancy) flockKernel<FP, 8><<<blocks, kFusedThreads, smem, st>>>(A);
-  else flockKernel<FP, 1><<<blocks, kFusedThreads, smem, st>>>(A);
+cudaError_t launchFlockFP(const FusedArgs& A, uint32_t blocks, size_t smem, int phase2, cudaStream_t st) {
+  if (phase2) flockKernel<FP, 1><<<blocks, kFusedThreads, smem, st>>>(A);
+  else flockKernel<FP, 0><<<blocks, kFusedThreads, smem, st>>>(A);
   return cudaGetLastError();
 }
 template <int FP>
 cudaError_t configureFlockFP(int smem) {
-  cudaError_t e = cudaFuncSetAttribute(flockKernel<FP, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaError_t e = cudaFuncSetAttribute(flockKernel<FP, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(flockKernel<FP, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
 }  // namespace
 
-// occupancy != 0 caps registers so that 8 blocks of 128 threads fit per SM.
-cudaError_t launchFlock(const FusedArgs& A, int occupancy, cudaStream_t st) {
+// phase2 != 0 walks the list two neighbours at a time with their loads issued
+// together.
+cudaError_t launchFlock(const FusedArgs& A, int phase2, cudaStream_t st) {
   if (A.n == 0) return cudaSuccess;
   const uint32_t blocks = (A.n + kFusedThreads - 1) / kFusedThreads;
   const uint32_t fp = A.Fs;
   const size_t smem = (size_t)kFusedThreads * A.Mmax * 4;
-  if (fp == 0) return launchFlockFP<0>(A, blocks, smem, occupancy, st);
-  if (fp <= 4) return launchFlockFP<4>(A, blocks, smem, occupancy, st);
-  if (fp <= 8) return launchFlockFP<8>(A, blocks, smem, occupancy, st);
-  if (fp <= 16) return launchFlockFP<16>(A, blocks, smem, occupancy, st);
-  return launchFlockFP<32>(A, blocks, smem, occupancy, st);
+  if (fp == 0) return launchFlockFP<0>(A, blocks, smem, phase2, st);
+  if (fp <= 4) return launchFlockFP<4>(A, blocks, smem, phase2, st);
+  if (fp <= 8) return launchFlockFP<8>(A, blocks, smem, phase2, st);
+  if (fp <= 16) return launchFlockFP<16>(A, blocks, smem, phase2, st);
+  return launchFlockFP<32>(A, blocks, smem, phase2, st);
 }
 
 cudaError_t configureFlockKernels(uint32_t Mmax) {

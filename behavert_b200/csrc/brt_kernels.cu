@@ -169,7 +169,9 @@ __global__ void __launch_bounds__(128) listsKernel(StageArgs A) {
   const FlockDev& fl = A.flocks[f];
   uint32_t* out = A.lists + (size_t)i * A.listStride;
   float distL[KNN ? BRT_MAX_NEIGHBORS : 1];
-  const uint32_t n = buildNeighborList<KNN>(i, xyz(__ldg(&A.posS[i])), fl, A.cellStart, A.cellEnd, A.posS, out + 1, 1, distL);
+  const f3 p = xyz(__ldg(&A.posS[i]));
+  const uint32_t n = KNN ? buildNeighborList<KNN>(i, p, fl, A.cellStart, A.cellEnd, A.posS, out + 1, 1, distL)
+                         : scanNeighborsPipelined<4, true>(i, p, fl, A.cellStart, A.cellEnd, A.posS, out + 1, 1);
   out[0] = n;
 }
 

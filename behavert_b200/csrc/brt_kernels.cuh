@@ -51,6 +51,7 @@ struct FusedArgs {
   uint32_t listStride;
   uint32_t nflocks, n, Mmax, Fs;
   float dt;
+  int scanVariant;             // 0: pipelined x4 + cell culling, 1: x2 + culling, 2: x4, 3: flat loop
 };
 
 struct StageArgs {
@@ -70,7 +71,7 @@ struct StageArgs {
 cudaError_t launchHash(const HashArgs& A, uint32_t maxBlocks, cudaStream_t st);
 cudaError_t launchReorder(const ReorderArgs& A, cudaStream_t st);
 cudaError_t launchFused(const FusedArgs& A, bool knn, cudaStream_t st);
-cudaError_t launchFlock(const FusedArgs& A, int occupancy, cudaStream_t st);
+cudaError_t launchFlock(const FusedArgs& A, int phase2, cudaStream_t st);
 cudaError_t launchLists(const StageArgs& A, bool knn, cudaStream_t st);
 cudaError_t launchSteerStage(const StageArgs& A, int which, cudaStream_t st);
 cudaError_t launchIntegrateStage(const StageArgs& A, float dt, cudaStream_t st);

@@ -190,6 +190,62 @@ def cpu_baseline_leg(w, eng_state_before, gpu_state_after, budget_s=12.0):
     return base, acc_err
 
 
+def batched_leg(device: int, steps: int = 100, loop_steps: int = 3):
+    """Config 2: 1,024 flocks of log-uniform sizes in one engine, the 100-step
+    loop as one CUDA graph, against the same flocks stepped one engine per
+    flock (plain per-step launches, looped over the flocks)."""
+    import torch
+    from behavert_b200 import Engine, workloads
+    w = workloads.batched()
+    n = w.num_agents
+    dt = w.dt
+    eng = Engine(w.params, device=device)
+    eng.set_state(w.pos, w.fwd, w.acc)
+    stream = torch.cuda.ExternalStream(eng.stream_handle())
+    eng.step(dt, 3)
+    eng.step_prepare(dt, steps)
+    eng.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    eng.step(dt, steps)
+    e1.record(stream)
+    e1.synchronize()
+    t_batched = e0.elapsed_time(e1) / 1e3
+    eng.sync()
+    eng.close()
+    # looped per-flock launches
+    engines = []
+    off = 0
+    for p in w.params:
+        e = Engine([p], device=device)
+        k = int(p.numBodies)
+        e.set_state(np.ascontiguousarray(w.pos[off:off + k]), np.ascontiguousarray(w.fwd[off:off + k]),
+                    np.ascontiguousarray(w.acc[off:off + k]))
+        off += k
+        e.step(dt, 1)
+        engines.append(e)
+    for e in engines:
+        e.sync()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(loop_steps):
+        for e in engines:
+            e.step(dt, 1)
+    for e in engines:
+        e.sync()
+    t_loop = time.perf_counter() - t0
+    for e in engines:
+        e.close()
+    batched = n * steps / t_batched
+    looped = n * loop_steps / t_loop
+    return {"workload": "config 2: %d flocks, %d agents, sizes log-uniform [128, 65536], maxNeighbors 16" %
+                        (len(w.params), n),
+            "value": batched, "unit": UNIT, "ms_per_step": 1e3 * t_batched / steps, "steps": steps,
+            "looped_value": looped, "looped_ms_per_step": 1e3 * t_loop / loop_steps,
+            "looped": "one engine per flock, %d steps of plain per-step launches looped over the flocks" % loop_steps,
+            "speedup_vs_looped": batched / looped}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -197,6 +253,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--e2e-iters", type=int, default=3)
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="run W warm-up + this many single steps and exit (for ncu)")
@@ -349,6 +406,8 @@ def main():
         line["cpu_baseline"] = base
         line["accuracy"] = accuracy
     eng.close()
+    if world == 1 and not args.no_batched:
+        line["batched"] = batched_leg(local)
     if pg:
         pg.barrier()
         pg.destroy_process_group()

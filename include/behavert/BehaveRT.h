@@ -1,0 +1,484 @@
+// BehaveRT.h -- header-only C++ facade of the reference's plugin engine over
+// the C-ABI of libbehavert_b200.so.
+//
+// Keeps the reference's class names, mixin structure and per-frame method
+// names so that an application written against the reference compiles
+// against this header:
+//   CommonResources m_CommonRes                      Core/include/CommonResources.h:62-126
+//   DeviceInterface                                  Core/include/DeviceInterface.cuh:53-297
+//   DeviceArrayWrapper<T>                            Core/include/DeviceArrayWrapper.h:58-192
+//   SimEnginePlugIn / DummyPlugIn                    Core/include/SimEnginePlugIn.h:79-200
+//   Body3DPlugIn / EnvGrid3DPlugIn / Proximity3DPlugIn / OpenSteerWrapperPlugIn /
+//   BehaviorClusteringPlugIn                         PlugIns/*/include/*PlugIn.h
+//   UtilityConfigFile ([Section] key = value)        Core/include/UtilityConfigFile.h:54-81
+//
+// Differences: there is no GL/VBO interop (arrays are plain device memory
+// inside the engine), the world is the periodic cube [0, worldSize)^3, errors
+// throw BehaveRT::Error instead of exiting, and the random initialisation of
+// reset() uses an explicit seed instead of rand().
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <fstream>
+#include <map>
+#include <memory>
+#include <random>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../behavert_b200.h"
+
+namespace BehaveRT {
+
+typedef unsigned int uint;
+typedef std::vector<std::string> DependenciesList;
+
+struct float4v { float x, y, z, w; };
+struct uint2v { uint32_t x, y; };
+
+class Error : public std::runtime_error {
+ public:
+  Error(const std::string& where, int status)
+      : std::runtime_error(where + ": " + brt_error_string(status) + " (" + brt_last_error() + ")"), status(status) {}
+  int status;
+};
+
+inline void check(int status, const char* where) {
+  if (status != BRT_OK) throw Error(where, status);
+}
+
+// ---------------------------------------------------------------------------
+// [Section] key = value configuration (UtilityConfigFile).
+class UtilityConfigFile {
+ public:
+  void load(const std::string& path) {
+    std::ifstream in(path);
+    if (!in) throw std::runtime_error("cannot open config file " + path);
+    std::string line, section;
+    while (std::getline(in, line)) {
+      const size_t hash = line.find_first_of("#;");
+      if (hash != std::string::npos) line = line.substr(0, hash);
+      line = trim(line);
+      if (line.empty()) continue;
+      if (line.front() == '[' && line.back() == ']') { section = trim(line.substr(1, line.size() - 2)); continue; }
+      const size_t eq = line.find('=');
+      if (eq == std::string::npos) continue;
+      m_Settings[section][trim(line.substr(0, eq))] = trim(line.substr(eq + 1));
+    }
+  }
+  void setSetting(const std::string& key, const std::string& section, const std::string& value) {
+    m_Settings[section][key] = value;
+  }
+  std::string getSetting(const std::string& key, const std::string& section, const std::string& def = "") const {
+    auto s = m_Settings.find(section);
+    if (s == m_Settings.end()) return def;
+    auto k = s->second.find(key);
+    return k == s->second.end() ? def : k->second;
+  }
+  bool has(const std::string& key, const std::string& section) const { return !getSetting(key, section).empty(); }
+
+ private:
+  static std::string trim(const std::string& s) {
+    const size_t a = s.find_first_not_of(" \t\r\n"), b = s.find_last_not_of(" \t\r\n");
+    return a == std::string::npos ? std::string() : s.substr(a, b - a + 1);
+  }
+  std::map<std::string, std::map<std::string, std::string>> m_Settings;
+};
+
+inline float parseFloat(const std::string& s) { return std::stof(s); }
+inline int parseInt(const std::string& s) { return std::stoi(s); }
+inline bool parseBool(const std::string& s) { return s == "true" || s == "1" || s == "yes"; }
+inline void parseFloat3(const std::string& s, float* v) {
+  std::istringstream in(s);
+  in >> v[0] >> v[1] >> v[2];
+}
+
+// ---------------------------------------------------------------------------
+// DeviceInterface: device selection, synchronisation and the engine handle.
+class DeviceInterface {
+ public:
+  explicit DeviceInterface(int device = 0) : m_Device(device) {}
+  ~DeviceInterface() { release(); }
+  int device() const { return m_Device; }
+  brt_engine* engine() const { return m_Engine; }
+  bool hasEngine() const { return m_Engine != nullptr; }
+  void createEngine(const brt_params& p) {
+    release();
+    check(brt_engine_create(&p, 1, m_Device, &m_Engine), "brt_engine_create");
+  }
+  void release() {
+    if (m_Engine) brt_engine_destroy(m_Engine);
+    m_Engine = nullptr;
+  }
+  // Core/DeviceInterface.cu:114-118
+  void threadSync() {
+    if (m_Engine) check(brt_sync(m_Engine), "brt_sync");
+  }
+
+ private:
+  int m_Device;
+  brt_engine* m_Engine = nullptr;
+};
+
+// ---------------------------------------------------------------------------
+// CommonResources: configuration, device interface and the parameters the
+// installed plugins fill in (the reference's hXParams globals).
+class CommonResources {
+ public:
+  CommonResources() { brt_params_default(&m_Params); }
+  void initialize(const std::string& configFileName) {
+    if (!configFileName.empty()) m_Config.load(configFileName);
+    m_Initialized = true;
+  }
+  bool isInitialized() const { return m_Initialized; }
+  DeviceInterface* getDeviceInterface() { return &m_DeviceInterface; }
+  UtilityConfigFile* getConfig() { return &m_Config; }
+  brt_params& params() { return m_Params; }
+  // The engine is created the first time a functionality needs it, once
+  // every plugin has installed its parameters.
+  brt_engine* engine() {
+    if (!m_DeviceInterface.hasEngine()) m_DeviceInterface.createEngine(m_Params);
+    return m_DeviceInterface.engine();
+  }
+  void installPlugIn(const std::string& name) { m_Installed.push_back(name); }
+  const std::vector<std::string>& installedPlugIns() const { return m_Installed; }
+  uint32_t seed = 1;
+
+ private:
+  bool m_Initialized = false;
+  UtilityConfigFile m_Config;
+  DeviceInterface m_DeviceInterface;
+  brt_params m_Params;
+  std::vector<std::string> m_Installed;
+};
+
+inline CommonResources m_CommonRes;
+
+#define BRT_READ_PARAM(section, key, target, parser)                                                       \
+  do {                                                                                                     \
+    const std::string _v = m_CommonRes.getConfig()->getSetting(key, section);                             \
+    if (!_v.empty()) target = parser(_v);                                                                  \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// DeviceArrayWrapper<T>: host image of one engine feature.  The device image
+// is the engine's own array; copyArrayFromDevice / copyArrayToDevice move
+// the whole feature in agent-id order.
+enum class Feature { Position, Forward, SmoothAccel, Features, SimilarityStats, Hash, CellStart, NeighList, SteerForce };
+
+template <class Type>
+class DeviceArrayWrapper {
+ public:
+  DeviceArrayWrapper(Feature feature, int size, int dimension = 1)
+      : m_Feature(feature), m_Size(size), m_Dimension(dimension), m_Host((size_t)size * dimension) {}
+  Type* getHostArray() { return m_Host.data(); }
+  int getSize() const { return m_Size; }
+  int getElementBytesCount() const { return (int)sizeof(Type) * m_Dimension; }
+  int getBytesCount() const { return getElementBytesCount() * m_Size; }
+  Type getHostArrayElement(int index, bool copyFromDevice = false) {
+    if (copyFromDevice) copyArrayFromDevice();
+    return m_Host[(size_t)index * m_Dimension];
+  }
+  void setHostArrayElement(int index, const Type* element, bool copyToDevice = false) {
+    for (int d = 0; d < m_Dimension; ++d) m_Host[(size_t)index * m_Dimension + d] = element[d];
+    if (copyToDevice) copyArrayToDevice();
+  }
+  void reset(char val) { std::fill((char*)m_Host.data(), (char*)m_Host.data() + m_Host.size() * sizeof(Type), val); }
+  void copyArrayFromDevice() {
+    brt_engine* e = m_CommonRes.engine();
+    void* h = m_Host.data();
+    switch (m_Feature) {
+      case Feature::Position: check(brt_get_state(e, (float*)h, nullptr, nullptr, nullptr, BRT_MEM_HOST), "getPos"); break;
+      case Feature::Forward: check(brt_get_state(e, nullptr, (float*)h, nullptr, nullptr, BRT_MEM_HOST), "getForward"); break;
+      case Feature::SmoothAccel: check(brt_get_state(e, nullptr, nullptr, (float*)h, nullptr, BRT_MEM_HOST), "getSmoothAccel"); break;
+      case Feature::Features: check(brt_get_state(e, nullptr, nullptr, nullptr, (float*)h, BRT_MEM_HOST), "getFeatures"); break;
+      case Feature::SimilarityStats: check(brt_get_similarity_stats(e, (float*)h, BRT_MEM_HOST), "getSimilarityStats"); break;
+      case Feature::Hash: {
+        std::vector<uint32_t> k(m_Size), id(m_Size);
+        check(brt_get_hash(e, k.data(), id.data(), BRT_MEM_HOST), "getHash");
+        uint2v* o = (uint2v*)h;
+        for (int i = 0; i < m_Size; ++i) o[i] = uint2v{k[i], id[i]};
+        break;
+      }
+      case Feature::CellStart: check(brt_get_cell_ranges(e, (uint32_t*)h, nullptr, BRT_MEM_HOST), "getCellStart"); break;
+      case Feature::NeighList: check(brt_get_neighbor_lists(e, (uint32_t*)h, BRT_MEM_HOST), "neighList"); break;
+      case Feature::SteerForce: check(brt_get_steer_force(e, (float*)h, BRT_MEM_HOST), "steerForce"); break;
+    }
+  }
+  void copyArrayToDevice() {
+    brt_engine* e = m_CommonRes.engine();
+    const float* h = (const float*)m_Host.data();
+    switch (m_Feature) {
+      case Feature::Position: check(brt_set_state(e, h, nullptr, nullptr, nullptr, BRT_MEM_HOST), "setPos"); break;
+      case Feature::Forward: check(brt_set_state(e, nullptr, h, nullptr, nullptr, BRT_MEM_HOST), "setForward"); break;
+      case Feature::SmoothAccel: check(brt_set_state(e, nullptr, nullptr, h, nullptr, BRT_MEM_HOST), "setSmoothAccel"); break;
+      case Feature::Features: check(brt_set_state(e, nullptr, nullptr, nullptr, h, BRT_MEM_HOST), "setFeatures"); break;
+      case Feature::SimilarityStats: check(brt_set_similarity_stats(e, h, BRT_MEM_HOST), "setSimilarityStats"); break;
+      default: throw std::runtime_error("feature is computed by the engine and cannot be written");
+    }
+  }
+  // Double buffering is internal to the engine; kept for source compatibility.
+  void swapPosReadWrite() {}
+
+ private:
+  Feature m_Feature;
+  int m_Size, m_Dimension;
+  std::vector<Type> m_Host;
+};
+
+// ---------------------------------------------------------------------------
+// SimEnginePlugIn / DummyPlugIn (Core/include/SimEnginePlugIn.h:79-200).
+class SimEnginePlugIn {
+ public:
+  virtual ~SimEnginePlugIn() {}
+  virtual const std::string name() = 0;
+  virtual const DependenciesList plugInDependencies() = 0;
+  virtual void reset() = 0;
+  virtual void update(const float elapsedTime) = 0;
+
+ protected:
+  // Dependency check of Core/src/SimEnginePlugIn.cpp:69-116, throwing
+  // instead of exiting.
+  void installPlugIn() {
+    for (const std::string& dep : plugInDependencies()) {
+      bool found = false;
+      for (const std::string& p : m_CommonRes.installedPlugIns()) found = found || p == dep;
+      if (!found) throw std::runtime_error("missing plugIn dependency " + dep + " of " + name());
+    }
+    m_CommonRes.installPlugIn(name());
+  }
+};
+
+class DummyPlugIn : public SimEnginePlugIn {
+ public:
+  const std::string name() override { return "PlugInRoot"; }
+  const DependenciesList plugInDependencies() override { return {}; }
+  void reset() override {}
+  void update(const float) override {}
+};
+
+// ---------------------------------------------------------------------------
+// Body3DPlugIn (PlugIns/Body/include/Body3DPlugIn.h:105-129)
+template <class Super>
+class Body3DPlugIn : public Super {
+ public:
+  Body3DPlugIn() {
+    brt_params& p = m_CommonRes.params();
+    const std::string s = "Body3DPlugIn";
+    BRT_READ_PARAM(s, "numBodies", p.numBodies, parseInt);
+    if (parseBool(m_CommonRes.getConfig()->getSetting("isBodyNumExponent", s))) p.numBodies = 1u << p.numBodies;
+    BRT_READ_PARAM(s, "commonRadius", p.commonRadius, parseFloat);
+    BRT_READ_PARAM(s, "use2DProjection", p.use2DProjection, parseBool);
+    SimEnginePlugIn::installPlugIn();
+  }
+  const std::string name() override { return "Body3DPlugIn"; }
+  const DependenciesList plugInDependencies() override { return {}; }
+  void reset() override { Super::reset(); }
+  void update(const float t) override { Super::update(t); }
+};
+
+// EnvGrid3DPlugIn (PlugIns/EnvGrid3D/include/EnvGrid3DPlugIn.h:56-140)
+template <class Super>
+class EnvGrid3DPlugIn : public Super {
+ public:
+  EnvGrid3DPlugIn() {
+    brt_params& p = m_CommonRes.params();
+    const std::string s = "EnvGrid3DPlugIn";
+    float cell[3] = {p.cellSize, p.cellSize, p.cellSize};
+    const std::string cs = m_CommonRes.getConfig()->getSetting("cellSize", s);
+    if (!cs.empty()) { parseFloat3(cs, cell); p.cellSize = cell[0]; }
+    BRT_READ_PARAM(s, "worldSize", p.worldSize, parseFloat);
+    BRT_READ_PARAM(s, "maxBodiesPerCell", p.maxBodiesPerCell, parseInt);
+    SimEnginePlugIn::installPlugIn();
+  }
+  const std::string name() override { return "EnvGrid3DPlugIn"; }
+  const DependenciesList plugInDependencies() override { return {"Body3DPlugIn"}; }
+  // EnvGrid3DPlugIn::reset (:225-275): positions uniform in the world.
+  void reset() override {
+    Super::reset();
+    brt_params& p = m_CommonRes.params();
+    std::mt19937 rng(m_CommonRes.seed);
+    std::uniform_real_distribution<float> u(0.0f, p.worldSize);
+    DeviceArrayWrapper<float4v>* pos = getPos();
+    for (uint32_t i = 0; i < p.numBodies; ++i) {
+      float4v v{u(rng), u(rng), u(rng), 1.0f};
+      for (float* c : {&v.x, &v.y, &v.z}) if (*c >= p.worldSize) *c = 0.0f;
+      pos->setHostArrayElement((int)i, &v);
+    }
+    pos->copyArrayToDevice();
+  }
+  void update(const float t) override { Super::update(t); }
+  void reorderSimData() { check(brt_reorder_sim_data(m_CommonRes.engine()), "reorderSimData"); }
+  DeviceArrayWrapper<float4v>* getPos() {
+    if (!m_Pos) m_Pos.reset(new DeviceArrayWrapper<float4v>(Feature::Position, (int)m_CommonRes.params().numBodies));
+    return m_Pos.get();
+  }
+  DeviceArrayWrapper<uint2v>* getHash() {
+    if (!m_Hash) m_Hash.reset(new DeviceArrayWrapper<uint2v>(Feature::Hash, (int)m_CommonRes.params().numBodies));
+    return m_Hash.get();
+  }
+  // Agent id of the agent at sorted slot `index`.
+  uint getSortedIndex(uint index, bool copyFromDevice = true) { return getHash()->getHostArrayElement((int)index, copyFromDevice).y; }
+
+ protected:
+  std::unique_ptr<DeviceArrayWrapper<float4v>> m_Pos;
+  std::unique_ptr<DeviceArrayWrapper<uint2v>> m_Hash;
+};
+
+// Proximity3DPlugIn (PlugIns/Proximity3D/include/Proximity3DPlugIn.h:56-110)
+template <class Super>
+class Proximity3DPlugIn : public Super {
+ public:
+  Proximity3DPlugIn() {
+    brt_params& p = m_CommonRes.params();
+    const std::string s = "Proximity3DPlugIn";
+    BRT_READ_PARAM(s, "useKnn", p.useKnn, parseBool);
+    BRT_READ_PARAM(s, "maxNeighbors", p.maxNeighbors, parseInt);
+    BRT_READ_PARAM(s, "commonSearchRadius", p.commonSearchRadius, parseFloat);
+    if (parseBool(m_CommonRes.getConfig()->getSetting("useCellSizeAsSearchRadius", s))) p.commonSearchRadius = p.cellSize;
+    SimEnginePlugIn::installPlugIn();
+  }
+  const std::string name() override { return "Proximity3DPlugIn"; }
+  const DependenciesList plugInDependencies() override { return {"Body3DPlugIn", "EnvGrid3DPlugIn"}; }
+  void reset() override { Super::reset(); }
+  void update(const float t) override { Super::update(t); }
+  void computeNeighborhoods() { check(brt_compute_neighborhoods(m_CommonRes.engine()), "computeNeighborhoods"); }
+  DeviceArrayWrapper<uint>* getCellStart() {
+    if (!m_CellStart) {
+      uint32_t cells = 0;
+      check(brt_engine_num_cells(m_CommonRes.engine(), &cells), "num_cells");
+      m_CellStart.reset(new DeviceArrayWrapper<uint>(Feature::CellStart, (int)cells));
+    }
+    return m_CellStart.get();
+  }
+  DeviceArrayWrapper<uint>* getNeighList() {
+    if (!m_NeighList) {
+      uint32_t stride = 0;
+      check(brt_neighbor_list_stride(m_CommonRes.engine(), &stride), "list_stride");
+      m_NeighList.reset(new DeviceArrayWrapper<uint>(Feature::NeighList, (int)m_CommonRes.params().numBodies, (int)stride));
+    }
+    return m_NeighList.get();
+  }
+
+ protected:
+  std::unique_ptr<DeviceArrayWrapper<uint>> m_CellStart;
+  std::unique_ptr<DeviceArrayWrapper<uint>> m_NeighList;
+};
+
+// OpenSteerWrapperPlugIn (PlugIns/OpenSteerWrapper/include/OpenSteerWrapperPlugIn.h:54-120)
+template <class Super>
+class OpenSteerWrapperPlugIn : public Super {
+ public:
+  OpenSteerWrapperPlugIn() {
+    brt_params& p = m_CommonRes.params();
+    const std::string s = "OpenSteerWrapperPlugIn";
+    UtilityConfigFile* c = m_CommonRes.getConfig();
+    if (c->has("separationParams", s)) parseFloat3(c->getSetting("separationParams", s), p.separationParams);
+    if (c->has("cohesionParams", s)) parseFloat3(c->getSetting("cohesionParams", s), p.cohesionParams);
+    if (c->has("alignmentParams", s)) parseFloat3(c->getSetting("alignmentParams", s), p.alignmentParams);
+    BRT_READ_PARAM(s, "commonMass", p.commonMass, parseFloat);
+    BRT_READ_PARAM(s, "commonMaxSpeed", p.commonMaxSpeed, parseFloat);
+    BRT_READ_PARAM(s, "commonMaxForce", p.commonMaxForce, parseFloat);
+    BRT_READ_PARAM(s, "commonSensingMinRadius", p.commonSensingMinRadius, parseFloat);
+    SimEnginePlugIn::installPlugIn();
+  }
+  const std::string name() override { return "OpenSteerWrapperPlugIn"; }
+  const DependenciesList plugInDependencies() override { return {"EnvGrid3DPlugIn", "Proximity3DPlugIn"}; }
+  // OpenSteerWrapperPlugIn::reset (:195-263): random unit forward, w = maxSpeed.
+  void reset() override {
+    Super::reset();
+    brt_params& p = m_CommonRes.params();
+    std::mt19937 rng(m_CommonRes.seed + 1);
+    std::normal_distribution<float> g(0.0f, 1.0f);
+    DeviceArrayWrapper<float4v>* fwd = getForward();
+    DeviceArrayWrapper<float4v>* acc = getSmoothAccel();
+    for (uint32_t i = 0; i < p.numBodies; ++i) {
+      float x = g(rng), y = g(rng), z = g(rng);
+      const float l = std::sqrt(x * x + y * y + z * z);
+      float4v f{x / l, y / l, z / l, p.commonMaxSpeed}, a{0, 0, 0, 0};
+      fwd->setHostArrayElement((int)i, &f);
+      acc->setHostArrayElement((int)i, &a);
+    }
+    fwd->copyArrayToDevice();
+    acc->copyArrayToDevice();
+  }
+  void update(const float t) override { Super::update(t); }
+  void resetSteerForce() { check(brt_reset_steer_force(m_CommonRes.engine()), "resetSteerForce"); }
+  void computeSeparations() { check(brt_compute_separations(m_CommonRes.engine()), "computeSeparations"); }
+  void computeAlignments() { check(brt_compute_alignments(m_CommonRes.engine()), "computeAlignments"); }
+  void computeCohesions() { check(brt_compute_cohesions(m_CommonRes.engine()), "computeCohesions"); }
+  void computeSeekingsWorldCenter() { check(brt_compute_seekings_world_center(m_CommonRes.engine()), "computeSeekingsWorldCenter"); }
+  void applySteeringForces(float elapsedTime) { check(brt_apply_steering_forces(m_CommonRes.engine(), elapsedTime), "applySteeringForces"); }
+  DeviceArrayWrapper<float4v>* getForward() {
+    if (!m_Forward) m_Forward.reset(new DeviceArrayWrapper<float4v>(Feature::Forward, (int)m_CommonRes.params().numBodies));
+    return m_Forward.get();
+  }
+  DeviceArrayWrapper<float4v>* getSmoothAccel() {
+    if (!m_Accel) m_Accel.reset(new DeviceArrayWrapper<float4v>(Feature::SmoothAccel, (int)m_CommonRes.params().numBodies));
+    return m_Accel.get();
+  }
+  DeviceArrayWrapper<float4v>* getSteerForce() {
+    if (!m_Steer) m_Steer.reset(new DeviceArrayWrapper<float4v>(Feature::SteerForce, (int)m_CommonRes.params().numBodies));
+    return m_Steer.get();
+  }
+  // The whole per-frame update of BehaveRT_Flocking.cpp:177-199 as one call
+  // (fused kernel; nsteps > 1 runs a captured CUDA graph).
+  void step(float elapsedTime, uint32_t nsteps = 1) { check(brt_step(m_CommonRes.engine(), elapsedTime, nsteps), "brt_step"); }
+
+ protected:
+  std::unique_ptr<DeviceArrayWrapper<float4v>> m_Forward, m_Accel, m_Steer;
+};
+
+// BehaviorClusteringPlugIn (PlugIns/BehaviorClustering/include/BehaviorClusteringPlugIn.h:60-230)
+template <class Super>
+class BehaviorClusteringPlugIn : public Super {
+ public:
+  BehaviorClusteringPlugIn() {
+    brt_params& p = m_CommonRes.params();
+    const std::string s = "BehaviorClusteringPlugIn";
+    UtilityConfigFile* c = m_CommonRes.getConfig();
+    BRT_READ_PARAM(s, "featuresCount", p.featuresCount, parseInt);
+    if (c->has("clusteringForceParams", s)) parseFloat3(c->getSetting("clusteringForceParams", s), p.clusteringForceParams);
+    if (c->has("alignmentClusteringForceParams", s))
+      parseFloat3(c->getSetting("alignmentClusteringForceParams", s), p.alignmentClusteringForceParams);
+    if (c->has("similarityStatsParams", s)) parseFloat3(c->getSetting("similarityStatsParams", s), p.similarityStatsParams);
+    BRT_READ_PARAM(s, "featureRelaxRate", p.featureRelaxRate, parseFloat);
+    SimEnginePlugIn::installPlugIn();
+  }
+  const std::string name() override { return "BehaviorClusteringPlugIn"; }
+  const DependenciesList plugInDependencies() override {
+    return {"Body3DPlugIn", "EnvGrid3DPlugIn", "Proximity3DPlugIn", "OpenSteerWrapperPlugIn"};
+  }
+  void reset() override {
+    Super::reset();
+    brt_params& p = m_CommonRes.params();
+    if (!p.featuresCount) return;
+    std::mt19937 rng(m_CommonRes.seed + 2);
+    std::uniform_real_distribution<float> u(0.0f, 1.0f);
+    DeviceArrayWrapper<float>* f = getFeaturesVector();
+    std::vector<float> v(p.featuresCount);
+    for (uint32_t i = 0; i < p.numBodies; ++i) {
+      for (float& x : v) x = u(rng);
+      f->setHostArrayElement((int)i, v.data());
+    }
+    f->copyArrayToDevice();
+  }
+  void update(const float t) override { Super::update(t); }
+  void steerForClustering() { check(brt_steer_for_clustering(m_CommonRes.engine()), "steerForClustering"); }
+  DeviceArrayWrapper<float>* getFeaturesVector() {
+    if (!m_Features)
+      m_Features.reset(new DeviceArrayWrapper<float>(Feature::Features, (int)m_CommonRes.params().numBodies,
+                                                      (int)m_CommonRes.params().featuresCount));
+    return m_Features.get();
+  }
+
+ protected:
+  std::unique_ptr<DeviceArrayWrapper<float>> m_Features;
+};
+
+}  // namespace BehaveRT
