@@ -44,6 +44,12 @@ def lib():
         L.oracle_num_cells.restype = C.c_int
         L.oracle_num_cells.argtypes = [C.c_uint32, _vp, _u32p]
         L.oracle_hardware_threads.restype = C.c_int
+        L.oracle_frozen_forward.restype = C.c_int
+        L.oracle_frozen_forward.argtypes = [C.c_uint32, _vp, _vp, C.c_uint32, C.c_double, _vp, _vp, _vp, _vp,
+                                            _vp, _vp, _vp, _vp, _vp, C.c_int]
+        L.oracle_frozen_reverse.restype = C.c_int
+        L.oracle_frozen_reverse.argtypes = [C.c_uint32, _vp, _vp, C.c_uint32, C.c_double, _vp, _vp, _vp, _vp,
+                                            _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int]
         _LIB = L
     return _LIB
 
@@ -107,3 +113,86 @@ def step(params: Sequence, pos, fwd, acc, feat=None, stats=None, dt: float = 0.1
     if rc:
         raise RuntimeError("oracle_step failed: %d" % rc)
     return out
+
+
+# ---------------------------------------------------------------------------
+# FP64 frozen-neighbour / frozen-branch model (oracle/brt_oracle_adjoint.cpp)
+
+def _threads(threads: int) -> int:
+    if threads <= 0:
+        threads = min(hardware_threads(), int(os.environ.get("BRT_ORACLE_THREADS", "64")))
+    return threads
+
+
+def lists_by_id(step_out: dict) -> np.ndarray:
+    """Neighbour lists of one oracle step re-indexed by agent id: row id is
+    the count, then the neighbours' agent ids in list order."""
+    ids = step_out["ids"]
+    lists = step_out["lists"]
+    out = np.zeros_like(lists)
+    n = lists[:, 0]
+    out[ids, 0] = n
+    stride = lists.shape[1]
+    k = np.arange(stride - 1)[None, :]
+    valid = k < n[:, None]
+    nb = np.where(valid, ids[np.minimum(lists[:, 1:], len(ids) - 1)], 0)
+    out[ids, 1:] = nb
+    return out
+
+
+def frozen_forward(params: Sequence, pos, fwd, acc, lists, weights=None, flags=None, dt: float = 0.1,
+                   want_flags: bool = False, threads: int = 0) -> dict:
+    """FP64 trajectory over len(lists) steps with the given per-step lists
+    (T x N x stride, by agent id) and, optionally, frozen branch flags
+    (T x N x 4).  Returns the final state (float64, agent-id order)."""
+    from behavert_b200._abi import BrtParams
+    lists = np.ascontiguousarray(lists, np.uint32)
+    T, n = lists.shape[0], lists.shape[1]
+    pos = np.ascontiguousarray(pos, np.float64)
+    fwd = np.ascontiguousarray(fwd, np.float64)
+    acc = np.ascontiguousarray(acc, np.float64)
+    w = None if weights is None else np.ascontiguousarray(weights, np.float64).reshape(-1)
+    fz = None if flags is None else np.ascontiguousarray(flags, np.uint32)
+    fo = np.zeros((T, n, 4), np.uint32) if want_flags else None
+    out = {"pos": np.empty((n, 4)), "fwd": np.empty((n, 4)), "acc": np.empty((n, 4))}
+    arr = (BrtParams * len(params))(*params)
+    rc = lib().oracle_frozen_forward(len(params), C.cast(arr, _vp), _p(w), T, float(dt), _p(pos), _p(fwd), _p(acc),
+                                     _p(lists), _p(fz), _p(fo), _p(out["pos"]), _p(out["fwd"]), _p(out["acc"]),
+                                     _threads(threads))
+    if rc:
+        raise RuntimeError("oracle_frozen_forward failed: %d" % rc)
+    if want_flags:
+        out["flags"] = fo
+    return out
+
+
+def frozen_reverse(params: Sequence, pos, fwd, acc, lists, gpos_T, gfwd_T=None, gacc_T=None, weights=None,
+                   flags=None, dt: float = 0.1, threads: int = 0) -> dict:
+    """Reverse mode of frozen_forward: adjoint of the initial state and of
+    the per-flock weights (nflocks x 3) given the final state's adjoint."""
+    from behavert_b200._abi import BrtParams
+    lists = np.ascontiguousarray(lists, np.uint32)
+    T, n = lists.shape[0], lists.shape[1]
+    z = np.zeros((n, 4))
+    pos = np.ascontiguousarray(pos, np.float64)
+    fwd = np.ascontiguousarray(fwd, np.float64)
+    acc = np.ascontiguousarray(acc, np.float64)
+    gp = np.ascontiguousarray(gpos_T, np.float64)
+    gf = z if gfwd_T is None else np.ascontiguousarray(gfwd_T, np.float64)
+    ga = z if gacc_T is None else np.ascontiguousarray(gacc_T, np.float64)
+    w = None if weights is None else np.ascontiguousarray(weights, np.float64).reshape(-1)
+    fz = None if flags is None else np.ascontiguousarray(flags, np.uint32)
+    out = {"pos": np.empty((n, 4)), "fwd": np.empty((n, 4)), "acc": np.empty((n, 4)),
+           "weights": np.empty((len(params), 3))}
+    arr = (BrtParams * len(params))(*params)
+    rc = lib().oracle_frozen_reverse(len(params), C.cast(arr, _vp), _p(w), T, float(dt), _p(pos), _p(fwd), _p(acc),
+                                     _p(lists), _p(fz), _p(gp), _p(gf), _p(ga), _p(out["pos"]), _p(out["fwd"]),
+                                     _p(out["acc"]), _p(out["weights"]), _threads(threads))
+    if rc:
+        raise RuntimeError("oracle_frozen_reverse failed: %d" % rc)
+    return out
+
+
+def min_image(d, L):
+    """Minimum image of offsets in a periodic cube of side L."""
+    return d - L * np.round(d / L)
