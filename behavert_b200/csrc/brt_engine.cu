@@ -3,6 +3,7 @@
 // stage-wise functionalities of the reference's plugin chain.
 #include "brt_internal.cuh"
 #include "brt_kernels.cuh"
+#include "brt_engine_impl.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -102,75 +103,12 @@ static FlockDev toDev(const brt_params& p, uint32_t G) {
 
 using namespace brt;
 
-struct brt_engine {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  uint32_t nflocks = 0, N = 0, C = 0, Cpad = 0, Mmax = 0, Fmax = 0, Fs = 0;
-  std::vector<brt_params> params;
-  std::vector<FlockDev> flocksHost;
-  FlockDev* flocks = nullptr;
-  uint32_t* agentBase = nullptr;
-  float4* obstacles = nullptr;
-  bool anyKnn = false;
-  bool forceTwoPass = false;  // option "two_pass": run the list-first kernel even when not needed
-  int phase2Variant = 0;      // option "phase2_variant": list walk one or two neighbours at a time
-  int scanVariant = 0;        // option "scan_variant": neighbour-scan loop shape
-  // state
-  float4 *posA = nullptr, *fwdA = nullptr, *accA = nullptr, *posS = nullptr, *fwdS = nullptr, *accS = nullptr;
-  float *featA = nullptr, *featS = nullptr, *featNormS = nullptr;
-  uint32_t *idA = nullptr, *idS = nullptr;
-  float4* statsById = nullptr;
-  float4* steer = nullptr;
-  uint32_t* lists = nullptr;
-  uint32_t listStride = 0;
-  uint2* pairs[2] = {nullptr, nullptr};
-  uint32_t *cellStart = nullptr, *cellEnd = nullptr;
-  SortPlan plan;
-  void* sortMem = nullptr;
-  SortScratch ss;
-  uint32_t* errWord = nullptr;
-  float4* stage4 = nullptr;  // id-order staging (N float4)
-  float* stageF = nullptr;   // id-order staging (N * Fmax)
-  // pipeline state
-  bool reordered = false, listsValid = false, recordLists = false;
-  uint32_t finalPairs = 0;
-  uint32_t paramsVersion = 0;
-  std::map<std::tuple<uint32_t, uint32_t, bool, uint32_t>, cudaGraphExec_t> graphs;
-  uint32_t smCount = 148;
-  // per-stage timing: a ring of event sets, drained into totals
-  static constexpr int kRing = 32;
-  bool timing = false, capturing = false;
-  cudaEvent_t ev[kRing][5] = {};
-  bool pending[kRing] = {};
-  int ringPos = 0;
-  double stageMs[4] = {0, 0, 0, 0};
-  uint64_t timedSteps = 0;
-};
 
 namespace {
 
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
-    cudaGetDevice(&prev);
-    if (prev != dev) cudaSetDevice(dev);
-  }
-  ~DeviceGuard() {
-    int cur = -1;
-    cudaGetDevice(&cur);
-    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
-  }
-};
-
-template <class T>
-int devAlloc(T** p, size_t count) {
-  *p = nullptr;
-  if (count == 0) return BRT_OK;
-  BRT_CUDA_TRY(cudaMalloc((void**)p, count * sizeof(T)));
-  return BRT_OK;
-}
-
 void freeAll(brt_engine* e) {
+  freeAdjoint(e->adj);
+  e->adj = nullptr;
   for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second);
   e->graphs.clear();
   for (int r = 0; r < brt_engine::kRing; ++r)
@@ -249,6 +187,7 @@ int enqueueReorder(brt_engine* e) {
   R.posA = e->posA; R.fwdA = e->fwdA; R.accA = e->accA; R.featA = e->featA; R.idA = e->idA;
   R.posS = e->posS; R.fwdS = e->fwdS; R.accS = e->accS; R.featS = e->featS; R.idS = e->idS;
   R.featNormS = e->featNormS;
+  R.prevOut = e->tapePrev;
   R.fs4 = e->Fs / 4;
   R.cellStart = e->cellStart; R.cellEnd = e->cellEnd;
   R.hist = e->ss.hist; R.histWords = e->plan.passes * e->plan.bins;
@@ -335,6 +274,11 @@ int syncAndCheck(brt_engine* e) { return checkDeviceError(e, true); }
 int configureKernels(brt_engine* e);
 
 }  // namespace
+
+namespace brt {
+int engineEnqueueStep(brt_engine* e, float dt, bool record) { return enqueueStep(e, dt, record); }
+int engineSyncAndCheck(brt_engine* e) { return syncAndCheck(e); }
+}  // namespace brt
 
 // ---------------------------------------------------------------------------
 extern "C" {
@@ -558,6 +502,10 @@ int brt_engine_set_option(brt_engine* e, const char* key, int64_t value) {
   } else if (k == "scan_variant") {
     if (value < 0 || value > 3) { setLastError("scan_variant must be in [0, 3]"); return BRT_ERR_ARG; }
     e->scanVariant = (int)value;
+  } else if (k == "adjoint_graphs") {
+    e->adjointGraphs = value != 0;
+  } else if (k == "adjoint_export") {
+    e->adjointExport = value != 0;
   } else if (k == "sort_digit_bits") {
     if (value < 4 || value > 9) { setLastError("sort_digit_bits must be in [4, 9]"); return BRT_ERR_ARG; }
     BRT_CUDA_TRY(cudaStreamSynchronize(e->stream));

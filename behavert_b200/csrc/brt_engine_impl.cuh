@@ -1,0 +1,96 @@
+// brt_engine_impl.cuh -- the engine object shared by the host-side files of
+// the library (brt_engine.cu, brt_adjoint_host.cu).  Not installed.
+#pragma once
+
+#include "brt_internal.cuh"
+#include "brt_kernels.cuh"
+
+#include <map>
+#include <memory>
+#include <tuple>
+#include <vector>
+
+namespace brt {
+struct AdjointState;
+void freeAdjoint(AdjointState* a);
+}  // namespace brt
+
+struct brt_engine {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  uint32_t nflocks = 0, N = 0, C = 0, Cpad = 0, Mmax = 0, Fmax = 0, Fs = 0;
+  std::vector<brt_params> params;
+  std::vector<brt::FlockDev> flocksHost;
+  brt::FlockDev* flocks = nullptr;
+  uint32_t* agentBase = nullptr;
+  float4* obstacles = nullptr;
+  bool anyKnn = false;
+  bool forceTwoPass = false;  // option "two_pass": run the list-first kernel even when not needed
+  int phase2Variant = 0;      // option "phase2_variant": list walk one or two neighbours at a time
+  int scanVariant = 0;        // option "scan_variant": neighbour-scan loop shape
+  // state
+  float4 *posA = nullptr, *fwdA = nullptr, *accA = nullptr, *posS = nullptr, *fwdS = nullptr, *accS = nullptr;
+  float *featA = nullptr, *featS = nullptr, *featNormS = nullptr;
+  uint32_t *idA = nullptr, *idS = nullptr;
+  float4* statsById = nullptr;
+  float4* steer = nullptr;
+  uint32_t* lists = nullptr;
+  uint32_t listStride = 0;
+  uint2* pairs[2] = {nullptr, nullptr};
+  uint32_t *cellStart = nullptr, *cellEnd = nullptr;
+  brt::SortPlan plan;
+  void* sortMem = nullptr;
+  brt::SortScratch ss;
+  uint32_t* errWord = nullptr;
+  float4* stage4 = nullptr;  // id-order staging (N float4)
+  float* stageF = nullptr;   // id-order staging (N * Fmax)
+  // pipeline state
+  bool reordered = false, listsValid = false, recordLists = false;
+  uint32_t finalPairs = 0;
+  uint32_t paramsVersion = 0;
+  std::map<std::tuple<uint32_t, uint32_t, bool, uint32_t>, cudaGraphExec_t> graphs;
+  uint32_t smCount = 148;
+  // per-stage timing: a ring of event sets, drained into totals
+  static constexpr int kRing = 32;
+  bool timing = false, capturing = false;
+  cudaEvent_t ev[kRing][5] = {};
+  bool pending[kRing] = {};
+  int ringPos = 0;
+  double stageMs[4] = {0, 0, 0, 0};
+  uint64_t timedSteps = 0;
+  // adjoint (brt_adjoint_host.cu): tape slot of the reorder's source slots
+  uint32_t* tapePrev = nullptr;
+  brt::AdjointState* adj = nullptr;
+  bool adjointGraphs = true;  // option "adjoint_graphs"
+  bool adjointExport = false; // option "adjoint_export"
+  uint32_t weightsVersion = 0; // bumped by brt_set_steering_weights
+};
+
+namespace brt {
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+template <class T>
+inline int devAlloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) return BRT_OK;
+  BRT_CUDA_TRY(cudaMalloc((void**)p, count * sizeof(T)));
+  return BRT_OK;
+}
+
+// Defined in brt_engine.cu.
+int engineEnqueueStep(brt_engine* e, float dt, bool record);
+int engineSyncAndCheck(brt_engine* e);
+
+}  // namespace brt

@@ -72,6 +72,7 @@ __global__ void __launch_bounds__(256) reorderKernel(ReorderArgs A) {
     A.fwdS[i] = __ldg(&A.fwdA[ps]);
     A.accS[i] = __ldg(&A.accA[ps]);
     A.idS[i] = __ldg(&A.idA[ps]);
+    if (A.prevOut) A.prevOut[i] = ps;
     if (A.fs4) {
       // The feature norm sqrtf(sum f^2) (computeSimilarity's norma,
       // BehaviorClustering_resources.cu:164-175) is the same for every pair

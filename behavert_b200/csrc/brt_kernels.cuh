@@ -31,6 +31,7 @@ struct ReorderArgs {
   const float* featA; const uint32_t* idA;
   float4* posS; float4* fwdS; float4* accS; float* featS; uint32_t* idS;
   float* featNormS;            // sqrtf(sum f^2) per sorted slot (optional)
+  uint32_t* prevOut;           // source slot per sorted slot (optional, adjoint tape)
   uint32_t fs4;                // feature float4s per agent
   uint32_t* cellStart; uint32_t* cellEnd;
   uint32_t* hist; uint32_t histWords;
@@ -67,6 +68,49 @@ struct StageArgs {
   uint32_t listStride;
   uint32_t nflocks, n, Fs;
 };
+
+// Reverse of one taped step (brt_adjoint.cu).
+constexpr uint32_t kAdjointThreads = 128;
+struct AdjointStepArgs {
+  const float4* posS; const float4* fwdS; const float4* accS;   // the step's sorted input state
+  const uint32_t* lists; uint32_t listStride;                    // its neighbour lists (sorted slots)
+  const uint32_t* prev;                                          // canonical slot of each sorted slot
+  const uint32_t* idS;                                           // agent id per sorted slot
+  const FlockDev* flocks; const uint32_t* agentBase; const float4* obstacles;
+  uint32_t nflocks, n;
+  float dt;
+  float4* gOutP; float4* gOutF; float4* gOutA;                   // output adjoint by sorted slot (zeroed)
+  float4* gInP; float4* gInF; float4* gInA;                      // input adjoint by canonical slot
+  double* gW;                                                    // nflocks * 3, accumulated
+  uint32_t* exportLists;                                         // optional, by agent id
+  uint32_t* exportFlags;                                         // optional, 4 words by agent id
+};
+struct LossArgs {
+  const float4* posA; const uint32_t* idA;    // final state, canonical order
+  const float4* target;                       // by agent id
+  const FlockDev* flocks; const uint32_t* agentBase;
+  uint32_t nflocks, n;
+  double* lossPerFlock;                       // accumulated
+  float4* gT;                                 // unscaled terminal position adjoint, canonical order
+};
+struct SeedArgs {
+  const float4* gT; const float* scale;       // scale per flock (device) or null for 1
+  const float4* extraP; const float4* extraF; const float4* extraA;  // optional, by agent id
+  const uint32_t* idA;
+  const uint32_t* agentBase;
+  uint32_t nflocks, n;
+  float4* gP; float4* gF; float4* gA;
+};
+struct OutArgs {
+  const float4* gP; const float4* gF; const float4* gA;
+  const uint32_t* id0; const float4* fwd0;    // initial canonical order
+  uint32_t n;
+  float4* outP; float4* outF; float4* outA; float4* outV;  // by agent id, each optional
+};
+cudaError_t launchAdjointStep(const AdjointStepArgs& A, cudaStream_t st);
+cudaError_t launchLoss(const LossArgs& A, cudaStream_t st);
+cudaError_t launchAdjointSeed(const SeedArgs& A, cudaStream_t st);
+cudaError_t launchAdjointOut(const OutArgs& A, cudaStream_t st);
 
 cudaError_t launchHash(const HashArgs& A, uint32_t maxBlocks, cudaStream_t st);
 cudaError_t launchReorder(const ReorderArgs& A, cudaStream_t st);

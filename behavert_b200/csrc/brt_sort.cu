@@ -178,11 +178,12 @@ onesweepKernel(const uint2* __restrict__ in, uint2* __restrict__ out, uint32_t n
           const uint32_t v = ldRelaxed(&status[(size_t)p * BINS + d]);
           const uint32_t f = v & kFlagMask;
           if (f == 0u) {
+            // Plain bounded polling: a predecessor that has claimed its tile
+            // is resident and publishes within microseconds.
             if (++spins > kLookbackSpinLimit) {
               atomicOr(errWord, kDevErrLookback);
               break;
             }
-            __nanosleep(32);
             continue;
           }
           excl += v & kValMask;

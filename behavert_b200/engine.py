@@ -198,6 +198,58 @@ class Engine:
         check(lib().brt_get_steer_force(self._h, ptr(out), BRT_MEM_HOST), "getSteerForce")
         return out
 
+    # -- differentiable rollout (no reference counterpart) -----------------------
+    def set_steering_weights(self, weights) -> None:
+        """Per-flock (separation, alignment, cohesion) weights, nflocks x 3."""
+        if isinstance(weights, np.ndarray) or not getattr(weights, "is_cuda", False):
+            weights = np.ascontiguousarray(np.asarray(weights, np.float32).reshape(-1, 3))
+        check(lib().brt_set_steering_weights(self._h, ptr(weights), self._where(weights)), "set_steering_weights")
+
+    def get_steering_weights(self) -> np.ndarray:
+        out = np.empty((len(self.flocks), 3), np.float32)
+        check(lib().brt_get_steering_weights(self._h, ptr(out), BRT_MEM_HOST), "get_steering_weights")
+        return out
+
+    def adjoint_forward(self, target_pos4, nsteps: int, checkpoint_every: int, dt: float) -> np.ndarray:
+        """Taped forward of nsteps steps; returns the FP64 loss of every flock
+        (mean squared minimum-image distance of final positions to targets)."""
+        if isinstance(target_pos4, np.ndarray):
+            t = np.zeros((self.num_agents, 4), np.float32)
+            t[:, :target_pos4.shape[1]] = target_pos4[:, :4]
+            target_pos4 = t
+        loss = np.empty(len(self.flocks), np.float64)
+        check(lib().brt_adjoint_forward(self._h, dt, nsteps, checkpoint_every, ptr(target_pos4),
+                                        self._where(target_pos4), ptr(loss)), "brt_adjoint_forward")
+        return loss
+
+    def adjoint_backward(self, loss_scale=None, gpos_T=None, gfwd_T=None, gacc_T=None) -> dict:
+        """Gradients of sum_f loss_scale[f] * loss_f (+ <g_T, final state>)
+        with respect to the initial state and the per-flock weights."""
+        n = self.num_agents
+        scale = None if loss_scale is None else np.ascontiguousarray(loss_scale, np.float64)
+        extras = []
+        for g in (gpos_T, gfwd_T, gacc_T):
+            if g is None:
+                extras.append(None)
+            else:
+                e = np.zeros((n, 4), np.float32)
+                e[:, :g.shape[1]] = g
+                extras.append(e)
+        out = {k: np.empty((n, 4), np.float32) for k in ("pos", "fwd", "vel", "acc")}
+        out["weights"] = np.empty((len(self.flocks), 3), np.float64)
+        check(lib().brt_adjoint_backward(self._h, ptr(scale), ptr(extras[0]), ptr(extras[1]), ptr(extras[2]),
+                                         BRT_MEM_HOST, ptr(out["pos"]), ptr(out["fwd"]), ptr(out["vel"]),
+                                         ptr(out["acc"]), ptr(out["weights"]), BRT_MEM_HOST), "brt_adjoint_backward")
+        return out
+
+    def adjoint_tape(self, nsteps: int):
+        """Frozen lists (T x N x stride, neighbour agent ids) and flag words
+        (T x N x 4) of the last backward (needs option adjoint_export)."""
+        lists = np.empty((nsteps, self.num_agents, self.list_stride), np.uint32)
+        flags = np.empty((nsteps, self.num_agents, 4), np.uint32)
+        check(lib().brt_adjoint_get_tape(self._h, ptr(lists), ptr(flags), BRT_MEM_HOST), "brt_adjoint_get_tape")
+        return lists, flags
+
 
 def radix_sort_pairs(pairs_in, pairs_out, n: int, bits: int, scratch, stream: Optional[int] = None) -> None:
     """Standalone onesweep sort of uint2 (key, value) pairs on device memory."""

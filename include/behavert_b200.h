@@ -218,6 +218,53 @@ int brt_engine_record_lists(brt_engine* e, int enable);
    fired inside a kernel; cleared by this call. */
 int brt_engine_check_device_error(brt_engine* e, uint32_t* word);
 
+/* ---- differentiable rollout ---------------------------------------------------
+   No counterpart in the reference (BehaveRT has no differentiation).
+   Neighbour sets and branch decisions (inBoidNeighborhood memberships, the
+   adjustRawSteeringForce low-speed and deviation-limit branches, the two
+   truncateLength clips) are frozen per step; the gradient is that of the FP32
+   forward through those fixed choices.  Supported: flocking, static sphere
+   obstacles and integration; kNN lists, use2DProjection, feature clustering
+   steering and maxNeighbors > 32 return BRT_ERR_CONFIG.
+
+   brt_adjoint_forward runs nsteps fused steps from the current state,
+   checkpointing the state every checkpoint_every steps, and evaluates
+       loss_f = (1 / n_f) sum_{i in flock f} |minimum image(p_i(T) - target_i)|^2
+   in FP64 (target_pos4: float4 per agent in agent-id order).  loss_per_flock
+   (nflocks doubles, may be NULL) follows `where`.  The engine is left at the
+   final state.
+
+   brt_adjoint_backward propagates the adjoint of
+       sum_f loss_scale[f] * loss_f  (+ <g*_T, final state> for the optional
+       id-ordered adjoints gpos4_T / gfwd4_T (xyz forward, w speed) / gacc4_T)
+   back through the taped forward, recomputing hash, sort and neighbour lists
+   of each checkpoint segment.  loss_scale: host array of nflocks doubles or
+   NULL for 1.  Outputs (float4 per agent, agent-id order, each may be NULL):
+   grad_pos4 = dL/dposition(0), grad_fwd4 = dL/dforward(0) (w = dL/dspeed),
+   grad_vel4 = dL/dvelocity(0) with velocity = forward * speed,
+   grad_acc4 = dL/dsmoothed acceleration(0); grad_weights = dL/d(separation,
+   alignment, cohesion weight) per flock (nflocks x 3 doubles, reduced in
+   FP64).  The engine is left at the forward's final state. */
+int brt_adjoint_forward(brt_engine* e, float elapsedTime, uint32_t nsteps, uint32_t checkpoint_every,
+                        const float* target_pos4, int where, double* loss_per_flock);
+int brt_adjoint_backward(brt_engine* e, const double* loss_scale,
+                         const float* gpos4_T, const float* gfwd4_T, const float* gacc4_T, int where_in,
+                         float* grad_pos4, float* grad_fwd4, float* grad_vel4, float* grad_acc4,
+                         double* grad_weights, int where_out);
+/* With option "adjoint_export" set before brt_adjoint_forward, the backward
+   also writes, for every step t and agent id, the frozen neighbour list
+   (count, then neighbour agent ids; stride brt_neighbor_list_stride) and
+   four flag words: branch bits (1 low-speed adjust, 2 deviation limited,
+   4 force clipped, 8 velocity clipped) and the separation, alignment and
+   cohesion membership masks over list positions.  Sizes: nsteps * N *
+   stride and nsteps * N * 4 uint32. */
+int brt_adjoint_get_tape(brt_engine* e, uint32_t* lists_by_id, uint32_t* flags_by_id, int where);
+/* Per-flock steering weights (separationParams[0], alignmentParams[0],
+   cohesionParams[0]; nflocks x 3 floats).  Setting them does not invalidate
+   captured step graphs (the kernels read them from device memory). */
+int brt_set_steering_weights(brt_engine* e, const float* weights3, int where);
+int brt_get_steering_weights(brt_engine* e, float* weights3, int where);
+
 /* ---- standalone key/value radix sort (BehaveRT::RadixSort replacement) ----
    Stable LSD onesweep sort with decoupled look-back of `n` (key, value) pairs
    (uint2: key in .x, value in .y) on the low `bits` bits of the key.

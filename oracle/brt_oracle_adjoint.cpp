@@ -125,9 +125,9 @@ void stepAgent(uint32_t i, const std::vector<Agent>& S, const uint32_t* list, co
     } else {
       const double cosA = dot(A.f, o * (1.0 / dist));
       const double minR = p.commonSensingMinRadius;
-      is = p.separationParams[0] != 0 && inBoid(dist, cosA, minR, p.separationParams[1], p.separationParams[2]);
-      ia = p.alignmentParams[0] != 0 && inBoid(dist, cosA, minR, p.alignmentParams[1], p.alignmentParams[2]);
-      ic = p.cohesionParams[0] != 0 && inBoid(dist, cosA, minR, p.cohesionParams[1], p.cohesionParams[2]);
+      is = inBoid(dist, cosA, minR, p.separationParams[1], p.separationParams[2]);
+      ia = inBoid(dist, cosA, minR, p.alignmentParams[1], p.alignmentParams[2]);
+      ic = inBoid(dist, cosA, minR, p.cohesionParams[1], p.cohesionParams[2]);
     }
     if (is) { sum[0] += o / (-d2); ++r.cnt[0]; r.mS |= 1u << k; }
     if (ia) { sum[1] += B.f; ++r.cnt[1]; r.mA |= 1u << k; }
@@ -138,8 +138,10 @@ void stepAgent(uint32_t i, const std::vector<Agent>& S, const uint32_t* list, co
   r.xs[2] = r.cnt[2] ? sum[2] / (double)r.cnt[2] - A.p : d3(0, 0, 0);
   D3 steer = d3(0, 0, 0);
   for (int b = 0; b < 3; ++b) {
+    // Memberships do not depend on the weight; a zero weight only drops the
+    // term from the force, as the reference's `if (weight != 0)` does.
     r.on[b] = r.cnt[b] > 0;
-    if (r.on[b]) steer += normalize(r.xs[b]) * F.w[b];
+    if (r.on[b] && F.w[b] != 0) steer += normalize(r.xs[b]) * F.w[b];
   }
   if (p.numObstacles && p.obstacleAvoidanceWeight != 0) {
     D3 s = d3(0, 0, 0);
