@@ -119,6 +119,7 @@ _SIGS = {
     "brt_get_steer_force": (C.c_int, [_vp, _vp, C.c_int]),
     "brt_engine_record_lists": (C.c_int, [_vp, C.c_int]),
     "brt_engine_check_device_error": (C.c_int, [_vp, _u32p]),
+    "brt_engine_autotune": (C.c_int, [_vp, C.c_float, C.c_uint32, C.c_char_p, C.c_size_t]),
     "brt_adjoint_forward": (C.c_int, [_vp, C.c_float, C.c_uint32, C.c_uint32, _vp, C.c_int, _vp]),
     "brt_adjoint_backward": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_int]),
     "brt_adjoint_get_tape": (C.c_int, [_vp, _vp, _vp, C.c_int]),

@@ -55,10 +55,44 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
     return LIB
 
 
+def torch_ext_path() -> Path:
+    import sysconfig
+    return PKG / ("_brt_torch" + sysconfig.get_config_var("EXT_SUFFIX"))
+
+
+def build_torch_ext(force: bool = False) -> Path:
+    """Builds the libtorch autograd binding (csrc/torch_adjoint.cpp) in-tree,
+    linked against libbehavert_b200.so and the installed torch."""
+    import sysconfig
+    import torch
+    from torch.utils import cpp_extension as ce
+    target = torch_ext_path()
+    src = CSRC / "torch_adjoint.cpp"
+    deps = [src, ROOT / "include" / "behavert_b200.h", LIB, Path(__file__)]
+    if not force and not _stale(target, deps):
+        return target
+    abi = int(torch.compiled_with_cxx11_abi())
+    cmd = ["g++", "-shared", "-fPIC", "-O2", "-std=c++17", str(src), "-o", str(target),
+           "-DTORCH_EXTENSION_NAME=_brt_torch", "-DTORCH_API_INCLUDE_EXTENSION_H", f"-D_GLIBCXX_USE_CXX11_ABI={abi}",
+           "-I", sysconfig.get_paths()["include"], "-I", "/usr/local/cuda/include"]
+    for inc in ce.include_paths():
+        cmd += ["-isystem", inc]
+    for libdir in ce.library_paths():
+        cmd += ["-L", libdir, f"-Wl,-rpath,{libdir}"]
+    cmd += ["-lc10", "-lc10_cuda", "-ltorch", "-ltorch_cpu", "-ltorch_python",
+            "-L", str(PKG), "-lbehavert_b200", "-Wl,-rpath,$ORIGIN"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError("building the torch extension failed")
+    return target
+
+
 def build_oracle(force: bool = False) -> Path:
     """Builds the CPU oracle (test infrastructure) under oracle/_build/."""
     target = ROOT / "oracle" / "_build" / "liboracle_brt.so"
-    deps = [ROOT / "oracle" / "brt_oracle.cpp", ROOT / "include" / "behavert_b200.h"]
+    deps = [ROOT / "oracle" / "brt_oracle.cpp", ROOT / "oracle" / "brt_oracle_adjoint.cpp",
+            ROOT / "include" / "behavert_b200.h"]
     if not force and not _stale(target, deps):
         return target
     res = subprocess.run(["make", "-C", str(ROOT / "oracle")], capture_output=True, text=True)
@@ -70,5 +104,6 @@ def build_oracle(force: bool = False) -> Path:
 
 if __name__ == "__main__":
     build_library(force="--force" in sys.argv, verbose="-v" in sys.argv)
+    build_torch_ext(force="--force" in sys.argv)
     build_oracle(force="--force" in sys.argv)
     print(LIB)

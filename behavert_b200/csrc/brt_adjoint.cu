@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(kAdjointThreads) adjointStepKernel(AdjointStep
       u[b] = cnt[b] ? normalize3(x[b]) : x[b];
       if (w[b] != 0.0f) steer = add3(mul3(u[b], w[b]), steer);
     }
-    if (fl.numObstacles && fl.obsW != 0.0f) steer = obstacleSteer(a, fl, A.obstacles, steer);
+    if (fl.numObstacles && fl.obsW != 0.0f) steer = obstacleSteer(a, fl, A.obstacles, A.obsMask, steer);
 
     f3 gSteer = mk3(0.f, 0.f, 0.f);
     f3 selfP = xyz(gOp), selfF = mk3(0.f, 0.f, 0.f), selfA = xyz(gOa);
@@ -225,7 +225,8 @@ __global__ void __launch_bounds__(kAdjointThreads) adjointStepKernel(AdjointStep
     if (fl.numObstacles && fl.obsW != 0.0f) {
       const f3 g = mul3(gSteer, fl.obsW);
       const float L = fl.L, hL = 0.5f * fl.L;
-      for (uint32_t o = 0; o < fl.numObstacles; ++o) {
+      for (uint64_t bits = obstacleBits(a, fl, A.obsMask); bits; bits &= bits - 1ull) {
+        const uint32_t o = (uint32_t)__ffsll((long long)bits) - 1u;
         const float4 c = __ldg(&A.obstacles[fl.obsBase + o]);
         f3 off = sub3(a.pos, xyz(c));
         if (off.x > hL) off.x = off.x - L; else if (off.x < -hL) off.x = off.x + L;

@@ -229,7 +229,7 @@ int enqueueBackward(brt_engine* e, uint32_t variant) {
       R.posS = a->tPos + s * n; R.fwdS = a->tFwd + s * n; R.accS = a->tAcc + s * n;
       R.lists = a->tLists + s * n * e->listStride; R.listStride = e->listStride;
       R.prev = a->tPrev + s * n; R.idS = a->tId + s * n;
-      R.flocks = e->flocks; R.agentBase = e->agentBase; R.obstacles = e->obstacles;
+      R.flocks = e->flocks; R.agentBase = e->agentBase; R.obstacles = e->obstacles; R.obsMask = e->obsMask;
       R.nflocks = e->nflocks; R.n = e->N; R.dt = a->dt;
       R.gOutP = a->g[cur][0]; R.gOutF = a->g[cur][1]; R.gOutA = a->g[cur][2];
       R.gInP = a->g[cur ^ 1][0]; R.gInF = a->g[cur ^ 1][1]; R.gInA = a->g[cur ^ 1][2];

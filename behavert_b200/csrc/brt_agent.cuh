@@ -388,14 +388,30 @@ __device__ __forceinline__ f3 clusteringSteer(const AgentCtx& a, const FlockDev&
   return steer;
 }
 
+// Bits of the obstacles (by index within the flock) that can reach the
+// agent's cell: the per-cell obstacle field built on the grid by the host
+// (a superset of the obstacles with d < reach for any position in the cell),
+// or every obstacle when the engine has no field.
+__device__ __forceinline__ uint64_t obstacleBits(const AgentCtx& a, const FlockDev& fl, const uint2* __restrict__ obsMask) {
+  if (obsMask) {
+    const uint2 m = __ldg(&obsMask[fl.cellBase + ((uint32_t)a.g[2] * fl.G + (uint32_t)a.g[1]) * fl.G + (uint32_t)a.g[0]]);
+    return ((uint64_t)m.y << 32) | m.x;
+  }
+  return fl.numObstacles >= 64 ? ~0ull : ((1ull << fl.numObstacles) - 1ull);
+}
+
 // Static sphere obstacles: flee every sphere whose centre is closer than
-// radius + commonSearchRadius (minimum-image offset), linear falloff to zero
-// at that distance, weight obstacleAvoidanceWeight.  No reference counterpart
-// (nearest analogue moveAwayFromTarget_kernel, OpenSteerWrapper_kernel.cu:185-212).
-__device__ __forceinline__ f3 obstacleSteer(const AgentCtx& a, const FlockDev& fl, const float4* __restrict__ obstacles, f3 steer) {
+// radius + commonSearchRadius, linear falloff to zero there, weight
+// obstacleAvoidanceWeight (no reference counterpart; nearest analogue
+// moveAwayFromTarget_kernel, OpenSteerWrapper_kernel.cu:185-212).  The
+// obstacles are visited in index order; the ones the cell's field leaves
+// out contribute nothing, so the sum is the same as over all of them.
+__device__ __forceinline__ f3 obstacleSteer(const AgentCtx& a, const FlockDev& fl, const float4* __restrict__ obstacles,
+                                            const uint2* __restrict__ obsMask, f3 steer) {
   f3 s = mk3(0.f, 0.f, 0.f);
   const float L = fl.L, hL = 0.5f * fl.L;
-  for (uint32_t o = 0; o < fl.numObstacles; ++o) {
+  for (uint64_t bits = obstacleBits(a, fl, obsMask); bits; bits &= bits - 1ull) {
+    const uint32_t o = (uint32_t)__ffsll((long long)bits) - 1u;
     const float4 c = __ldg(&obstacles[fl.obsBase + o]);
     f3 off = sub3(a.pos, xyz(c));
     if (off.x > hL) off.x = off.x - L; else if (off.x < -hL) off.x = off.x + L;

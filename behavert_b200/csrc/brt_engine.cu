@@ -99,6 +99,47 @@ static FlockDev toDev(const brt_params& p, uint32_t G) {
   return d;
 }
 
+// Distance on a circle of circumference L from c to the arc [a, b].
+static double arcGap(double c, double a, double b, double L) {
+  double t = std::fmod(c - a, L);
+  if (t < 0) t += L;
+  if (t <= b - a) return 0.0;
+  auto circ = [L](double x) { x = std::fmod(std::fabs(x), L); return std::min(x, L - x); };
+  return std::min(circ(c - a), circ(c - b));
+}
+
+// The obstacle field of one flock on its EnvGrid3D grid: bit o of a cell's
+// mask is set when obstacle o's reach (radius + commonSearchRadius, as the
+// kernels compute it in float) comes within a small margin of the cell's box
+// under the periodic wrap, so the set is a superset of the obstacles that
+// any position in the cell can feel.  Entries are at the flock's global
+// cell indices.
+static void buildObstacleField(const brt_params& p, const FlockDev& d, std::vector<uint2>& mask) {
+  const double L = d.L, cell = d.cell;
+  for (uint32_t c = 0; c < d.C; ++c) mask[d.cellBase + c] = make_uint2(0u, 0u);
+  std::vector<double> gap[3];
+  for (uint32_t o = 0; o < p.numObstacles; ++o) {
+    const float reachF = p.obstacles[o][3] + p.commonSearchRadius;
+    const double reach = (double)reachF + 1e-3 + 1e-5 * L;
+    for (int ax = 0; ax < 3; ++ax) {
+      gap[ax].assign(d.G, 0.0);
+      for (uint32_t g = 0; g < d.G; ++g) gap[ax][g] = arcGap(p.obstacles[o][ax], g * cell, (g + 1) * cell, L);
+    }
+    for (uint32_t gz = 0; gz < d.G; ++gz) {
+      if (gap[2][gz] > reach) continue;
+      for (uint32_t gy = 0; gy < d.G; ++gy) {
+        if (gap[1][gy] > reach) continue;
+        for (uint32_t gx = 0; gx < d.G; ++gx) {
+          const double q = gap[0][gx] * gap[0][gx] + gap[1][gy] * gap[1][gy] + gap[2][gz] * gap[2][gz];
+          if (gap[0][gx] > reach || q > reach * reach) continue;
+          uint2& m = mask[d.cellBase + (gz * d.G + gy) * d.G + gx];
+          if (o < 32) m.x |= 1u << o; else m.y |= 1u << (o - 32);
+        }
+      }
+    }
+  }
+}
+
 }  // namespace brt
 
 using namespace brt;
@@ -114,7 +155,7 @@ void freeAll(brt_engine* e) {
   for (int r = 0; r < brt_engine::kRing; ++r)
     for (int k = 0; k < 5; ++k)
       if (e->ev[r][k]) cudaEventDestroy(e->ev[r][k]);
-  void* ptrs[] = {e->flocks, e->agentBase, e->obstacles, e->posA, e->fwdA, e->accA, e->posS, e->fwdS, e->accS,
+  void* ptrs[] = {e->flocks, e->agentBase, e->obstacles, e->obsMask, e->posA, e->fwdA, e->accA, e->posS, e->fwdS, e->accS,
                   e->featA, e->featS, e->featNormS, e->idA, e->idS, e->statsById, e->steer, e->lists, e->pairs[0], e->pairs[1],
                   e->cellStart, e->cellEnd, e->sortMem, e->errWord, e->stage4, e->stageF};
   for (void* p : ptrs)
@@ -143,7 +184,7 @@ StageArgs stageArgs(brt_engine* e) {
   A.posA = e->posA; A.fwdA = e->fwdA; A.accA = e->accA; A.featA = e->featA; A.idA = e->idA;
   A.statsById = e->statsById; A.steer = e->steer;
   A.cellStart = e->cellStart; A.cellEnd = e->cellEnd;
-  A.flocks = e->flocks; A.agentBase = e->agentBase; A.obstacles = e->obstacles;
+  A.flocks = e->flocks; A.agentBase = e->agentBase; A.obstacles = e->obstacles; A.obsMask = e->obsMask;
   A.lists = e->lists; A.listStride = e->listStride;
   A.nflocks = e->nflocks; A.n = e->N; A.Fs = e->Fs;
   return A;
@@ -211,7 +252,7 @@ int enqueueStep(brt_engine* e, float dt, bool record) {
   F.posA = e->posA; F.fwdA = e->fwdA; F.accA = e->accA; F.featA = e->featA; F.idA = e->idA;
   F.statsById = e->statsById;
   F.cellStart = e->cellStart; F.cellEnd = e->cellEnd;
-  F.flocks = e->flocks; F.agentBase = e->agentBase; F.obstacles = e->obstacles;
+  F.flocks = e->flocks; F.agentBase = e->agentBase; F.obstacles = e->obstacles; F.obsMask = e->obsMask;
   F.lists = record ? e->lists : nullptr; F.listStride = e->listStride;
   F.nflocks = e->nflocks; F.n = e->N; F.Mmax = e->Mmax; F.Fs = e->Fs; F.dt = dt;
   F.scanVariant = e->scanVariant;
@@ -220,7 +261,7 @@ int enqueueStep(brt_engine* e, float dt, bool record) {
   bool twoPass = e->anyKnn || e->forceTwoPass;
   for (const FlockDev& d : e->flocksHost) twoPass = twoPass || (d.F > 0 && (d.clus != 0.0f || d.aclus != 0.0f));
   if (twoPass) BRT_CUDA_TRY(launchFused(F, e->anyKnn, e->stream));
-  else BRT_CUDA_TRY(launchFlock(F, e->phase2Variant, e->stream));
+  else BRT_CUDA_TRY(launchFlock(F, e->phase2Variant, e->fusedBlock, e->stream));
   if (timed) {
     if ((rc = stageMark(e, 4))) return rc;
     e->pending[e->ringPos] = true;
@@ -390,6 +431,7 @@ int brt_engine_create(const brt_params* flocks, uint32_t num_flocks, int device,
   chk(devAlloc(&e->flocks, num_flocks));
   chk(devAlloc(&e->agentBase, num_flocks + 1));
   chk(devAlloc(&e->obstacles, std::max<size_t>(1, obs.size())));
+  if (!obs.empty()) chk(devAlloc(&e->obsMask, e->C));
   chk(devAlloc(&e->posA, n)); chk(devAlloc(&e->fwdA, n)); chk(devAlloc(&e->accA, n));
   chk(devAlloc(&e->posS, n)); chk(devAlloc(&e->fwdS, n)); chk(devAlloc(&e->accS, n));
   chk(devAlloc(&e->featA, n * e->Fs)); chk(devAlloc(&e->featS, n * e->Fs));
@@ -410,7 +452,13 @@ int brt_engine_create(const brt_params* flocks, uint32_t num_flocks, int device,
   cudaStream_t st = e->stream;
   BRT_CUDA_TRY(cudaMemcpyAsync(e->flocks, e->flocksHost.data(), sizeof(FlockDev) * num_flocks, cudaMemcpyHostToDevice, st));
   BRT_CUDA_TRY(cudaMemcpyAsync(e->agentBase, agentBase.data(), 4 * (num_flocks + 1), cudaMemcpyHostToDevice, st));
-  if (!obs.empty()) BRT_CUDA_TRY(cudaMemcpyAsync(e->obstacles, obs.data(), sizeof(float4) * obs.size(), cudaMemcpyHostToDevice, st));
+  if (!obs.empty()) {
+    BRT_CUDA_TRY(cudaMemcpyAsync(e->obstacles, obs.data(), sizeof(float4) * obs.size(), cudaMemcpyHostToDevice, st));
+    std::vector<uint2> field(e->C, make_uint2(0u, 0u));
+    for (uint32_t f = 0; f < num_flocks; ++f) buildObstacleField(flocks[f], e->flocksHost[f], field);
+    BRT_CUDA_TRY(cudaMemcpyAsync(e->obsMask, field.data(), sizeof(uint2) * field.size(), cudaMemcpyHostToDevice, st));
+    BRT_CUDA_TRY(cudaStreamSynchronize(st));
+  }
   BRT_CUDA_TRY(cudaMemsetAsync(e->sortMem, 0, sortBytes, st));
   BRT_CUDA_TRY(cudaMemsetAsync(e->errWord, 0, 4, st));
   if (n) {
@@ -484,6 +532,13 @@ int brt_engine_set_params(brt_engine* e, uint32_t flock, const brt_params* p) {
     obs.push_back(make_float4(p->obstacles[k][0], p->obstacles[k][1], p->obstacles[k][2], p->obstacles[k][3]));
   if (!obs.empty())
     BRT_CUDA_TRY(cudaMemcpyAsync(e->obstacles + d.obsBase, obs.data(), sizeof(float4) * obs.size(), cudaMemcpyHostToDevice, e->stream));
+  std::vector<uint2> field;
+  if (e->obsMask) {
+    field.assign(e->C, make_uint2(0u, 0u));
+    buildObstacleField(*p, d, field);
+    BRT_CUDA_TRY(cudaMemcpyAsync(e->obsMask + d.cellBase, field.data() + d.cellBase, sizeof(uint2) * d.C,
+                                 cudaMemcpyHostToDevice, e->stream));
+  }
   BRT_CUDA_TRY(cudaStreamSynchronize(e->stream));
   for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second);
   e->graphs.clear();
@@ -502,6 +557,12 @@ int brt_engine_set_option(brt_engine* e, const char* key, int64_t value) {
   } else if (k == "scan_variant") {
     if (value < 0 || value > 3) { setLastError("scan_variant must be in [0, 3]"); return BRT_ERR_ARG; }
     e->scanVariant = (int)value;
+  } else if (k == "block_size") {
+    if (value < 32 || value > (int64_t)kFlockMaxThreads || value % 32) {
+      setLastError("block_size must be a multiple of 32 in [32, 256]");
+      return BRT_ERR_ARG;
+    }
+    e->fusedBlock = (uint32_t)value;
   } else if (k == "adjoint_graphs") {
     e->adjointGraphs = value != 0;
   } else if (k == "adjoint_export") {
@@ -696,6 +757,124 @@ int brt_engine_stage_times(brt_engine* e, double* ms4, uint64_t* steps, uint32_t
   if (launches_per_step) *launches_per_step = 3 + e->plan.passes;
   e->stageMs[0] = e->stageMs[1] = e->stageMs[2] = e->stageMs[3] = 0;
   e->timedSteps = 0;
+  return BRT_OK;
+}
+
+int brt_engine_autotune(brt_engine* e, float elapsedTime, uint32_t steps, char* report, size_t report_len) {
+  if (!e || steps == 0) return BRT_ERR_ARG;
+  if (e->N == 0) return BRT_OK;
+  DeviceGuard guard(e->device);
+  cudaStream_t st = e->stream;
+  const size_t n = e->N;
+  BRT_CUDA_TRY(cudaStreamSynchronize(st));
+  // Snapshot of the canonical state: every trial starts from it, and the
+  // engine is left in it.
+  float4 *sp = nullptr, *sf = nullptr, *sa = nullptr, *ss = nullptr;
+  uint32_t* si = nullptr;
+  float* sx = nullptr;
+  int rc = BRT_OK;
+  auto chk = [&](int r) { if (r && !rc) rc = r; };
+  chk(devAlloc(&sp, n)); chk(devAlloc(&sf, n)); chk(devAlloc(&sa, n)); chk(devAlloc(&ss, n)); chk(devAlloc(&si, n));
+  chk(devAlloc(&sx, n * e->Fs));
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  if (!rc && (cudaEventCreate(&t0) != cudaSuccess || cudaEventCreate(&t1) != cudaSuccess)) {
+    setLastError("event creation failed");
+    rc = BRT_ERR_CUDA;
+  }
+  auto copyAll = [&](bool save) -> cudaError_t {
+    cudaError_t c = cudaSuccess;
+    auto cp = [&](void* dst, const void* src, size_t bytes) {
+      if (c == cudaSuccess && bytes) c = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, st);
+    };
+    if (save) {
+      cp(sp, e->posA, n * 16); cp(sf, e->fwdA, n * 16); cp(sa, e->accA, n * 16); cp(ss, e->statsById, n * 16);
+      cp(si, e->idA, n * 4); cp(sx, e->featA, n * e->Fs * 4);
+    } else {
+      cp(e->posA, sp, n * 16); cp(e->fwdA, sf, n * 16); cp(e->accA, sa, n * 16); cp(e->statsById, ss, n * 16);
+      cp(e->idA, si, n * 4); cp(e->featA, sx, n * e->Fs * 4);
+    }
+    return c;
+  };
+  if (!rc && copyAll(true) != cudaSuccess) { setLastError("autotune snapshot failed"); rc = BRT_ERR_CUDA; }
+  // One trial: the steps-step graph launched twice from the snapshot, the
+  // faster launch counted.
+  auto measure = [&](double* msPerStep) -> int {
+    cudaGraphExec_t ge = nullptr;
+    int r = getGraph(e, elapsedTime, steps, false, &ge);
+    if (r) return r;
+    double best = 1e30;
+    for (int rep = 0; rep < 2; ++rep) {
+      BRT_CUDA_TRY(copyAll(false));
+      BRT_CUDA_TRY(cudaEventRecord(t0, st));
+      BRT_CUDA_TRY(cudaGraphLaunch(ge, st));
+      BRT_CUDA_TRY(cudaEventRecord(t1, st));
+      BRT_CUDA_TRY(cudaEventSynchronize(t1));
+      float ms = 0.0f;
+      BRT_CUDA_TRY(cudaEventElapsedTime(&ms, t0, t1));
+      best = std::min(best, (double)ms / steps);
+    }
+    if ((r = checkDeviceError(e, true))) return r;
+    *msPerStep = best;
+    return BRT_OK;
+  };
+  bool twoPass = e->anyKnn || e->forceTwoPass;
+  for (const FlockDev& d : e->flocksHost) twoPass = twoPass || (d.F > 0 && (d.clus != 0.0f || d.aclus != 0.0f));
+  std::string log;
+  char buf[256];
+  auto trial = [&](const char* what, int64_t v, double* ms) -> int {
+    int r = measure(ms);
+    std::snprintf(buf, sizeof(buf), "%s{\"%s\": %lld, \"ms_per_step\": %.6f}", log.empty() ? "" : ", ", what, (long long)v, *ms);
+    log += buf;
+    return r;
+  };
+  // Coordinate descent: radix digit width, then block size x scan loop
+  // shape, then the list-walk variant (the last two only when the
+  // single-pass kernel runs).
+  uint32_t bestBits = e->plan.digitBits;
+  double bestMs = 1e30, ms = 0.0;
+  for (uint32_t b = 4; b <= 8 && !rc; ++b) {
+    chk(brt_engine_set_option(e, "sort_digit_bits", b));
+    if (!rc) chk(trial("sort_digit_bits", b, &ms));
+    if (!rc && ms < bestMs) { bestMs = ms; bestBits = b; }
+  }
+  if (!rc) chk(brt_engine_set_option(e, "sort_digit_bits", bestBits));
+  uint32_t bestBlock = e->fusedBlock;
+  int bestScan = e->scanVariant, bestP2 = e->phase2Variant;
+  if (!twoPass) {
+    bestMs = 1e30;
+    const uint32_t blocks[3] = {64, 128, 256};
+    for (uint32_t bs : blocks)
+      for (int sv = 0; sv < 3 && !rc; ++sv) {
+        chk(brt_engine_set_option(e, "block_size", bs));
+        chk(brt_engine_set_option(e, "scan_variant", sv));
+        if (!rc) chk(trial(sv == 0 ? "block_size" : (sv == 1 ? "block_size/scan1" : "block_size/scan2"), bs, &ms));
+        if (!rc && ms < bestMs) { bestMs = ms; bestBlock = bs; bestScan = sv; }
+      }
+    if (!rc) { chk(brt_engine_set_option(e, "block_size", bestBlock)); chk(brt_engine_set_option(e, "scan_variant", bestScan)); }
+    for (int p2 = 0; p2 < 2 && !rc; ++p2) {
+      chk(brt_engine_set_option(e, "phase2_variant", p2));
+      if (!rc) chk(trial("phase2_variant", p2, &ms));
+      if (!rc && ms <= bestMs) { bestMs = ms; bestP2 = p2; }
+    }
+    if (!rc) chk(brt_engine_set_option(e, "phase2_variant", bestP2));
+  }
+  if (!rc && copyAll(false) != cudaSuccess) { setLastError("autotune restore failed"); rc = BRT_ERR_CUDA; }
+  if (!rc) cudaStreamSynchronize(st);
+  e->reordered = false;
+  e->listsValid = false;
+  if (t0) cudaEventDestroy(t0);
+  if (t1) cudaEventDestroy(t1);
+  for (void* p : {(void*)sp, (void*)sf, (void*)sa, (void*)ss, (void*)si, (void*)sx})
+    if (p) cudaFree(p);
+  if (rc) return rc;
+  if (report && report_len) {
+    std::snprintf(buf, sizeof(buf),
+                  "{\"sort_digit_bits\": %u, \"block_size\": %u, \"scan_variant\": %d, \"phase2_variant\": %d, "
+                  "\"ms_per_step\": %.6f, \"trials\": [",
+                  bestBits, bestBlock, bestScan, bestP2, bestMs);
+    std::string out = std::string(buf) + log + "]}";
+    std::snprintf(report, report_len, "%s", out.c_str());
+  }
   return BRT_OK;
 }
 

@@ -24,10 +24,12 @@ struct brt_engine {
   brt::FlockDev* flocks = nullptr;
   uint32_t* agentBase = nullptr;
   float4* obstacles = nullptr;
+  uint2* obsMask = nullptr;   // per-cell obstacle field (null when no flock has obstacles)
   bool anyKnn = false;
   bool forceTwoPass = false;  // option "two_pass": run the list-first kernel even when not needed
   int phase2Variant = 0;      // option "phase2_variant": list walk one or two neighbours at a time
   int scanVariant = 0;        // option "scan_variant": neighbour-scan loop shape
+  uint32_t fusedBlock = 128;  // option "block_size": threads per block of the single-pass flock kernel
   // state
   float4 *posA = nullptr, *fwdA = nullptr, *accA = nullptr, *posS = nullptr, *fwdS = nullptr, *accS = nullptr;
   float *featA = nullptr, *featS = nullptr, *featNormS = nullptr;

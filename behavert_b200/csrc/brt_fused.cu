@@ -35,7 +35,7 @@ __device__ __forceinline__ float shiftOf(uint32_t code, float L) {
 }
 
 template <int FP, int P2>
-__global__ void __launch_bounds__(kFusedThreads, 8) flockKernel(FusedArgs A) {
+__global__ void __launch_bounds__(kFlockMaxThreads, 4) flockKernel(FusedArgs A) {
   extern __shared__ uint32_t sList[];
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.n) return;
@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(kFusedThreads, 8) flockKernel(FusedArgs A) {
     if (cCoh > 0) sCoh = normalize3(sub3(div3(sCoh, (float)cCoh), p));
     steer = add3(mul3(sCoh, fl.coh[0]), steer);
   }
-  if (fl.numObstacles && fl.obsW != 0.0f) steer = obstacleSteer(a, fl, A.obstacles, steer);
+  if (fl.numObstacles && fl.obsW != 0.0f) steer = obstacleSteer(a, fl, A.obstacles, A.obsMask, steer);
   if (FP > 0) {
     if (relaxOn && n > 0 && sumS > 0.0f) {
 #pragma unroll
@@ -209,9 +209,9 @@ __global__ void __launch_bounds__(kFusedThreads, 8) flockKernel(FusedArgs A) {
 
 namespace {
 template <int FP>
-cudaError_t launchFlockFP(const FusedArgs& A, uint32_t blocks, size_t smem, int phase2, cudaStream_t st) {
-  if (phase2) flockKernel<FP, 1><<<blocks, kFusedThreads, smem, st>>>(A);
-  else flockKernel<FP, 0><<<blocks, kFusedThreads, smem, st>>>(A);
+cudaError_t launchFlockFP(const FusedArgs& A, uint32_t blocks, uint32_t block, size_t smem, int phase2, cudaStream_t st) {
+  if (phase2) flockKernel<FP, 1><<<blocks, block, smem, st>>>(A);
+  else flockKernel<FP, 0><<<blocks, block, smem, st>>>(A);
   return cudaGetLastError();
 }
 template <int FP>
@@ -223,21 +223,22 @@ cudaError_t configureFlockFP(int smem) {
 }  // namespace
 
 // phase2 != 0 walks the list two neighbours at a time with their loads issued
-// together.
-cudaError_t launchFlock(const FusedArgs& A, int phase2, cudaStream_t st) {
+// together.  block: threads per block, a multiple of 32 in [32, 256].
+cudaError_t launchFlock(const FusedArgs& A, int phase2, uint32_t block, cudaStream_t st) {
   if (A.n == 0) return cudaSuccess;
-  const uint32_t blocks = (A.n + kFusedThreads - 1) / kFusedThreads;
+  if (block < 32 || block > kFlockMaxThreads || block % 32) return cudaErrorInvalidValue;
+  const uint32_t blocks = (A.n + block - 1) / block;
   const uint32_t fp = A.Fs;
-  const size_t smem = (size_t)kFusedThreads * A.Mmax * 4;
-  if (fp == 0) return launchFlockFP<0>(A, blocks, smem, phase2, st);
-  if (fp <= 4) return launchFlockFP<4>(A, blocks, smem, phase2, st);
-  if (fp <= 8) return launchFlockFP<8>(A, blocks, smem, phase2, st);
-  if (fp <= 16) return launchFlockFP<16>(A, blocks, smem, phase2, st);
-  return launchFlockFP<32>(A, blocks, smem, phase2, st);
+  const size_t smem = (size_t)block * A.Mmax * 4;
+  if (fp == 0) return launchFlockFP<0>(A, blocks, block, smem, phase2, st);
+  if (fp <= 4) return launchFlockFP<4>(A, blocks, block, smem, phase2, st);
+  if (fp <= 8) return launchFlockFP<8>(A, blocks, block, smem, phase2, st);
+  if (fp <= 16) return launchFlockFP<16>(A, blocks, block, smem, phase2, st);
+  return launchFlockFP<32>(A, blocks, block, smem, phase2, st);
 }
 
 cudaError_t configureFlockKernels(uint32_t Mmax) {
-  const int smem = (int)((size_t)kFusedThreads * Mmax * 4);
+  const int smem = (int)((size_t)kFlockMaxThreads * Mmax * 4);
   cudaError_t e = cudaSuccess;
   if ((e = configureFlockFP<0>(smem))) return e;
   if ((e = configureFlockFP<4>(smem))) return e;

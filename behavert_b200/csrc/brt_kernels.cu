@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(kFusedThreads) fusedKernel(FusedArgs A) {
     steer = clusteringSteer(a, fl, list, ls, n, A.posS, A.fwdS, fi, norm1, A.featS, A.Fs, st, sims, steer);
     A.statsById[id] = st;
   }
-  if (fl.numObstacles && fl.obsW != 0.0f) steer = obstacleSteer(a, fl, A.obstacles, steer);
+  if (fl.numObstacles && fl.obsW != 0.0f) steer = obstacleSteer(a, fl, A.obstacles, A.obsMask, steer);
   if (F) {
     float fo[BRT_MAX_FEATUREDIM];
     relaxFeatures(fl, list, ls, n, fi, norm1, A.featS, A.Fs, fo);
@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(128) steerStageKernel(StageArgs A, int which) 
     steer = clusteringSteer(a, fl, lst + 1, 1, n, A.posS, A.fwdS, fi, norm1, A.featS, A.Fs, st, sims, steer);
     A.statsById[id] = st;
   }
-  if (which == 4 && fl.numObstacles && fl.obsW != 0.0f) steer = obstacleSteer(a, fl, A.obstacles, steer);
+  if (which == 4 && fl.numObstacles && fl.obsW != 0.0f) steer = obstacleSteer(a, fl, A.obstacles, A.obsMask, steer);
   A.steer[i] = make_float4(steer.x, steer.y, steer.z, 0.0f);
 }
 

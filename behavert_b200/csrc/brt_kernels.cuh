@@ -6,6 +6,7 @@
 namespace brt {
 
 constexpr uint32_t kFusedThreads = 128;
+constexpr uint32_t kFlockMaxThreads = 256;  // largest block of the single-pass flock kernel
 
 struct HashArgs {
   const float4* pos;           // canonical slot order
@@ -48,6 +49,7 @@ struct FusedArgs {
   const uint32_t* cellStart; const uint32_t* cellEnd;
   const FlockDev* flocks; const uint32_t* agentBase;
   const float4* obstacles;
+  const uint2* obsMask;          // per-cell obstacle field (global cell index) or null
   uint32_t* lists;             // optional, stride listStride
   uint32_t listStride;
   uint32_t nflocks, n, Mmax, Fs;
@@ -64,6 +66,7 @@ struct StageArgs {
   const uint32_t* cellStart; const uint32_t* cellEnd;
   const FlockDev* flocks; const uint32_t* agentBase;
   const float4* obstacles;
+  const uint2* obsMask;          // per-cell obstacle field (global cell index) or null
   uint32_t* lists;
   uint32_t listStride;
   uint32_t nflocks, n, Fs;
@@ -77,6 +80,7 @@ struct AdjointStepArgs {
   const uint32_t* prev;                                          // canonical slot of each sorted slot
   const uint32_t* idS;                                           // agent id per sorted slot
   const FlockDev* flocks; const uint32_t* agentBase; const float4* obstacles;
+  const uint2* obsMask;
   uint32_t nflocks, n;
   float dt;
   float4* gOutP; float4* gOutF; float4* gOutA;                   // output adjoint by sorted slot (zeroed)
@@ -115,7 +119,7 @@ cudaError_t launchAdjointOut(const OutArgs& A, cudaStream_t st);
 cudaError_t launchHash(const HashArgs& A, uint32_t maxBlocks, cudaStream_t st);
 cudaError_t launchReorder(const ReorderArgs& A, cudaStream_t st);
 cudaError_t launchFused(const FusedArgs& A, bool knn, cudaStream_t st);
-cudaError_t launchFlock(const FusedArgs& A, int phase2, cudaStream_t st);
+cudaError_t launchFlock(const FusedArgs& A, int phase2, uint32_t block, cudaStream_t st);
 cudaError_t launchLists(const StageArgs& A, bool knn, cudaStream_t st);
 cudaError_t launchSteerStage(const StageArgs& A, int which, cudaStream_t st);
 cudaError_t launchIntegrateStage(const StageArgs& A, float dt, cudaStream_t st);

@@ -246,7 +246,9 @@ SortPlan makeSortPlan(uint32_t n, uint32_t bits, uint32_t maxDigitBits) {
   p.n = n;
   p.bits = std::max(1u, std::min(bits, 32u));
   maxDigitBits = std::max(4u, std::min(maxDigitBits, 9u));
-  p.passes = (p.bits + maxDigitBits - 1) / maxDigitBits;
+  // At most 4 passes (the plan's shift table and the hash kernel's
+  // histograms): narrow digits on wide keys become wider digits.
+  p.passes = std::min(4u, (p.bits + maxDigitBits - 1) / maxDigitBits);
   p.digitBits = std::max(4u, (p.bits + p.passes - 1) / p.passes);
   p.bins = 1u << p.digitBits;
   p.tiles = (n + kSortTile - 1) / kSortTile;

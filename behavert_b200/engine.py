@@ -198,6 +198,14 @@ class Engine:
         check(lib().brt_get_steer_force(self._h, ptr(out), BRT_MEM_HOST), "getSteerForce")
         return out
 
+    def autotune(self, dt: float, steps: int = 10) -> dict:
+        """Times launch configurations on the current state, keeps the
+        fastest and returns the choice with every trial's ms per step."""
+        import json
+        buf = C.create_string_buffer(8192)
+        check(lib().brt_engine_autotune(self._h, dt, steps, buf, len(buf)), "brt_engine_autotune")
+        return json.loads(buf.value.decode())
+
     # -- differentiable rollout (no reference counterpart) -----------------------
     def set_steering_weights(self, weights) -> None:
         """Per-flock (separation, alignment, cohesion) weights, nflocks x 3."""

@@ -203,6 +203,7 @@ def batched_leg(device: int, steps: int = 100, loop_steps: int = 3):
     eng.set_state(w.pos, w.fwd, w.acc)
     stream = torch.cuda.ExternalStream(eng.stream_handle())
     eng.step(dt, 3)
+    tuned = eng.autotune(dt, steps=5)
     eng.step_prepare(dt, steps)
     eng.sync()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -243,7 +244,195 @@ def batched_leg(device: int, steps: int = 100, loop_steps: int = 3):
             "value": batched, "unit": UNIT, "ms_per_step": 1e3 * t_batched / steps, "steps": steps,
             "looped_value": looped, "looped_ms_per_step": 1e3 * t_loop / loop_steps,
             "looped": "one engine per flock, %d steps of plain per-step launches looped over the flocks" % loop_steps,
-            "speedup_vs_looped": batched / looped}
+            "speedup_vs_looped": batched / looped, "tuned": tuned}
+
+
+def _events_ms(stream, fn):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def adjoint_leg(device: int, reps: int = 5):
+    """Config 3: 65,536 agents, T=50, checkpoint every 10.  Device time of
+    the plain 50-step forward (one graph), the taped forward (checkpoints +
+    FP64 loss) and the backward (per segment: recompute hash/sort/lists,
+    reverse kernels), each the best of `reps`, on the engine's stream."""
+    import torch
+    from behavert_b200 import Engine, workloads
+    w = workloads.adjoint()
+    T, k, dt = w.steps, w.meta["checkpoint_every"], w.dt
+    hidden = np.asarray([w.meta["hidden"]], np.float32)
+    eng = Engine(w.params, device=device)
+    stream = torch.cuda.ExternalStream(eng.stream_handle())
+    eng.set_steering_weights(hidden)
+    eng.set_state(w.pos, w.meta["fwd_hidden"], w.acc)
+    eng.step(dt, T)
+    target = eng.get_state(features=False)[0]
+    eng.set_steering_weights(np.asarray([w.meta["trial"]], np.float32))
+    tuned = eng.autotune(dt, steps=10)
+    eng.step_prepare(dt, T)
+    t_plain, t_fwd, t_bwd = [], [], []
+    from behavert_b200._abi import BRT_MEM_DEVICE, check, lib, ptr
+    tgt = torch.from_numpy(target).to("cuda:%d" % device)
+    gw = torch.empty((1, 3), dtype=torch.float64, device=tgt.device)
+    loss = torch.empty(1, dtype=torch.float64, device=tgt.device)
+    h = eng.handle
+    for r in range(reps + 1):
+        eng.set_state(w.pos, w.fwd, w.acc)
+        eng.sync()
+        tp = _events_ms(stream, lambda: eng.step(dt, T))
+        eng.set_state(w.pos, w.fwd, w.acc)
+        eng.sync()
+        tf = _events_ms(stream, lambda: check(lib().brt_adjoint_forward(h, dt, T, k, ptr(tgt), BRT_MEM_DEVICE, ptr(loss)),
+                                              "adjoint_forward"))
+        tb = _events_ms(stream, lambda: check(lib().brt_adjoint_backward(h, None, None, None, None, BRT_MEM_DEVICE, None,
+                                                                         None, None, None, ptr(gw), BRT_MEM_DEVICE),
+                                              "adjoint_backward"))
+        eng.sync()
+        if r:  # the first round captures the graphs
+            t_plain.append(tp)
+            t_fwd.append(tf)
+            t_bwd.append(tb)
+    eng.close()
+    n = w.num_agents
+    tp, tf, tb = min(t_plain), min(t_fwd), min(t_bwd)
+    return {"workload": "config 3: %d agents, T=%d, checkpoint every %d, maxNeighbors 16" % (n, T, k),
+            "forward_value": n * T / (tp / 1e3), "unit": UNIT,
+            "adjoint_value": n * T / ((tf + tb) / 1e3),
+            "ms": {"plain_forward": tp, "taped_forward": tf, "backward": tb},
+            "cost_vs_forward": (tf + tb) / tp, "backward_vs_forward": tb / tp,
+            "loss": float(loss.item()), "grad_weights": gw.cpu().numpy()[0].tolist(), "tuned": tuned}
+
+
+def adjoint_accuracy(device: int):
+    """Config 3 gradients against the FP64 frozen-neighbour oracle (the CPU
+    checker): the FP64 reverse with the GPU's frozen lists and branches, and
+    central differences of the FP64 model at h=1e-4 (the specified step) and
+    h=1e-6 (converged) on the three weights."""
+    from behavert_b200 import Engine, workloads
+    from oracle import oracle
+    w = workloads.adjoint()
+    T, k, dt = w.steps, w.meta["checkpoint_every"], float(np.float32(w.dt))
+    with Engine(w.params, device=device) as eng:
+        eng.set_steering_weights(np.asarray([w.meta["hidden"]], np.float32))
+        eng.set_state(w.pos, w.meta["fwd_hidden"], w.acc)
+        eng.step(dt, T)
+        target = eng.get_state(features=False)[0]
+        eng.set_steering_weights(np.asarray([w.meta["trial"]], np.float32))
+        eng.set_option("adjoint_export", 1)
+        eng.set_state(w.pos, w.fwd, w.acc)
+        eng.adjoint_forward(target, T, k, dt)
+        g = eng.adjoint_backward()
+        lists, flags = eng.adjoint_tape(T)
+    L = float(w.params[0].worldSize)
+    n = w.num_agents
+    pos0, fwd0, acc0 = (a.astype(np.float64) for a in (w.pos, w.fwd, w.acc))
+    w0 = np.asarray([w.meta["trial"]], np.float64)
+
+    def loss_at(wts):
+        fin = oracle.frozen_forward(w.params, pos0, fwd0, acc0, lists, weights=wts, flags=flags, dt=dt)
+        d = oracle.min_image(fin["pos"][:, :3] - target[:, :3].astype(np.float64), L)
+        return float(np.mean(np.sum(d * d, axis=1))), d
+
+    _, d = loss_at(w0)
+    gT = np.zeros((n, 4))
+    gT[:, :3] = 2.0 * d / n
+    rev = oracle.frozen_reverse(w.params, pos0, fwd0, acc0, lists, gT, weights=w0, flags=flags, dt=dt)
+    f0, s0 = fwd0[:, :3], fwd0[:, 3]
+    gf, gs = rev["fwd"][:, :3], rev["fwd"][:, 3]
+    rev["vel"] = gs[:, None] * f0 + (gf - f0 * np.sum(f0 * gf, axis=1)[:, None]) / s0[:, None]
+    out = {"grad_weights_gpu": g["weights"][0].tolist(), "grad_weights_fp64_reverse": rev["weights"][0].tolist()}
+    nr = np.linalg.norm(rev["weights"][0])
+    out["weights_rel_err_vs_fp64_reverse"] = float(np.linalg.norm(g["weights"][0] - rev["weights"][0]) / nr)
+    for h in (1e-4, 1e-6):
+        fd = np.zeros(3)
+        for b in range(3):
+            wp, wm = w0.copy(), w0.copy()
+            wp[0, b] += h
+            wm[0, b] -= h
+            fd[b] = (loss_at(wp)[0] - loss_at(wm)[0]) / (2 * h)
+        out["fd_h%g" % h] = fd.tolist()
+        out["weights_rel_err_gpu_vs_fd_h%g" % h] = float(np.linalg.norm(g["weights"][0] - fd) / np.linalg.norm(fd))
+        out["weights_rel_err_fp64_reverse_vs_fd_h%g" % h] = float(np.linalg.norm(rev["weights"][0] - fd) / np.linalg.norm(fd))
+    for key in ("pos", "vel"):
+        a, b = g[key][:, :3].astype(np.float64), rev[key][:, :3]
+        rel = np.linalg.norm(a - b, axis=1) / np.linalg.norm(b, axis=1)
+        out[key + "_grad_rel_err"] = {"median": float(np.median(rel)), "p99": float(np.quantile(rel, 0.99)),
+                                      "normwise": float(np.linalg.norm(a - b) / np.linalg.norm(b))}
+    return out
+
+
+def fitting_leg(device: int, iters: int = 200):
+    """Config 4: per-flock steering weights of 256 flocks (with 32 sphere
+    obstacles each) fitted by Adam (lr 0.05) through the batched adjoint
+    (libtorch autograd function), against the same iteration run one engine
+    per flock."""
+    import torch
+    from behavert_b200 import Engine, workloads
+    from behavert_b200.autograd import flock_loss
+    w = workloads.fitting()
+    T, k, dt = w.steps, 10, w.dt
+    hidden = np.asarray(w.meta["hidden"], np.float32)
+    nf = len(w.params)
+    dev = torch.device("cuda:%d" % device)
+    eng = Engine(w.params, device=device)
+    eng.set_steering_weights(hidden)
+    eng.set_state(w.pos, w.fwd, w.acc)
+    eng.step(dt, T)
+    tgt = torch.tensor(eng.get_state(features=False)[0][:, :3], device=dev)
+    tuned = eng.autotune(dt, steps=5)
+    pos0 = torch.tensor(w.pos[:, :3], device=dev)
+    vel0 = torch.tensor(w.fwd[:, :3] * w.fwd[:, 3:4], device=dev)
+    wt = torch.ones((nf, 3), device=dev, requires_grad=True)
+    opt = torch.optim.Adam([wt], lr=w.meta["lr"])
+    losses = []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for it in range(iters):
+        opt.zero_grad()
+        loss = flock_loss(eng, wt, pos0, vel0, tgt, dt, T, k)
+        loss.sum().backward()
+        opt.step()
+        if it in (0, iters - 1):
+            losses.append(float(loss.sum()))
+    torch.cuda.synchronize()
+    t_fit = time.perf_counter() - t0
+    eng.close()
+    err = np.abs(wt.detach().cpu().numpy() - hidden)
+    rel = np.linalg.norm(wt.detach().cpu().numpy() - hidden, axis=1) / np.linalg.norm(hidden, axis=1)
+    # the same iteration, one engine per flock (first iteration per engine
+    # captures its graphs and is not timed)
+    sizes = np.asarray(w.meta["sizes"])
+    bounds = np.concatenate([[0], np.cumsum(sizes)])
+    t_loop = 0.0
+    for f in range(nf):
+        a, b = int(bounds[f]), int(bounds[f + 1])
+        e1 = Engine([w.params[f]], device=device)
+        wf = torch.ones((1, 3), device=dev, requires_grad=True)
+        for r in range(2):
+            torch.cuda.synchronize()
+            ts = time.perf_counter()
+            lf = flock_loss(e1, wf, pos0[a:b], vel0[a:b], tgt[a:b], dt, T, k)
+            lf.sum().backward()
+            torch.cuda.synchronize()
+            if r:
+                t_loop += time.perf_counter() - ts
+        e1.close()
+    return {"workload": "config 4: %d flocks, %d agents, 32 sphere obstacles per flock (weight 2), T=%d, "
+                        "checkpoint every %d, Adam lr %g" % (nf, w.num_agents, T, k, w.meta["lr"]),
+            "iterations": iters, "fit_iters_per_s": iters / t_fit, "ms_per_iter": 1e3 * t_fit / iters,
+            "looped_ms_per_iter": 1e3 * t_loop, "looped_fit_iters_per_s": 1.0 / t_loop,
+            "speedup_vs_looped": t_loop / (t_fit / iters),
+            "loss_first_last": losses,
+            "recovered_weight_abs_err": {"mean": float(err.mean()), "median": float(np.median(err)),
+                                         "max": float(err.max())},
+            "recovered_weight_rel_err": {"median": float(np.median(rel)), "p90": float(np.quantile(rel, 0.9))},
+            "tuned": tuned}
 
 
 def main():
@@ -254,6 +443,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-fit", action="store_true")
+    ap.add_argument("--fit-iters", type=int, default=200)
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--e2e-iters", type=int, default=3)
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="run W warm-up + this many single steps and exit (for ncu)")
@@ -293,6 +486,7 @@ def main():
     for _ in range(args.warmup):
         eng.step(dt, 1)
     eng.sync()
+    tuned = None if args.no_autotune else eng.autotune(dt, steps=10)
     state_before = eng.get_state()
     eng.step(dt, 1)
     state_after = eng.get_state()
@@ -386,7 +580,8 @@ def main():
         "config": {"workload": WORKLOAD, "parallelism": "replicas" if world > 1 else "single",
                    "l2": "no flush between steps: per-step working set ~%.0f MB > 126 MB L2" %
                          ((2 * state_bytes + 16 * n + 8 * eng.num_cells) / 1e6),
-                   "graph": "K steps as one CUDA graph"},
+                   "graph": "K steps as one CUDA graph",
+                   "tuned": tuned},
         "roofline": {"bound": "hbm", "kernel": "fusedKernel", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
                      "peak_source": peak_kind,
@@ -408,6 +603,12 @@ def main():
     eng.close()
     if world == 1 and not args.no_batched:
         line["batched"] = batched_leg(local)
+    if world == 1 and not args.no_adjoint:
+        line["adjoint"] = adjoint_leg(local)
+        if rank == 0 and not args.no_cpu_baseline:
+            line["adjoint"]["accuracy"] = adjoint_accuracy(local)
+    if world == 1 and not args.no_fit:
+        line["fitting"] = fitting_leg(local, args.fit_iters)
     if pg:
         pg.barrier()
         pg.destroy_process_group()

@@ -144,11 +144,26 @@ int brt_engine_num_cells(const brt_engine* e, uint32_t* num_cells);
 int brt_engine_set_params(brt_engine* e, uint32_t flock, const brt_params* p);
 /* Tuning options (the reference's DeviceInterface BlockDim / commonBlockDim
    knobs, Core/src/CommonResources.cpp:78-82, generalised):
-     "sort_digit_bits"  4..9  radix digit width of the onesweep passes (default 8)
+     "sort_digit_bits"  4..9  radix digit width of the onesweep passes (default 8;
+                              at most 4 passes, so narrow digits on wide keys widen)
      "two_pass"         0/1   build each neighbour list before steering even
                               when the single-pass kernel applies (default 0)
-   Unknown keys return BRT_ERR_ARG. */
+     "block_size"       32..256, multiple of 32: threads per block of the
+                              single-pass flock kernel (default 128)
+     "scan_variant"     0..3  neighbour-scan loop: 0 four candidates in flight
+                              with exact cell culling, 1 two in flight with
+                              culling, 2 four without culling, 3 one at a time
+     "phase2_variant"   0/1   list walk one or two neighbours at a time
+     "adjoint_graphs"   0/1   capture the adjoint forward/backward as graphs (default 1)
+     "adjoint_export"   0/1   keep the frozen lists and branch flags (brt_adjoint_get_tape)
+   None of these changes results; unknown keys return BRT_ERR_ARG. */
 int brt_engine_set_option(brt_engine* e, const char* key, int64_t value);
+/* Autotuner: times the sort digit width, then the flock kernel's block size
+   and scan loop, then its list walk, on the engine's own state (graphs of
+   `steps` steps, each trial started from the same snapshot), keeps the
+   fastest, and leaves the state as it found it.  report (optional) receives
+   a JSON object with the choice and every trial's ms per step. */
+int brt_engine_autotune(brt_engine* e, float elapsedTime, uint32_t steps, char* report, size_t report_len);
 /* The engine's CUDA stream (a cudaStream_t), for callers that enqueue their
    own work around the engine's. */
 int brt_engine_stream(brt_engine* e, void** stream);
