@@ -185,7 +185,32 @@ __device__ __forceinline__ uint32_t scanNeighborsPipelined(uint32_t self, f3 p, 
         if (CULL && bxy + (k == 0 ? lo2[2] : (k == 2 ? hi2[2] : 0.0f)) > cullThr) continue;
         if (fl.maxPerCell && stop - start > fl.maxPerCell) stop = start + fl.maxPerCell;
         const float sz = imageShift(gz, k - 1, fl.G, fl.L);
-        for (uint32_t j = start; j < stop; j += UNROLL) {
+        // Without an image shift (every cell away from the periodic seam)
+        // (q + 0) - p and q - p differ at most in the sign of a zero, which
+        // the squares remove: the cheaper form gives the same d2 bit for bit.
+        const bool shifted = sx != 0.0f || sy != 0.0f || sz != 0.0f;
+        uint32_t j = start;
+        for (; j + UNROLL <= stop; j += UNROLL) {
+          float4 q[UNROLL];
+#pragma unroll
+          for (int u = 0; u < UNROLL; ++u) q[u] = __ldg(&posS[j + u]);
+#pragma unroll
+          for (int u = 0; u < UNROLL; ++u) {
+            const uint32_t jj = j + u;
+            float dx, dy, dz;
+            if (shifted) {
+              dx = (q[u].x + sx) - p.x; dy = (q[u].y + sy) - p.y; dz = (q[u].z + sz) - p.z;
+            } else {
+              dx = q[u].x - p.x; dy = q[u].y - p.y; dz = q[u].z - p.z;
+            }
+            const float d2 = dx * dx + dy * dy + dz * dz;
+            if (!(d2 > thr) && jj != self) {
+              list[(n++) * ls] = jj;
+              if (n == M) return n;
+            }
+          }
+        }
+        if (j < stop) {
           float4 q[UNROLL];
 #pragma unroll
           for (int u = 0; u < UNROLL; ++u)

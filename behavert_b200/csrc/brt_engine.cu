@@ -261,7 +261,7 @@ int enqueueStep(brt_engine* e, float dt, bool record) {
   bool twoPass = e->anyKnn || e->forceTwoPass;
   for (const FlockDev& d : e->flocksHost) twoPass = twoPass || (d.F > 0 && (d.clus != 0.0f || d.aclus != 0.0f));
   if (twoPass) BRT_CUDA_TRY(launchFused(F, e->anyKnn, e->stream));
-  else BRT_CUDA_TRY(launchFlock(F, e->phase2Variant, e->fusedBlock, e->stream));
+  else BRT_CUDA_TRY(launchFlock(F, e->phase2Variant, e->fusedBlock, e->wideRegs, e->stream));
   if (timed) {
     if ((rc = stageMark(e, 4))) return rc;
     e->pending[e->ringPos] = true;
@@ -563,6 +563,8 @@ int brt_engine_set_option(brt_engine* e, const char* key, int64_t value) {
       return BRT_ERR_ARG;
     }
     e->fusedBlock = (uint32_t)value;
+  } else if (k == "wide_registers") {
+    e->wideRegs = value != 0;
   } else if (k == "adjoint_graphs") {
     e->adjointGraphs = value != 0;
   } else if (k == "adjoint_export") {
@@ -840,6 +842,7 @@ int brt_engine_autotune(brt_engine* e, float elapsedTime, uint32_t steps, char* 
   if (!rc) chk(brt_engine_set_option(e, "sort_digit_bits", bestBits));
   uint32_t bestBlock = e->fusedBlock;
   int bestScan = e->scanVariant, bestP2 = e->phase2Variant;
+  bool bestWide = e->wideRegs;
   if (!twoPass) {
     bestMs = 1e30;
     const uint32_t blocks[3] = {64, 128, 256};
@@ -857,6 +860,14 @@ int brt_engine_autotune(brt_engine* e, float elapsedTime, uint32_t steps, char* 
       if (!rc && ms <= bestMs) { bestMs = ms; bestP2 = p2; }
     }
     if (!rc) chk(brt_engine_set_option(e, "phase2_variant", bestP2));
+    double wideMs[2] = {1e30, 1e30};
+    for (int wr = 0; wr < 2 && !rc; ++wr) {
+      chk(brt_engine_set_option(e, "wide_registers", wr));
+      if (!rc) chk(trial("wide_registers", wr, &wideMs[wr]));
+    }
+    bestWide = wideMs[1] < wideMs[0];
+    bestMs = std::min(wideMs[0], wideMs[1]);
+    if (!rc) chk(brt_engine_set_option(e, "wide_registers", bestWide ? 1 : 0));
   }
   if (!rc && copyAll(false) != cudaSuccess) { setLastError("autotune restore failed"); rc = BRT_ERR_CUDA; }
   if (!rc) cudaStreamSynchronize(st);
@@ -870,8 +881,8 @@ int brt_engine_autotune(brt_engine* e, float elapsedTime, uint32_t steps, char* 
   if (report && report_len) {
     std::snprintf(buf, sizeof(buf),
                   "{\"sort_digit_bits\": %u, \"block_size\": %u, \"scan_variant\": %d, \"phase2_variant\": %d, "
-                  "\"ms_per_step\": %.6f, \"trials\": [",
-                  bestBits, bestBlock, bestScan, bestP2, bestMs);
+                  "\"wide_registers\": %d, \"ms_per_step\": %.6f, \"trials\": [",
+                  bestBits, bestBlock, bestScan, bestP2, bestWide ? 1 : 0, bestMs);
     std::string out = std::string(buf) + log + "]}";
     std::snprintf(report, report_len, "%s", out.c_str());
   }

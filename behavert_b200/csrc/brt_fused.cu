@@ -34,8 +34,8 @@ __device__ __forceinline__ float shiftOf(uint32_t code, float L) {
   return code == 1u ? -L : (code == 2u ? L : 0.0f);
 }
 
-template <int FP, int P2>
-__global__ void __launch_bounds__(kFlockMaxThreads, 4) flockKernel(FusedArgs A) {
+template <int FP, int P2, int MINB>
+__global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs A) {
   extern __shared__ uint32_t sList[];
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.n) return;
@@ -209,32 +209,44 @@ __global__ void __launch_bounds__(kFlockMaxThreads, 4) flockKernel(FusedArgs A) 
 
 namespace {
 template <int FP>
-cudaError_t launchFlockFP(const FusedArgs& A, uint32_t blocks, uint32_t block, size_t smem, int phase2, cudaStream_t st) {
-  if (phase2) flockKernel<FP, 1><<<blocks, block, smem, st>>>(A);
-  else flockKernel<FP, 0><<<blocks, block, smem, st>>>(A);
+cudaError_t launchFlockFP(const FusedArgs& A, uint32_t blocks, uint32_t block, size_t smem, int phase2, bool wideRegs,
+                          cudaStream_t st) {
+  if (wideRegs) {
+    if (phase2) flockKernel<FP, 1, 2><<<blocks, block, smem, st>>>(A);
+    else flockKernel<FP, 0, 2><<<blocks, block, smem, st>>>(A);
+  } else {
+    if (phase2) flockKernel<FP, 1, 4><<<blocks, block, smem, st>>>(A);
+    else flockKernel<FP, 0, 4><<<blocks, block, smem, st>>>(A);
+  }
   return cudaGetLastError();
 }
 template <int FP>
 cudaError_t configureFlockFP(int smem) {
-  cudaError_t e = cudaFuncSetAttribute(flockKernel<FP, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(flockKernel<FP, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  const void* fns[4] = {(const void*)flockKernel<FP, 0, 4>, (const void*)flockKernel<FP, 1, 4>,
+                        (const void*)flockKernel<FP, 0, 2>, (const void*)flockKernel<FP, 1, 2>};
+  for (const void* fn : fns) {
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 }  // namespace
 
 // phase2 != 0 walks the list two neighbours at a time with their loads issued
 // together.  block: threads per block, a multiple of 32 in [32, 256].
-cudaError_t launchFlock(const FusedArgs& A, int phase2, uint32_t block, cudaStream_t st) {
+// wideRegs: compiled for 2 resident 256-thread blocks per SM (up to 128
+// registers a thread) instead of 4 (64 registers).
+cudaError_t launchFlock(const FusedArgs& A, int phase2, uint32_t block, bool wideRegs, cudaStream_t st) {
   if (A.n == 0) return cudaSuccess;
   if (block < 32 || block > kFlockMaxThreads || block % 32) return cudaErrorInvalidValue;
   const uint32_t blocks = (A.n + block - 1) / block;
   const uint32_t fp = A.Fs;
   const size_t smem = (size_t)block * A.Mmax * 4;
-  if (fp == 0) return launchFlockFP<0>(A, blocks, block, smem, phase2, st);
-  if (fp <= 4) return launchFlockFP<4>(A, blocks, block, smem, phase2, st);
-  if (fp <= 8) return launchFlockFP<8>(A, blocks, block, smem, phase2, st);
-  if (fp <= 16) return launchFlockFP<16>(A, blocks, block, smem, phase2, st);
-  return launchFlockFP<32>(A, blocks, block, smem, phase2, st);
+  if (fp == 0) return launchFlockFP<0>(A, blocks, block, smem, phase2, wideRegs, st);
+  if (fp <= 4) return launchFlockFP<4>(A, blocks, block, smem, phase2, wideRegs, st);
+  if (fp <= 8) return launchFlockFP<8>(A, blocks, block, smem, phase2, wideRegs, st);
+  if (fp <= 16) return launchFlockFP<16>(A, blocks, block, smem, phase2, wideRegs, st);
+  return launchFlockFP<32>(A, blocks, block, smem, phase2, wideRegs, st);
 }
 
 cudaError_t configureFlockKernels(uint32_t Mmax) {

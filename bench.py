@@ -450,6 +450,8 @@ def main():
     ap.add_argument("--e2e-iters", type=int, default=3)
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="run W warm-up + this many single steps and exit (for ncu)")
+    ap.add_argument("--options", default="",
+                    help="engine options key=value,... applied before stepping (replaces the autotuner)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world, rank, local = dist_setup(args)
@@ -470,6 +472,11 @@ def main():
 
     w = workloads.large()
     eng = Engine(w.params, device=local)
+    options = [kv.split("=") for kv in args.options.split(",") if kv]
+    for key, val in options:
+        eng.set_option(key, int(val))
+    if options:
+        args.no_autotune = True
     eng.set_state(w.pos, w.fwd, w.acc, w.feat)
     n = eng.num_agents
     dt = w.dt
