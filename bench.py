@@ -450,6 +450,8 @@ def main():
     ap.add_argument("--e2e-iters", type=int, default=3)
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="run W warm-up + this many single steps and exit (for ncu)")
+    ap.add_argument("--profile-adjoint", type=int, default=0,
+                    help="run this many config-3 adjoint iterations (taped forward + backward) and exit (for ncu)")
     ap.add_argument("--options", default="",
                     help="engine options key=value,... applied before stepping (replaces the autotuner)")
     args = ap.parse_args()
@@ -469,6 +471,17 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         pg = dist
+
+    if args.profile_adjoint:
+        a = workloads.adjoint()
+        with Engine(a.params, device=local) as eng:
+            target = np.zeros((a.num_agents, 4), np.float32)
+            target[:, :3] = a.pos[:, :3]
+            for _ in range(args.profile_adjoint):
+                eng.set_state(a.pos, a.fwd, a.acc)
+                eng.adjoint_forward(target, a.steps, a.meta["checkpoint_every"], a.dt)
+                eng.adjoint_backward()
+        return 0
 
     w = workloads.large()
     eng = Engine(w.params, device=local)
@@ -571,7 +584,7 @@ def main():
     fused_ms = stage_avg[3]
     fused_bytes = ab["fused_per_agent"] * n
     achieved = fused_bytes / (fused_ms / 1e3) / 1e9 if fused_ms > 0 else None
-    traffic_file = ROOT / "profiles" / "fused_traffic.json"
+    traffic_file = ROOT / "profiles" / "flockKernel_config1_traffic.json"
     traffic = None
     if traffic_file.exists():
         try:
@@ -589,7 +602,8 @@ def main():
                          ((2 * state_bytes + 16 * n + 8 * eng.num_cells) / 1e6),
                    "graph": "K steps as one CUDA graph",
                    "tuned": tuned},
-        "roofline": {"bound": "hbm", "kernel": "fusedKernel", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+        "roofline": {"bound": "hbm", "kernel": "flockKernel (fused neighbour search + steering + integration)",
+                     "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
                      "peak_source": peak_kind,
                      "alg_bytes_per_launch": fused_bytes,

@@ -154,6 +154,8 @@ int brt_engine_set_params(brt_engine* e, uint32_t flock, const brt_params* p);
                               with exact cell culling, 1 two in flight with
                               culling, 2 four without culling, 3 one at a time
      "phase2_variant"   0/1   list walk one or two neighbours at a time
+     "wide_registers"   0/1   the flock kernel built for 128 registers a thread
+                              (2 resident 256-thread blocks per SM) instead of 64
      "adjoint_graphs"   0/1   capture the adjoint forward/backward as graphs (default 1)
      "adjoint_export"   0/1   keep the frozen lists and branch flags (brt_adjoint_get_tape)
    None of these changes results; unknown keys return BRT_ERR_ARG. */
