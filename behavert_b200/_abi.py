@@ -27,6 +27,24 @@ BRT_MAX_OBSTACLES = 64
 F3 = C.c_float * 3
 
 
+class SchoolingParams(C.Structure):
+    """Mirror of struct brt_schooling_params (SchoolingParams field names)."""
+
+    _fields_ = [
+        ("mode", C.c_int32),
+        ("theta", C.c_float),
+        ("delta", C.c_float),
+        ("r_r", C.c_float),
+        ("r_p", C.c_float),
+        ("eta", C.c_float),
+        ("w_a", C.c_float),
+        ("w_o", C.c_float),
+        ("s", C.c_float),
+        ("randomDeviationWeight", C.c_float),
+        ("seed", C.c_uint32),
+    ]
+
+
 class BrtParams(C.Structure):
     """Mirror of brt_params (field names of the reference's parameter structs)."""
 
@@ -57,6 +75,7 @@ class BrtParams(C.Structure):
         ("numObstacles", C.c_uint32),
         ("obstacleAvoidanceWeight", C.c_float),
         ("obstacles", (C.c_float * 4) * BRT_MAX_OBSTACLES),
+        ("schooling", SchoolingParams),
     ]
 
     def set_obstacles(self, arr) -> None:
@@ -119,6 +138,10 @@ _SIGS = {
     "brt_get_steer_force": (C.c_int, [_vp, _vp, C.c_int]),
     "brt_engine_record_lists": (C.c_int, [_vp, C.c_int]),
     "brt_engine_check_device_error": (C.c_int, [_vp, _u32p]),
+    "brt_school_repulsion": (C.c_int, [_vp]),
+    "brt_school_attraction_orientation": (C.c_int, [_vp]),
+    "brt_school_movement": (C.c_int, [_vp]),
+    "brt_school_animate": (C.c_int, [_vp]),
     "brt_engine_autotune": (C.c_int, [_vp, C.c_float, C.c_uint32, C.c_char_p, C.c_size_t]),
     "brt_adjoint_forward": (C.c_int, [_vp, C.c_float, C.c_uint32, C.c_uint32, _vp, C.c_int, _vp]),
     "brt_adjoint_backward": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_int]),

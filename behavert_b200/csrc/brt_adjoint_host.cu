@@ -77,6 +77,7 @@ int checkSupported(brt_engine* e) {
   for (const FlockDev& d : e->flocksHost) {
     if (d.useKnn) { setLastError("adjoint: kNN neighbour lists are not supported"); return BRT_ERR_CONFIG; }
     if (d.use2D) { setLastError("adjoint: use2DProjection is not supported"); return BRT_ERR_CONFIG; }
+    if (d.school) { setLastError("adjoint: the Schooling law is not supported"); return BRT_ERR_CONFIG; }
     if (d.F > 0 && (d.clus != 0.0f || d.aclus != 0.0f)) {
       setLastError("adjoint: feature clustering steering is not supported");
       return BRT_ERR_CONFIG;

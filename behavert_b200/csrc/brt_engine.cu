@@ -58,6 +58,8 @@ static int validateParams(const brt_params& p, uint32_t& G) {
   if (p.featuresCount > BRT_MAX_FEATUREDIM) { setLastError("featuresCount must be <= 32"); return BRT_ERR_CONFIG; }
   if (p.numObstacles > BRT_MAX_OBSTACLES) { setLastError("numObstacles must be <= 64"); return BRT_ERR_CONFIG; }
   if (!(p.commonMass != 0.0f)) { setLastError("commonMass must be nonzero"); return BRT_ERR_CONFIG; }
+  if (p.schooling.mode < 0 || p.schooling.mode > 2) { setLastError("schooling.mode must be 0, 1 or 2"); return BRT_ERR_CONFIG; }
+  if (p.schooling.mode != 0 && p.useKnn) { setLastError("schooling flocks use the first-M neighbour lists (useKnn = 0)"); return BRT_ERR_CONFIG; }
   return BRT_OK;
 }
 
@@ -96,6 +98,16 @@ static FlockDev toDev(const brt_params& p, uint32_t G) {
     const float mc = std::max(p.separationParams[2], std::max(p.alignmentParams[2], p.cohesionParams[2]));
     d.cosBound2 = (mc < -1.0f) ? mc * mc : 0.0f;
   }
+  d.school = p.schooling.mode;
+  d.schTheta = p.schooling.theta;
+  d.schRr = p.schooling.r_r;
+  d.schRp = p.schooling.r_p;
+  d.schEta = p.schooling.eta;
+  d.schWa = p.schooling.w_a;
+  d.schWo = p.schooling.w_o;
+  d.schS = p.schooling.s;
+  d.schRand = p.schooling.randomDeviationWeight;
+  d.schSeed = p.schooling.seed;
   return d;
 }
 
@@ -157,7 +169,7 @@ void freeAll(brt_engine* e) {
       if (e->ev[r][k]) cudaEventDestroy(e->ev[r][k]);
   void* ptrs[] = {e->flocks, e->agentBase, e->obstacles, e->obsMask, e->posA, e->fwdA, e->accA, e->posS, e->fwdS, e->accS,
                   e->featA, e->featS, e->featNormS, e->idA, e->idS, e->statsById, e->steer, e->lists, e->pairs[0], e->pairs[1],
-                  e->cellStart, e->cellEnd, e->sortMem, e->errWord, e->stage4, e->stageF};
+                  e->cellStart, e->cellEnd, e->sortMem, e->errWord, e->stage4, e->stageF, e->stepCounter};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (e->stream) cudaStreamDestroy(e->stream);
@@ -174,6 +186,7 @@ HashArgs hashArgs(brt_engine* e) {
   A.cellStart = e->cellStart; A.cellEnd = e->cellEnd; A.cellWords4 = e->Cpad / 4;
   A.status = e->ss.status; A.statusWords = e->plan.passes * std::max(1u, e->plan.tiles) * e->plan.bins;
   A.counters = e->ss.counters;
+  A.stepCounter = e->stepCounter;
   return A;
 }
 
@@ -187,6 +200,7 @@ StageArgs stageArgs(brt_engine* e) {
   A.flocks = e->flocks; A.agentBase = e->agentBase; A.obstacles = e->obstacles; A.obsMask = e->obsMask;
   A.lists = e->lists; A.listStride = e->listStride;
   A.nflocks = e->nflocks; A.n = e->N; A.Fs = e->Fs;
+  A.stepCounter = e->stepCounter;
   return A;
 }
 
@@ -256,11 +270,13 @@ int enqueueStep(brt_engine* e, float dt, bool record) {
   F.lists = record ? e->lists : nullptr; F.listStride = e->listStride;
   F.nflocks = e->nflocks; F.n = e->N; F.Mmax = e->Mmax; F.Fs = e->Fs; F.dt = dt;
   F.scanVariant = e->scanVariant;
+  F.stepCounter = e->stepCounter;
   // The single-pass kernel covers every flock unless one needs kNN
   // replacement or clustering steering (both need the whole list first).
   bool twoPass = e->anyKnn || e->forceTwoPass;
   for (const FlockDev& d : e->flocksHost) twoPass = twoPass || (d.F > 0 && (d.clus != 0.0f || d.aclus != 0.0f));
-  if (twoPass) BRT_CUDA_TRY(launchFused(F, e->anyKnn, e->stream));
+  if (e->school) BRT_CUDA_TRY(launchSchool(F, e->stream));
+  else if (twoPass) BRT_CUDA_TRY(launchFused(F, e->anyKnn, e->stream));
   else BRT_CUDA_TRY(launchFlock(F, e->phase2Variant, e->fusedBlock, e->wideRegs, e->stream));
   if (timed) {
     if ((rc = stageMark(e, 4))) return rc;
@@ -372,6 +388,18 @@ int brt_params_default(brt_params* p) {
   p->similarityStatsParams[0] = 0.01f; p->similarityStatsParams[1] = 0.1f; p->similarityStatsParams[2] = 0.001f;
   p->avgSimilarityController = 1.0f;
   p->featureRelaxRate = 0.0f;
+  // SchoolingPlugIn::install (PlugIns/Schooling/include/SchoolingPlugIn.h:115-160)
+  p->schooling.mode = 0;
+  p->schooling.theta = (float)std::cos(0.1);
+  p->schooling.delta = 0.01f;
+  p->schooling.r_r = 1.0f;
+  p->schooling.r_p = p->commonSearchRadius;
+  p->schooling.eta = (float)std::cos(3.05);
+  p->schooling.w_a = 1.0f;
+  p->schooling.w_o = 16.0f;
+  p->schooling.s = 3.0f;
+  p->schooling.randomDeviationWeight = 0.1f;
+  p->schooling.seed = 0;
   return BRT_OK;
 }
 
@@ -405,6 +433,12 @@ int brt_engine_create(const brt_params* flocks, uint32_t num_flocks, int device,
     e->Mmax = std::max(e->Mmax, d.M);
     e->Fmax = std::max(e->Fmax, d.F);
     e->anyKnn = e->anyKnn || d.useKnn;
+    if (f > 0 && (d.school != 0) != e->school) {
+      delete e;
+      setLastError("all flocks of an engine use the same steering family (schooling.mode 0, or 1/2)");
+      return BRT_ERR_CONFIG;
+    }
+    e->school = d.school != 0;
     e->flocksHost.push_back(d);
   }
   // Neighbour-list entries hold a 26-bit sorted slot (brt_fused.cu).
@@ -443,6 +477,7 @@ int brt_engine_create(const brt_params* flocks, uint32_t num_flocks, int device,
   chk(devAlloc(&e->pairs[0], n)); chk(devAlloc(&e->pairs[1], n));
   chk(devAlloc(&e->cellStart, e->Cpad)); chk(devAlloc(&e->cellEnd, e->Cpad));
   chk(devAlloc(&e->errWord, 1));
+  chk(devAlloc(&e->stepCounter, 1));
   chk(devAlloc(&e->stage4, n));
   chk(devAlloc(&e->stageF, std::max<size_t>(1, n * e->Fmax)));
   const size_t sortBytes = sortScratchBytes(e->plan, false);
@@ -461,6 +496,7 @@ int brt_engine_create(const brt_params* flocks, uint32_t num_flocks, int device,
   }
   BRT_CUDA_TRY(cudaMemsetAsync(e->sortMem, 0, sortBytes, st));
   BRT_CUDA_TRY(cudaMemsetAsync(e->errWord, 0, 4, st));
+  BRT_CUDA_TRY(cudaMemsetAsync(e->stepCounter, 0, 4, st));
   if (n) {
     BRT_CUDA_TRY(cudaMemsetAsync(e->posA, 0, n * 16, st));
     BRT_CUDA_TRY(cudaMemsetAsync(e->fwdA, 0, n * 16, st));
@@ -511,7 +547,7 @@ int brt_engine_set_params(brt_engine* e, uint32_t flock, const brt_params* p) {
   const brt_params& o = e->params[flock];
   if (p->numBodies != o.numBodies || p->worldSize != o.worldSize || p->cellSize != o.cellSize ||
       p->maxNeighbors != o.maxNeighbors || p->featuresCount != o.featuresCount || p->numObstacles != o.numObstacles ||
-      (p->useKnn != 0) != (o.useKnn != 0)) {
+      (p->useKnn != 0) != (o.useKnn != 0) || (p->schooling.mode != 0) != (o.schooling.mode != 0)) {
     setLastError("brt_engine_set_params: geometry fields cannot change");
     return BRT_ERR_CONFIG;
   }
@@ -563,6 +599,12 @@ int brt_engine_set_option(brt_engine* e, const char* key, int64_t value) {
       return BRT_ERR_ARG;
     }
     e->fusedBlock = (uint32_t)value;
+  } else if (k == "random_step") {
+    if (value < 0 || value > 0xFFFFFFFFll) { setLastError("random_step must be a uint32"); return BRT_ERR_ARG; }
+    const uint32_t v = (uint32_t)value;
+    BRT_CUDA_TRY(cudaMemcpyAsync(e->stepCounter, &v, 4, cudaMemcpyHostToDevice, e->stream));
+    BRT_CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return BRT_OK;  // a value, not a launch configuration: graphs stay valid
   } else if (k == "wide_registers") {
     e->wideRegs = value != 0;
   } else if (k == "adjoint_graphs") {
@@ -819,7 +861,8 @@ int brt_engine_autotune(brt_engine* e, float elapsedTime, uint32_t steps, char* 
     *msPerStep = best;
     return BRT_OK;
   };
-  bool twoPass = e->anyKnn || e->forceTwoPass;
+  // The flock kernel's options only matter when that kernel runs.
+  bool twoPass = e->anyKnn || e->forceTwoPass || e->school;
   for (const FlockDev& d : e->flocksHost) twoPass = twoPass || (d.F > 0 && (d.clus != 0.0f || d.aclus != 0.0f));
   std::string log;
   char buf[256];
@@ -935,6 +978,20 @@ int brt_steer_for_clustering(brt_engine* e) { return steerStage(e, 3); }
 // this stage applies the static obstacle field of the EnvGrid3D grid instead.
 int brt_compute_seekings_world_center(brt_engine* e) { return steerStage(e, 4); }
 
+static int schoolStage(brt_engine* e, int which) {
+  if (!e) return BRT_ERR_ARG;
+  if (!e->school) { setLastError("Schooling functionality on a flocking engine (schooling.mode 0)"); return BRT_ERR_STATE; }
+  if (!e->reordered || !e->listsValid) { setLastError("Schooling functionality before computeNeighborhoods"); return BRT_ERR_STATE; }
+  DeviceGuard guard(e->device);
+  BRT_CUDA_TRY(launchSchoolStage(stageArgs(e), which, e->stream));
+  return BRT_OK;
+}
+
+int brt_school_repulsion(brt_engine* e) { return schoolStage(e, 0); }
+int brt_school_attraction_orientation(brt_engine* e) { return schoolStage(e, 1); }
+int brt_school_movement(brt_engine* e) { return schoolStage(e, 2); }
+int brt_school_animate(brt_engine* e) { return schoolStage(e, 3); }
+
 int brt_apply_steering_forces(brt_engine* e, float elapsedTime) {
   if (!e) return BRT_ERR_ARG;
   if (!e->reordered || !e->listsValid) { setLastError("applySteeringForces before computeNeighborhoods"); return BRT_ERR_STATE; }
@@ -998,6 +1055,7 @@ namespace {
 int configureKernels(brt_engine* e) {
   BRT_CUDA_TRY(configureFusedKernels(e->Mmax));
   BRT_CUDA_TRY(configureFlockKernels(e->Mmax));
+  BRT_CUDA_TRY(configureSchoolKernels(e->Mmax));
   return BRT_OK;
 }
 }  // namespace

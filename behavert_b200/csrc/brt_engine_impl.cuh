@@ -26,6 +26,8 @@ struct brt_engine {
   float4* obstacles = nullptr;
   uint2* obsMask = nullptr;   // per-cell obstacle field (null when no flock has obstacles)
   bool anyKnn = false;
+  bool school = false;        // the flocks use the Schooling law (schooling.mode 1 or 2)
+  uint32_t* stepCounter = nullptr;  // device word: steps taken (keys the Schooling random stream)
   bool forceTwoPass = false;  // option "two_pass": run the list-first kernel even when not needed
   int phase2Variant = 0;      // option "phase2_variant": list walk one or two neighbours at a time
   int scanVariant = 0;        // option "scan_variant": neighbour-scan loop shape

@@ -56,6 +56,10 @@ struct FlockDev {
   // agent with |forward|^2 * 1.002 below it, every finite cosine passes the
   // angle test, which then only rejects NaN (a zero offset).
   float cosBound2;
+  // SchoolingParams (0: flocking law; 1: animateSchool; 2: split path)
+  int32_t school;
+  float schTheta, schRr, schRp, schEta, schWa, schWo, schS, schRand;
+  uint32_t schSeed;
 };
 
 // ---------------------------------------------------------------------------

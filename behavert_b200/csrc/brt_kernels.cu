@@ -49,6 +49,7 @@ __global__ void __launch_bounds__(256) hashKernel(HashArgs A) {
   for (uint32_t c = gtid; c < A.cellWords4; c += gstride) { cs[c] = e4; ce[c] = e4; }
   for (uint32_t k = gtid; k < A.statusWords; k += gstride) A.status[k] = 0u;
   if (gtid < A.passes) A.counters[gtid] = 0u;
+  if (gtid == 0 && A.stepCounter) *A.stepCounter += 1u;
   __syncthreads();
   for (uint32_t k = threadIdx.x; k < histWords; k += blockDim.x)
     if (sHist[k]) atomicAdd(&A.hist[k], sHist[k]);

@@ -24,6 +24,7 @@ struct HashArgs {
   uint32_t* status;            // sort look-back state to clear
   uint32_t statusWords;
   uint32_t* counters;          // sort tile counters to clear
+  uint32_t* stepCounter;       // random-stream step counter, incremented once per step
 };
 
 struct ReorderArgs {
@@ -55,6 +56,7 @@ struct FusedArgs {
   uint32_t nflocks, n, Mmax, Fs;
   float dt;
   int scanVariant;             // 0: pipelined x4 + cell culling, 1: x2 + culling, 2: x4, 3: flat loop
+  const uint32_t* stepCounter; // random-stream step of the Schooling move
 };
 
 struct StageArgs {
@@ -70,6 +72,7 @@ struct StageArgs {
   uint32_t* lists;
   uint32_t listStride;
   uint32_t nflocks, n, Fs;
+  const uint32_t* stepCounter;
 };
 
 // Reverse of one taped step (brt_adjoint.cu).
@@ -123,6 +126,11 @@ cudaError_t launchFlock(const FusedArgs& A, int phase2, uint32_t block, bool wid
 cudaError_t launchLists(const StageArgs& A, bool knn, cudaStream_t st);
 cudaError_t launchSteerStage(const StageArgs& A, int which, cudaStream_t st);
 cudaError_t launchIntegrateStage(const StageArgs& A, float dt, cudaStream_t st);
+// Schooling (brt_school.cu): fused step, and stage which = 0 repulsion,
+// 1 attraction/orientation, 2 move, 3 animateSchool.
+cudaError_t launchSchool(const FusedArgs& A, cudaStream_t st);
+cudaError_t launchSchoolStage(const StageArgs& A, int which, cudaStream_t st);
+cudaError_t configureSchoolKernels(uint32_t Mmax);
 cudaError_t launchScatterToId(const float4* src, const uint32_t* id, float4* dst, uint32_t n, cudaStream_t st);
 cudaError_t launchScatterFeatToId(const float* src, uint32_t Fs, const uint32_t* id, float* dst, uint32_t F, uint32_t n, cudaStream_t st);
 cudaError_t launchLoadFeat(const float* src, uint32_t F, float* dst, uint32_t Fs, uint32_t n, cudaStream_t st);

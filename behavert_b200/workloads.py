@@ -191,5 +191,30 @@ def fitting(num_flocks: int = 256, lo: int = 1024, hi: int = 32768, seed: int = 
                      "hidden": hidden.tolist(), "adam_iters": 200, "lr": 0.05})
 
 
+def schooling(n: int = 4096, L: float = 64.0, M: int = 16, mode: int = 1, seed: int = 5, steps: int = 50,
+              random_weight: float = 0.1, flocks: int = 1) -> Workload:
+    """Schooling plugin (PlugIns/Schooling) with the reference's install-time
+    constants (SchoolingPlugIn.h:119-148: r_r 1, r_p = search radius, s 3,
+    w_a 1, w_o 16, theta cos 0.1, eta cos 3.05); `flocks` equal flocks of n
+    agents each in one engine."""
+    rng = np.random.default_rng(seed)
+    params, P, W = [], [], []
+    for _ in range(flocks):
+        p = _flock_params(n, L, M)
+        p.schooling.mode = int(mode)
+        p.schooling.randomDeviationWeight = float(random_weight)
+        p.schooling.seed = int(rng.integers(1 << 31))
+        params.append(p)
+        pos, fwd = _agents(rng, n, L)
+        fwd[:, 3] = p.schooling.s
+        P.append(pos)
+        W.append(fwd)
+    pos = np.concatenate(P)
+    fwd = np.concatenate(W)
+    return Workload("schooling", params, pos, fwd, np.zeros_like(pos), None, steps, DT,
+                    {"seed": seed, "mode": mode})
+
+
 def by_name(name: str, **kw) -> Workload:
-    return {"plain": plain, "large": large, "batched": batched, "adjoint": adjoint, "fitting": fitting}[name](**kw)
+    return {"plain": plain, "large": large, "batched": batched, "adjoint": adjoint, "fitting": fitting,
+            "schooling": schooling}[name](**kw)

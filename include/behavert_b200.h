@@ -73,6 +73,22 @@ extern "C" {
  * [0, worldSize)^3 split into gridSize^3 cells of side cellSize
  * (worldSize == gridSize * cellSize, gridSize >= 3).
  */
+/* SchoolingParams (PlugIns/Schooling/include/Schooling_kernel.cuh:36-56),
+   the schooling member of brt_params below. */
+typedef struct brt_schooling_params {
+    int32_t  mode;                 /* 0 flocking law, 1 animateSchool, 2 split path */
+    float    theta;                /* cos of the maximum turning angle     */
+    float    delta;                /* accepted, unused (as in the reference) */
+    float    r_r;                  /* repulsion radius                     */
+    float    r_p;                  /* attraction / orientation radius      */
+    float    eta;                  /* cos of the blind-angle limit         */
+    float    w_a;                  /* attraction weight                    */
+    float    w_o;                  /* orientation weight                   */
+    float    s;                    /* constant speed                       */
+    float    randomDeviationWeight;
+    uint32_t seed;                 /* random-stream seed                   */
+} brt_schooling_params;
+
 typedef struct brt_params {
     /* Body3DParams (PlugIns/Body/include/body3d_kernel.cuh:39-58) */
     uint32_t numBodies;
@@ -115,6 +131,22 @@ typedef struct brt_params {
     uint32_t numObstacles;         /* 0..BRT_MAX_OBSTACLES                    */
     float    obstacleAvoidanceWeight;
     float    obstacles[BRT_MAX_OBSTACLES][4]; /* centre xyz, radius            */
+
+    /* SchoolingParams (PlugIns/Schooling/include/Schooling_kernel.cuh:36-56).
+       mode selects the steering law of the flock:
+         0  flocking (OpenSteerWrapper separation / alignment / cohesion)
+         1  Schooling_animateSchool (Schooling_kernel.cu:226-318): repulsion
+            within r_r, else attraction + orientation within r_p; turn limited
+            to theta; constant speed s, step s * forward * 0.1
+         2  the split path calcRepulsion -> calcAttractionOrientation ->
+            calcMovement (Schooling_kernel.cu:64-221): as 1 but with the blind
+            angle eta in the attraction/orientation zone, a random deviation of
+            weight randomDeviationWeight, and step s * forward * 0.2.
+       The reference draws the deviation from a time-seeded Mersenne Twister;
+       here it is a counter-based generator (splitmix64 of seed, step, agent
+       id), so runs are reproducible.  All flocks of one engine use the same
+       family (mode 0, or modes 1/2). */
+    brt_schooling_params schooling;
 } brt_params;
 
 /* Fills *p with the reference defaults used by the flocking demo and the
@@ -158,6 +190,8 @@ int brt_engine_set_params(brt_engine* e, uint32_t flock, const brt_params* p);
                               (2 resident 256-thread blocks per SM) instead of 64
      "adjoint_graphs"   0/1   capture the adjoint forward/backward as graphs (default 1)
      "adjoint_export"   0/1   keep the frozen lists and branch flags (brt_adjoint_get_tape)
+     "random_step"      uint32 the step counter of the Schooling random stream
+                              (every hash pass adds 1 before the move reads it)
    None of these changes results; unknown keys return BRT_ERR_ARG. */
 int brt_engine_set_option(brt_engine* e, const char* key, int64_t value);
 /* Autotuner: times the sort digit width, then the flock kernel's block size
@@ -211,6 +245,13 @@ int brt_compute_cohesions(brt_engine* e);             /* OpenSteerWrapperPlugIn.
 int brt_steer_for_clustering(brt_engine* e);          /* BehaviorClusteringPlugIn.h:740-822 */
 int brt_compute_seekings_world_center(brt_engine* e); /* OpenSteerWrapperPlugIn.h:380-393   */
 int brt_apply_steering_forces(brt_engine* e, float elapsedTime); /* OpenSteerWrapperPlugIn.h:400-418 */
+/* SchoolingPlugIn functionalities (engines whose flocks have schooling.mode
+   1 or 2), after brt_compute_neighborhoods; the first two write the steering
+   force (brt_get_steer_force), the last two the new state. */
+int brt_school_repulsion(brt_engine* e);              /* calcRepulsion, SchoolingPlugIn.h:236-248             */
+int brt_school_attraction_orientation(brt_engine* e); /* calcAttractionOrientation, SchoolingPlugIn.h:252-264 */
+int brt_school_movement(brt_engine* e);               /* calcMovement, SchoolingPlugIn.h:268-299              */
+int brt_school_animate(brt_engine* e);                /* animateSchool, SchoolingPlugIn.h:219-232             */
 
 /* ---- getters of the intermediate features --------------------------------- */
 /* Sorted (cell hash, agent id) pairs as uint2, like getHash() after

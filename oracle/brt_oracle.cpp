@@ -583,6 +583,123 @@ void steerIntegrate(const Shared& S, const State<R>& st, R dt, State<R>& out, R*
   });
 }
 
+// splitmix64 (Steele, Lea, Flood 2014): the counter-based generator that
+// replaces the Schooling plugin's time-seeded Mersenne Twister.
+inline uint64_t splitmix64(uint64_t x) {
+  uint64_t z = x + 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+// Three uniforms in [0, 1) with 24 bits each, keyed on (seed, step, agent id).
+inline void schoolRandom(uint32_t seed, uint32_t step, uint32_t id, float r[3]) {
+  const uint64_t base = splitmix64(((uint64_t)seed << 32) | step);
+  const uint64_t u1 = splitmix64(base ^ (uint64_t)id);
+  const uint64_t u2 = splitmix64(u1);
+  const float k = 5.9604644775390625e-08f;
+  r[0] = (float)(uint32_t)(u1 >> 40) * k;
+  r[1] = (float)(uint32_t)((u1 >> 16) & 0xFFFFFFu) * k;
+  r[2] = (float)(uint32_t)(u2 >> 40) * k;
+}
+
+// The Schooling plugin's law per sorted slot (PlugIns/Schooling):
+//   mode 1  Schooling_animateSchool (Schooling_kernel.cu:226-318)
+//   mode 2  Schooling_repulsion (:64-95) -> Schooling_attractionOrientation
+//           (:100-145, zone test inAttractionOrientationZone,
+//           Schooling_resources.cu:34-71) -> Schooling_move (:150-221)
+// The boundary term is the identity in the periodic world; positions wrap.
+template <class R>
+void schoolIntegrate(const Shared& S, const State<R>& st, State<R>& out, R* steerOut, uint32_t step, int threads) {
+  const uint32_t stride = S.Mmax + 1;
+  parallelFor(S.N, threads, [&](uint32_t b, uint32_t e) {
+    std::vector<V3<R>> img(BRT_MAX_NEIGHBORS);
+    for (uint32_t i = b; i < e; ++i) {
+      const uint32_t id = S.sortedIds[i];
+      const Flock& F = S.fl[S.flockOfAgent[id]];
+      const brt_schooling_params& sc = F.p.schooling;
+      const uint32_t* lst = &S.lists[(size_t)i * stride];
+      const uint32_t n = lst[0];
+      const R* P = &st.pos[4 * (size_t)i];
+      const R* W = &st.fwd[4 * (size_t)i];
+      const V3<R> myPos = v3(P), myFwd = v3(W);
+      const float* pif = &S.sposf[4 * (size_t)i];
+      for (uint32_t k = 0; k < n; ++k) {
+        const uint32_t j = lst[1 + k];
+        img[k] = imagePos<R>(F, &st.pos[4 * (size_t)j], pif, &S.sposf[4 * (size_t)j]);
+      }
+      V3<R> rep = mk<R>(0, 0, 0);
+      uint32_t found = 0;
+      for (uint32_t k = 0; k < n; ++k) {
+        const V3<R> off = img[k] - myPos;
+        const R dist = length(off);
+        if (dist < R(sc.r_r)) { rep = rep + off / length(off); ++found; }
+      }
+      auto attractOrient = [&](bool blind) {
+        V3<R> orient = myFwd / length(myFwd);
+        V3<R> attr = mk<R>(0, 0, 0);
+        for (uint32_t k = 0; k < n; ++k) {
+          const V3<R> off = img[k] - myPos;
+          const R dist = length(off);
+          const bool in = blind ? (!(dist > R(sc.r_p)) && dot(myFwd, normalize(off)) > R(sc.eta)) : (dist < R(sc.r_p));
+          if (in) {
+            attr = attr + off / length(off);
+            const V3<R> wj = v3(&st.fwd[4 * (size_t)lst[1 + k]]);
+            orient = orient + wj / length(wj);
+          }
+        }
+        return (attr * R(sc.w_a)) + (orient * R(sc.w_o));
+      };
+      V3<R> fwd, pos;
+      if (sc.mode == 1) {
+        V3<R> nf = mk<R>(-rep.x, -rep.y, -rep.z);
+        if (found == 0) nf = attractOrient(false);
+        if (F.p.use2DProjection) nf.y = 0;
+        if (length(nf) > R(0)) nf = normalize(nf);
+        fwd = vecLimitDeviationAngleUtility(nf, R(sc.theta), myFwd);
+        pos = myPos + ((fwd * R(sc.s)) * R(0.1f));
+      } else {
+        V3<R> steer = rep;
+        if (length(rep) > R(0)) {
+          const V3<R> u = normalize(rep);
+          steer = mk<R>(-u.x, -u.y, -u.z);
+        }
+        if (!(length(steer) > R(0))) {
+          V3<R> nf = attractOrient(true);
+          if (length(nf) > R(0)) nf = normalize(nf);
+          steer = nf;
+        }
+        if (steerOut) {
+          R* so = steerOut + 4 * (size_t)i;
+          so[0] = steer.x; so[1] = steer.y; so[2] = steer.z; so[3] = 0;
+        }
+        V3<R> nf = steer;
+        if (sc.randomDeviationWeight > 0.0f) {
+          float r[3];
+          schoolRandom(sc.seed, step, id, r);
+          const R w = R(sc.randomDeviationWeight);
+          const V3<R> rd = ((mk<R>(R(r[0]), R(r[1]), R(r[2])) * w) * R(2)) - (mk<R>(1, 1, 1) * w);
+          nf = normalize(nf + rd);
+        }
+        fwd = vecLimitDeviationAngleUtility(nf, R(sc.theta), myFwd);
+        pos = myPos + ((fwd * R(sc.s)) * R(0.2f));
+      }
+      if (F.p.use2DProjection) pos.y = R(0.5f);
+      const R Lr = R(F.L);
+      R pc[3] = {pos.x, pos.y, pos.z};
+      for (int a = 0; a < 3; ++a) {
+        R x = pc[a];
+        if (x >= Lr) x = x - Lr;
+        else if (x < 0) { x = x + Lr; if (x >= Lr) x = 0; }
+        pc[a] = x;
+      }
+      R* po = &out.pos[4 * (size_t)i];
+      R* wo = &out.fwd[4 * (size_t)i];
+      po[0] = pc[0]; po[1] = pc[1]; po[2] = pc[2]; po[3] = 1;
+      wo[0] = fwd.x; wo[1] = fwd.y; wo[2] = fwd.z; wo[3] = R(sc.s);
+    }
+  });
+}
+
 }  // namespace
 
 extern "C" {
@@ -596,6 +713,7 @@ typedef struct oracle_io {
   uint32_t* lists;                                 // N * (Mmax+1), per sorted slot
   void* steer4;                                    // N * 4, per sorted slot
   uint32_t* scanned;                               // N, candidates examined per sorted slot
+  uint32_t random_step;                            // Schooling random-stream step of this step
 } oracle_io;
 }  // extern "C"
 
@@ -634,7 +752,10 @@ int stepImpl(uint32_t nflocks, const brt_params* params, R dt, const oracle_io* 
   out = st;
   std::vector<R> steer;
   if (io->steer4) steer.resize(4 * (size_t)N);
-  steerIntegrate<R>(S, st, dt, out, io->steer4 ? steer.data() : nullptr, threads);
+  if (params[0].schooling.mode != 0)
+    schoolIntegrate<R>(S, st, out, io->steer4 ? steer.data() : nullptr, io->random_step, threads);
+  else
+    steerIntegrate<R>(S, st, dt, out, io->steer4 ? steer.data() : nullptr, threads);
 
   // scatter back to agent-id order (OpenSteerWrapper_kernel.cu:324-331)
   R* po = (R*)io->pos4_out; R* wo = (R*)io->fwd4_out; R* ao = (R*)io->acc4_out;
