@@ -169,7 +169,8 @@ void freeAll(brt_engine* e) {
       if (e->ev[r][k]) cudaEventDestroy(e->ev[r][k]);
   void* ptrs[] = {e->flocks, e->agentBase, e->obstacles, e->obsMask, e->posA, e->fwdA, e->accA, e->posS, e->fwdS, e->accS,
                   e->featA, e->featS, e->featNormS, e->idA, e->idS, e->statsById, e->steer, e->lists, e->pairs[0], e->pairs[1],
-                  e->cellStart, e->cellEnd, e->sortMem, e->errWord, e->stage4, e->stageF, e->stepCounter};
+                  e->cellStart, e->cellEnd, e->sortMem, e->errWord, e->stage4, e->stageF, e->stepCounter,
+                  e->membership[0], e->membership[1]};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (e->stream) cudaStreamDestroy(e->stream);
@@ -977,6 +978,64 @@ int brt_steer_for_clustering(brt_engine* e) { return steerStage(e, 3); }
 // reference's seek-to-centre force is zero (OpenSteerWrapper_kernel.cu:236-246);
 // this stage applies the static obstacle field of the EnvGrid3D grid instead.
 int brt_compute_seekings_world_center(brt_engine* e) { return steerStage(e, 4); }
+
+// ---- BehaviorClustering analytics --------------------------------------------
+
+static ClusterArgs clusterArgs(brt_engine* e, float radius) {
+  ClusterArgs A;
+  std::memset(&A, 0, sizeof(A));
+  A.posS = e->posS; A.idS = e->idS; A.lists = e->lists; A.listStride = e->listStride;
+  A.flocks = e->flocks; A.agentBase = e->agentBase; A.nflocks = e->nflocks; A.n = e->N;
+  A.radius = radius;
+  A.in = e->membership[e->membershipCur];
+  A.out = e->membership[e->membershipCur ^ 1];
+  return A;
+}
+
+static int clusterReady(brt_engine* e) {
+  if (!e->listsValid) {
+    setLastError("cluster analytics need the neighbour lists (computeNeighborhoods or record_lists)");
+    return BRT_ERR_STATE;
+  }
+  for (int k = 0; k < 2 && !e->membership[k]; ++k) {
+    int rc = devAlloc(&e->membership[k], e->N);
+    if (rc) return rc;
+    BRT_CUDA_TRY(cudaMemsetAsync(e->membership[k], 0, (size_t)e->N * 16, e->stream));
+  }
+  return BRT_OK;
+}
+
+int brt_compute_cluster_membership(brt_engine* e, uint32_t iterations) {
+  if (!e) return BRT_ERR_ARG;
+  DeviceGuard guard(e->device);
+  int rc = clusterReady(e);
+  if (rc || e->N == 0) return rc;
+  for (uint32_t it = 0; it <= iterations; ++it) {
+    BRT_CUDA_TRY(launchCluster(clusterArgs(e, 0.0f), it == 0 ? 0 : 1, e->stream));
+    e->membershipCur ^= 1;
+  }
+  return BRT_OK;
+}
+
+int brt_analyze_cluster_hit_rate(brt_engine* e, float same_cluster_max_radius) {
+  if (!e) return BRT_ERR_ARG;
+  DeviceGuard guard(e->device);
+  int rc = clusterReady(e);
+  if (rc || e->N == 0) return rc;
+  BRT_CUDA_TRY(launchCluster(clusterArgs(e, same_cluster_max_radius), 2, e->stream));
+  e->membershipCur ^= 1;
+  return BRT_OK;
+}
+
+int brt_get_cluster_membership(brt_engine* e, float* membership4, int where) {
+  if (!e || !membership4) return BRT_ERR_ARG;
+  if (!e->membership[0]) { setLastError("no cluster membership computed yet"); return BRT_ERR_STATE; }
+  DeviceGuard guard(e->device);
+  BRT_CUDA_TRY(cudaMemcpyAsync(membership4, e->membership[e->membershipCur], (size_t)e->N * 16,
+                               where == BRT_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, e->stream));
+  if (where == BRT_MEM_HOST) return syncAndCheck(e);
+  return BRT_OK;
+}
 
 static int schoolStage(brt_engine* e, int which) {
   if (!e) return BRT_ERR_ARG;

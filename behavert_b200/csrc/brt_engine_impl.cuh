@@ -28,6 +28,8 @@ struct brt_engine {
   bool anyKnn = false;
   bool school = false;        // the flocks use the Schooling law (schooling.mode 1 or 2)
   uint32_t* stepCounter = nullptr;  // device word: steps taken (keys the Schooling random stream)
+  float4* membership[2] = {nullptr, nullptr};  // clusterMembership by agent id (ping-pong)
+  int membershipCur = 0;
   bool forceTwoPass = false;  // option "two_pass": run the list-first kernel even when not needed
   int phase2Variant = 0;      // option "phase2_variant": list walk one or two neighbours at a time
   int scanVariant = 0;        // option "scan_variant": neighbour-scan loop shape

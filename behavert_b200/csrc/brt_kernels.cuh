@@ -131,6 +131,17 @@ cudaError_t launchIntegrateStage(const StageArgs& A, float dt, cudaStream_t st);
 cudaError_t launchSchool(const FusedArgs& A, cudaStream_t st);
 cudaError_t launchSchoolStage(const StageArgs& A, int which, cudaStream_t st);
 cudaError_t configureSchoolKernels(uint32_t Mmax);
+// BehaviorClustering analytics (brt_cluster.cu): which = 0 reset labels,
+// 1 one propagation sweep, 2 hit rate; in / out are the membership buffers.
+struct ClusterArgs {
+  const float4* posS; const uint32_t* idS;
+  const uint32_t* lists; uint32_t listStride;
+  const FlockDev* flocks; const uint32_t* agentBase;
+  uint32_t nflocks, n;
+  float radius;
+  const float4* in; float4* out;
+};
+cudaError_t launchCluster(const ClusterArgs& A, int which, cudaStream_t st);
 cudaError_t launchScatterToId(const float4* src, const uint32_t* id, float4* dst, uint32_t n, cudaStream_t st);
 cudaError_t launchScatterFeatToId(const float* src, uint32_t Fs, const uint32_t* id, float* dst, uint32_t F, uint32_t n, cudaStream_t st);
 cudaError_t launchLoadFeat(const float* src, uint32_t F, float* dst, uint32_t Fs, uint32_t n, cudaStream_t st);

@@ -198,6 +198,18 @@ class Engine:
         check(lib().brt_get_steer_force(self._h, ptr(out), BRT_MEM_HOST), "getSteerForce")
         return out
 
+    # -- BehaviorClustering analytics ------------------------------------------------
+    def computeClusterMembership(self, iterations: int = 10) -> None:
+        check(lib().brt_compute_cluster_membership(self._h, iterations), "computeClusterMembership")
+
+    def analyzeClusterHitRate(self, same_cluster_max_radius: float = 1.5) -> None:
+        check(lib().brt_analyze_cluster_hit_rate(self._h, same_cluster_max_radius), "analyzeClusterHitRate")
+
+    def getClusterMembership(self) -> np.ndarray:
+        out = np.empty((self.num_agents, 4), np.float32)
+        check(lib().brt_get_cluster_membership(self._h, ptr(out), BRT_MEM_HOST), "getClusterMembership")
+        return out
+
     def autotune(self, dt: float, steps: int = 10) -> dict:
         """Times launch configurations on the current state, keeps the
         fastest and returns the choice with every trial's ms per step."""

@@ -448,6 +448,8 @@ class BehaviorClusteringPlugIn : public Super {
       parseFloat3(c->getSetting("alignmentClusteringForceParams", s), p.alignmentClusteringForceParams);
     if (c->has("similarityStatsParams", s)) parseFloat3(c->getSetting("similarityStatsParams", s), p.similarityStatsParams);
     BRT_READ_PARAM(s, "featureRelaxRate", p.featureRelaxRate, parseFloat);
+    BRT_READ_PARAM(s, "iterationLP", m_IterationLP, parseInt);
+    BRT_READ_PARAM(s, "sameClusterMaxRadius", m_SameClusterMaxRadius, parseFloat);
     SimEnginePlugIn::installPlugIn();
   }
   const std::string name() override { return "BehaviorClusteringPlugIn"; }
@@ -470,6 +472,21 @@ class BehaviorClusteringPlugIn : public Super {
   }
   void update(const float t) override { Super::update(t); }
   void steerForClustering() { check(brt_steer_for_clustering(m_CommonRes.engine()), "steerForClustering"); }
+  // computeClusterMembership / analyzeClusterHitRate (BehaviorClusteringPlugIn.h
+  // :828-894) with the reference's iterationLP = 10 and sameClusterMaxRadius =
+  // 1.5 unless the config section sets them.
+  void computeClusterMembership() {
+    check(brt_compute_cluster_membership(m_CommonRes.engine(), (uint32_t)m_IterationLP), "computeClusterMembership");
+  }
+  void analyzeClusterHitRate() {
+    check(brt_analyze_cluster_hit_rate(m_CommonRes.engine(), m_SameClusterMaxRadius), "analyzeClusterHitRate");
+  }
+  // (label, hit rate, mean close-neighbour label, unused) per agent id
+  std::vector<float4v> getClusterMembership() {
+    std::vector<float4v> out(m_CommonRes.params().numBodies);
+    check(brt_get_cluster_membership(m_CommonRes.engine(), (float*)out.data(), BRT_MEM_HOST), "getClusterMembership");
+    return out;
+  }
   DeviceArrayWrapper<float>* getFeaturesVector() {
     if (!m_Features)
       m_Features.reset(new DeviceArrayWrapper<float>(Feature::Features, (int)m_CommonRes.params().numBodies,
@@ -479,6 +496,61 @@ class BehaviorClusteringPlugIn : public Super {
 
  protected:
   std::unique_ptr<DeviceArrayWrapper<float>> m_Features;
+  int m_IterationLP = 10;
+  float m_SameClusterMaxRadius = 1.5f;
+};
+
+// SchoolingPlugIn (PlugIns/Schooling/include/SchoolingPlugIn.h:60-299): the
+// install-time constants of the reference (SchoolingPlugIn.h:119-148), each
+// overridable from the [SchoolingPlugIn] config section; mode 1 makes the
+// fused step run animateSchool, mode 2 the repulsion / attraction-orientation
+// / movement sequence.  The random deviation comes from a seeded
+// counter-based generator (key "seed") instead of a time-seeded Mersenne
+// Twister.
+template <class Super>
+class SchoolingPlugIn : public Super {
+ public:
+  SchoolingPlugIn() {
+    brt_params& p = m_CommonRes.params();
+    brt_schooling_params& sc = p.schooling;
+    sc.mode = 1;
+    sc.r_p = p.commonSearchRadius;
+    const std::string s = "SchoolingPlugIn";
+    BRT_READ_PARAM(s, "mode", sc.mode, parseInt);
+    BRT_READ_PARAM(s, "theta", sc.theta, parseFloat);
+    BRT_READ_PARAM(s, "delta", sc.delta, parseFloat);
+    BRT_READ_PARAM(s, "r_r", sc.r_r, parseFloat);
+    BRT_READ_PARAM(s, "r_p", sc.r_p, parseFloat);
+    BRT_READ_PARAM(s, "eta", sc.eta, parseFloat);
+    BRT_READ_PARAM(s, "w_a", sc.w_a, parseFloat);
+    BRT_READ_PARAM(s, "w_o", sc.w_o, parseFloat);
+    BRT_READ_PARAM(s, "s", sc.s, parseFloat);
+    BRT_READ_PARAM(s, "randomDeviationWeight", sc.randomDeviationWeight, parseFloat);
+    BRT_READ_PARAM(s, "seed", sc.seed, parseInt);
+    SimEnginePlugIn::installPlugIn();
+  }
+  const std::string name() override { return "SchoolingPlugIn"; }
+  const DependenciesList plugInDependencies() override {
+    return {"Body3DPlugIn", "EnvGrid3DPlugIn", "Proximity3DPlugIn", "OpenSteerWrapperPlugIn"};
+  }
+  // Forward speeds are the constant speed s.
+  void reset() override {
+    Super::reset();
+    brt_params& p = m_CommonRes.params();
+    DeviceArrayWrapper<float4v>* fwd = this->getForward();
+    float4v* host = fwd->getHostArray();
+    for (uint32_t i = 0; i < p.numBodies; ++i) host[i].w = p.schooling.s;
+    fwd->copyArrayToDevice();
+    // restart the random stream, so a reset replays the same run
+    check(brt_engine_set_option(m_CommonRes.engine(), "random_step", 0), "reset random stream");
+  }
+  void update(const float t) override { Super::update(t); }
+  void animateSchool() { check(brt_school_animate(m_CommonRes.engine()), "animateSchool"); }
+  void calcRepulsion() { check(brt_school_repulsion(m_CommonRes.engine()), "calcRepulsion"); }
+  void calcAttractionOrientation() {
+    check(brt_school_attraction_orientation(m_CommonRes.engine()), "calcAttractionOrientation");
+  }
+  void calcMovement() { check(brt_school_movement(m_CommonRes.engine()), "calcMovement"); }
 };
 
 }  // namespace BehaveRT

@@ -253,6 +253,24 @@ int brt_school_attraction_orientation(brt_engine* e); /* calcAttractionOrientati
 int brt_school_movement(brt_engine* e);               /* calcMovement, SchoolingPlugIn.h:268-299              */
 int brt_school_animate(brt_engine* e);                /* animateSchool, SchoolingPlugIn.h:219-232             */
 
+/* ---- BehaviorClustering analytics over the current neighbour lists
+        (after brt_compute_neighborhoods, or a brt_step with record_lists) ----
+   brt_compute_cluster_membership: local label propagation
+   (BehaviorClusteringPlugIn::computeClusterMembership,
+   BehaviorClusteringPlugIn.h:828-871): every agent's label starts as its
+   sorted slot, then `iterations` Jacobi sweeps (the reference uses
+   iterationLP = 10) replace it by the minimum over the agent and its listed
+   neighbours.
+   brt_analyze_cluster_hit_rate (analyzeClusterHitRate, :885-894): among the
+   listed neighbours closer than same_cluster_max_radius (reference 1.5), the
+   fraction sharing the agent's label and the mean of their labels (-1 with
+   none).
+   brt_get_cluster_membership: float4 per agent id (label, hit rate, mean
+   neighbour label, 0), the reference's float3 clusterMembership feature. */
+int brt_compute_cluster_membership(brt_engine* e, uint32_t iterations);
+int brt_analyze_cluster_hit_rate(brt_engine* e, float same_cluster_max_radius);
+int brt_get_cluster_membership(brt_engine* e, float* membership4, int where);
+
 /* ---- getters of the intermediate features --------------------------------- */
 /* Sorted (cell hash, agent id) pairs as uint2, like getHash() after
    reorderSimData (EnvGrid3DPlugIn.h:101-105).  keys/ids may be NULL. */

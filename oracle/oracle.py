@@ -197,3 +197,73 @@ def frozen_reverse(params: Sequence, pos, fwd, acc, lists, gpos_T, gfwd_T=None, 
 def min_image(d, L):
     """Minimum image of offsets in a periodic cube of side L."""
     return d - L * np.round(d / L)
+
+
+# ---------------------------------------------------------------------------
+# BehaviorClustering analytics (BehaviorClusteringPlugIn.h:828-894, kernels
+# BehaviorClustering_kernel.cu:502-652) over the lists of one step.
+
+def cluster_membership(step_out: dict, iterations: int) -> np.ndarray:
+    """Local label propagation: labels (float32, by agent id) start as each
+    agent's sorted slot; each sweep takes the minimum over the agent and its
+    listed neighbours (all reading the previous sweep)."""
+    ids = step_out["ids"]
+    lists = step_out["lists"]
+    n = len(ids)
+    lab = np.empty(n, np.float32)
+    lab[ids] = np.arange(n, dtype=np.float32)
+    cnt = lists[:, 0]
+    valid = np.arange(lists.shape[1] - 1)[None, :] < cnt[:, None]
+    nb = ids[np.where(valid, lists[:, 1:], 0)]
+    for _ in range(iterations):
+        cand = np.where(valid, lab[nb], np.float32(np.inf)).min(axis=1) if valid.shape[1] else np.full(n, np.inf)
+        new = np.empty_like(lab)
+        new[ids] = np.minimum(lab[ids], cand.astype(np.float32))
+        lab = new
+    return lab
+
+
+def cluster_hit_rate(params: Sequence, pos_in, step_out: dict, labels, radius: float) -> np.ndarray:
+    """(label, hit rate, mean close-neighbour label) per agent id: among the
+    listed neighbours closer than `radius` (float32 distance to the neighbour's
+    periodic image), the fraction sharing the label and their mean label, -1
+    without any; sums in list order in float32."""
+    ids = step_out["ids"]
+    lists = step_out["lists"]
+    n = len(ids)
+    L = np.float32(params[0].worldSize)
+    cell = np.float32(params[0].cellSize)
+    G = int(round(float(L) / float(cell)))
+    ps = np.ascontiguousarray(pos_in, np.float32)[ids, :3]
+
+    def grid(x):
+        return np.clip(np.floor(x / cell), 0, G - 1).astype(np.int64)
+
+    gi = grid(ps)
+    my = labels[ids]
+    close = np.zeros(n, np.int64)
+    real = np.zeros(n, np.float32)
+    hit = np.zeros(n, np.float32)
+    cnt = lists[:, 0]
+    for k in range(lists.shape[1] - 1):
+        valid = k < cnt
+        j = np.where(valid, lists[:, 1 + k], 0)
+        q = ps[j].copy()
+        gj = grid(q)
+        shift = np.where((gi == 0) & (gj == G - 1), -L, np.where((gi == G - 1) & (gj == 0), L, np.float32(0)))
+        q = (q + shift.astype(np.float32)).astype(np.float32)
+        d = (q - ps).astype(np.float32)
+        dist = np.sqrt(((d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2]).astype(np.float32))
+        use = valid & ~(dist > np.float32(radius))
+        other = labels[ids[j]]
+        close += use
+        real = np.where(use, (real + other).astype(np.float32), real)
+        hit = np.where(use & (my == other), (hit + np.float32(1)).astype(np.float32), hit)
+    out = np.zeros((n, 4), np.float32)
+    c = close.astype(np.float32)
+    hr = np.where(close > 0, hit / np.where(close > 0, c, 1), hit).astype(np.float32)
+    rl = np.where(close > 0, real / np.where(close > 0, c, 1), np.float32(-1)).astype(np.float32)
+    out[ids, 0] = my
+    out[ids, 1] = hr
+    out[ids, 2] = rl
+    return out
