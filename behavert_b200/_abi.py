@@ -138,6 +138,8 @@ _SIGS = {
     "brt_get_steer_force": (C.c_int, [_vp, _vp, C.c_int]),
     "brt_engine_record_lists": (C.c_int, [_vp, C.c_int]),
     "brt_engine_check_device_error": (C.c_int, [_vp, _u32p]),
+    "brt_save_snapshot": (C.c_int, [_vp, C.c_char_p]),
+    "brt_load_snapshot": (C.c_int, [_vp, C.c_char_p]),
     "brt_compute_cluster_membership": (C.c_int, [_vp, C.c_uint32]),
     "brt_analyze_cluster_hit_rate": (C.c_int, [_vp, C.c_float]),
     "brt_get_cluster_membership": (C.c_int, [_vp, _vp, C.c_int]),

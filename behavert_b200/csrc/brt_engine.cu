@@ -979,6 +979,66 @@ int brt_steer_for_clustering(brt_engine* e) { return steerStage(e, 3); }
 // this stage applies the static obstacle field of the EnvGrid3D grid instead.
 int brt_compute_seekings_world_center(brt_engine* e) { return steerStage(e, 4); }
 
+// ---- on-disk state snapshot ----------------------------------------------------
+
+namespace {
+constexpr char kSnapMagic[8] = {'B', 'R', 'T', 'S', 'N', 'A', 'P', '1'};
+struct SnapHeader {
+  char magic[8];
+  uint32_t version, n, features, nflocks, step, reserved[3];
+};
+}  // namespace
+
+int brt_save_snapshot(brt_engine* e, const char* path) {
+  if (!e || !path) return BRT_ERR_ARG;
+  DeviceGuard guard(e->device);
+  const size_t n = e->N, F = e->Fmax;
+  std::vector<float> pos(4 * n), fwd(4 * n), acc(4 * n), stats(4 * n), feat(n * F);
+  int rc = brt_get_state(e, pos.data(), fwd.data(), acc.data(), F ? feat.data() : nullptr, BRT_MEM_HOST);
+  if (rc) return rc;
+  if ((rc = brt_get_similarity_stats(e, stats.data(), BRT_MEM_HOST))) return rc;
+  SnapHeader h;
+  std::memset(&h, 0, sizeof(h));
+  std::memcpy(h.magic, kSnapMagic, 8);
+  h.version = 1; h.n = e->N; h.features = e->Fmax; h.nflocks = e->nflocks;
+  BRT_CUDA_TRY(cudaMemcpyAsync(&h.step, e->stepCounter, 4, cudaMemcpyDeviceToHost, e->stream));
+  BRT_CUDA_TRY(cudaStreamSynchronize(e->stream));
+  FILE* f = std::fopen(path, "wb");
+  if (!f) { setLastError(std::string("cannot open ") + path + " for writing"); return BRT_ERR_ARG; }
+  bool ok = std::fwrite(&h, sizeof(h), 1, f) == 1;
+  for (const std::vector<float>* v : {&pos, &fwd, &acc, &stats, &feat})
+    ok = ok && (v->empty() || std::fwrite(v->data(), 4, v->size(), f) == v->size());
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) { setLastError(std::string("writing ") + path + " failed"); return BRT_ERR_ARG; }
+  return BRT_OK;
+}
+
+int brt_load_snapshot(brt_engine* e, const char* path) {
+  if (!e || !path) return BRT_ERR_ARG;
+  DeviceGuard guard(e->device);
+  FILE* f = std::fopen(path, "rb");
+  if (!f) { setLastError(std::string("cannot open ") + path); return BRT_ERR_ARG; }
+  SnapHeader h;
+  bool ok = std::fread(&h, sizeof(h), 1, f) == 1 && std::memcmp(h.magic, kSnapMagic, 8) == 0 && h.version == 1;
+  if (ok && (h.n != e->N || h.features != e->Fmax || h.nflocks != e->nflocks)) {
+    std::fclose(f);
+    setLastError("snapshot does not match the engine (agents, features or flocks differ)");
+    return BRT_ERR_CONFIG;
+  }
+  const size_t n = e->N, F = e->Fmax;
+  std::vector<float> pos(4 * n), fwd(4 * n), acc(4 * n), stats(4 * n), feat(n * F);
+  for (std::vector<float>* v : {&pos, &fwd, &acc, &stats, &feat})
+    ok = ok && (v->empty() || std::fread(v->data(), 4, v->size(), f) == v->size());
+  std::fclose(f);
+  if (!ok) { setLastError(std::string(path) + " is not a complete snapshot"); return BRT_ERR_ARG; }
+  int rc = brt_set_state(e, pos.data(), fwd.data(), acc.data(), F ? feat.data() : nullptr, BRT_MEM_HOST);
+  if (rc) return rc;
+  if ((rc = brt_set_similarity_stats(e, stats.data(), BRT_MEM_HOST))) return rc;
+  BRT_CUDA_TRY(cudaMemcpyAsync(e->stepCounter, &h.step, 4, cudaMemcpyHostToDevice, e->stream));
+  BRT_CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return BRT_OK;
+}
+
 // ---- BehaviorClustering analytics --------------------------------------------
 
 static ClusterArgs clusterArgs(brt_engine* e, float radius) {

@@ -198,6 +198,12 @@ class Engine:
         check(lib().brt_get_steer_force(self._h, ptr(out), BRT_MEM_HOST), "getSteerForce")
         return out
 
+    def save_snapshot(self, path) -> None:
+        check(lib().brt_save_snapshot(self._h, str(path).encode()), "brt_save_snapshot")
+
+    def load_snapshot(self, path) -> None:
+        check(lib().brt_load_snapshot(self._h, str(path).encode()), "brt_load_snapshot")
+
     # -- BehaviorClustering analytics ------------------------------------------------
     def computeClusterMembership(self, iterations: int = 10) -> None:
         check(lib().brt_compute_cluster_membership(self._h, iterations), "computeClusterMembership")

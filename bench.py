@@ -179,14 +179,30 @@ def cpu_baseline_leg(w, eng_state_before, gpu_state_after, budget_s=12.0):
     o64 = oracle.step(w.params, pos.astype(np.float64), fwd.astype(np.float64), acc.astype(np.float64),
                       feat.astype(np.float64), dt=w.dt, mode=1, threads=threads, want_intermediates=False)
     gpos, gfwd, gacc, gfeat = gpu_state_after
+    L = float(w.params[0].worldSize)
 
-    def rel(x, y):
+    def stats(x, y, periodic=False):
+        """Normwise (L2) relative error, 99.99th percentile of the per-agent
+        relative error, and the maximum per-agent relative error."""
+        x = np.asarray(x, np.float64)
         y = np.asarray(y, np.float64)
-        return float(np.abs(np.asarray(x, np.float64) - y).max() / max(np.abs(y).max(), 1e-30))
+        d = x - y
+        if periodic:
+            d = d - L * np.round(d / L)
+        scale = np.linalg.norm(y, axis=1)
+        per = np.linalg.norm(d, axis=1) / np.maximum(scale, 1e-30)
+        return {"l2": float(np.linalg.norm(d) / np.linalg.norm(y)), "p9999": float(np.quantile(per, 0.9999)),
+                "max": float(per.max())}
 
     vel = lambda F: F[:, :3].astype(np.float64) * F[:, 3:4]
-    acc_err = {"pos_rel_err_vs_fp64": rel(gpos, o64["pos"]), "vel_rel_err_vs_fp64": rel(vel(gfwd), vel(o64["fwd"])),
-               "feat_rel_err_vs_fp64": rel(gfeat, o64["feat"]), "tolerance": 1e-5}
+    acc_err = {"pos_vs_fp64": stats(gpos[:, :3], o64["pos"][:, :3], periodic=True),
+               "vel_vs_fp64": stats(vel(gfwd), vel(o64["fwd"])),
+               "feat_vs_fp64": stats(gfeat, o64["feat"]),
+               "tolerance": 1e-5,
+               "gate": "l2 and p9999 of each quantity <= tolerance; max reported (a few agents with "
+                       "near-cancelling steering sums are ill-conditioned in FP32 itself)"}
+    acc_err["within_tolerance"] = all(acc_err[k][s] <= 1e-5 for k in ("pos_vs_fp64", "vel_vs_fp64", "feat_vs_fp64")
+                                      for s in ("l2", "p9999"))
     return base, acc_err
 
 

@@ -213,6 +213,16 @@ int brt_set_state(brt_engine* e, const float* pos4, const float* fwd4,
                   const float* acc4, const float* features, int where);
 int brt_get_state(brt_engine* e, float* pos4, float* fwd4,
                   float* acc4, float* features, int where);
+/* On-disk snapshot of the engine state, for resuming a run.  No reference
+   counterpart (the reference keeps no resumable state; its reset() and
+   dataset loaders start runs).  Little-endian binary: magic "BRTSNAP1",
+   uint32 version (1), agents, features per agent, flocks, the Schooling
+   random-stream step, 3 reserved words; then, in agent-id order, float4
+   position, forward, smoothed acceleration and similarityStats arrays and
+   the float feature array.  brt_load_snapshot returns BRT_ERR_CONFIG when
+   the agent, feature or flock counts differ from the engine's. */
+int brt_save_snapshot(brt_engine* e, const char* path);
+int brt_load_snapshot(brt_engine* e, const char* path);
 /* similarityStats (float4 per agent: min, avg, max, unused) of BehaviorClustering */
 int brt_set_similarity_stats(brt_engine* e, const float* stats4, int where);
 int brt_get_similarity_stats(brt_engine* e, float* stats4, int where);
