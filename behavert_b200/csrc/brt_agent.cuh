@@ -234,6 +234,119 @@ __device__ __forceinline__ uint32_t scanNeighborsPipelined(uint32_t self, f3 p, 
   return n;
 }
 
+// Warp-cooperative neighbour lists, one home cell at a time.
+//
+// All agents of a home cell share the same 27 neighbour cells in the same
+// visit order.  The warp's lanes form runs of equal home cell (sorted
+// order); for each run the warp lays the 27 cells' candidates out as one
+// sequence in the reference's visit order (x outer, y, z inner; ascending
+// slot inside a cell), loads 32 consecutive candidates at a time (one per
+// lane), and every agent of the run tests the 32 with one instruction
+// sequence: a ballot of the accepting lanes and a population count below
+// each lane give the position of each accepted candidate in that agent's
+// list.  Lists are identical to the per-agent scan: same candidates, same
+// order, same predicate !(d2 > r2thr) on ((q + s) - p)^2 sums, self excluded,
+// first M kept.  Cells are not culled (culling never changes a list).
+//
+// Called by all 32 lanes of a warp; `active` lanes own an agent (sorted slot
+// `self`, position p, home cell key `key`, flock `flock`).  Each agent's list
+// goes to column laneCol0 + lane of the shared array sList (stride ls).
+// Returns the lane's list length.
+__device__ __forceinline__ uint32_t scanNeighborsCooperative(bool active, uint32_t self, f3 p, uint32_t key,
+                                                             const FlockDev* __restrict__ flocks, uint32_t flock,
+                                                             const uint32_t* __restrict__ cellStart,
+                                                             const uint32_t* __restrict__ cellEnd,
+                                                             const float4* __restrict__ posS, uint32_t* sList,
+                                                             uint32_t ls, uint32_t laneCol0) {
+  const uint32_t full = 0xFFFFFFFFu;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t myKey = active ? key : 0xFFFFFFFFu;
+  const uint32_t prevKey = __shfl_up_sync(full, myKey, 1);
+  const bool head = active && (lane == 0 || prevKey != myKey);
+  uint32_t heads = __ballot_sync(full, head);
+  const uint32_t activeMask = __ballot_sync(full, active);
+  uint32_t n = 0;
+  while (heads) {
+    const uint32_t g0 = __ffs(heads) - 1;
+    heads &= heads - 1;
+    const uint32_t g1 = heads ? (__ffs(heads) - 1) : 32u;
+    // group lanes [g0, g1) among the active ones
+    const uint32_t groupMask = activeMask & (((g1 >= 32u) ? full : ((1u << g1) - 1u)) & ~((1u << g0) - 1u));
+    const uint32_t f = __shfl_sync(full, flock, g0);
+    const FlockDev& fl = flocks[f];
+    const uint32_t M = fl.M;
+    const float thr = fl.r2thr;
+    const uint32_t G = fl.G;
+    // home cell coordinates from the group's first agent
+    const float px = __shfl_sync(full, p.x, g0), py = __shfl_sync(full, p.y, g0), pz = __shfl_sync(full, p.z, g0);
+    const int gx = gridCoord(px, fl.cell, G), gy = gridCoord(py, fl.cell, G), gz = gridCoord(pz, fl.cell, G);
+    // lanes 0..26: one neighbour cell each, in visit order
+    uint32_t segStart = 0, segLen = 0;
+    float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+    if (lane < 27u) {
+      const int ox = (int)(lane / 9u) - 1, oy = (int)((lane / 3u) % 3u) - 1, oz = (int)(lane % 3u) - 1;
+      const int cx = wrapCoord(gx + ox, G), cy = wrapCoord(gy + oy, G), cz = wrapCoord(gz + oz, G);
+      const uint32_t h = fl.cellBase + ((uint32_t)cz * G + (uint32_t)cy) * G + (uint32_t)cx;
+      const uint32_t st = __ldg(&cellStart[h]), en = __ldg(&cellEnd[h]);
+      if (st != kEmpty && en > st) {
+        segStart = st;
+        segLen = en - st;
+        if (fl.maxPerCell && segLen > fl.maxPerCell) segLen = fl.maxPerCell;
+      }
+      sx = imageShift(gx, ox, G, fl.L);
+      sy = imageShift(gy, oy, G, fl.L);
+      sz = imageShift(gz, oz, G, fl.L);
+    }
+    // exclusive prefix of the segment lengths
+    uint32_t incl = segLen;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(full, incl, o);
+      if (lane >= (uint32_t)o) incl += v;
+    }
+    const uint32_t excl = incl - segLen;
+    const uint32_t total = __shfl_sync(full, incl, 31);
+    uint32_t open = groupMask;  // group agents whose list is not full yet
+    for (uint32_t base = 0; base < total && open; base += 32u) {
+      const uint32_t t = base + lane;
+      const bool valid = t < total;
+      // segment of t: the last segment whose exclusive prefix is <= t
+      uint32_t c = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        const uint32_t cand = c + (uint32_t)step;
+        const uint32_t e = __shfl_sync(full, excl, cand & 31u);
+        if (cand < 27u && e <= t) c = cand;
+      }
+      const uint32_t cStart = __shfl_sync(full, segStart, c), cExcl = __shfl_sync(full, excl, c);
+      const float csx = __shfl_sync(full, sx, c), csy = __shfl_sync(full, sy, c), csz = __shfl_sync(full, sz, c);
+      const uint32_t slot = valid ? cStart + (t - cExcl) : 0xFFFFFFFFu;
+      const float4 q = valid ? __ldg(&posS[slot]) : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float qx = q.x + csx, qy = q.y + csy, qz = q.z + csz;
+      for (uint32_t todo = open; todo; todo &= todo - 1u) {
+        const uint32_t a = __ffs(todo) - 1u;
+        const float ax = __shfl_sync(full, p.x, a), ay = __shfl_sync(full, p.y, a), az = __shfl_sync(full, p.z, a);
+        const uint32_t aSelf = __shfl_sync(full, self, a);
+        const uint32_t an = __shfl_sync(full, n, a);
+        const float dx = qx - ax, dy = qy - ay, dz = qz - az;
+        const float d2 = dx * dx + dy * dy + dz * dz;
+        const bool acc = valid && !(d2 > thr) && slot != aSelf;
+        const uint32_t bal = __ballot_sync(full, acc);
+        if (acc) {
+          const uint32_t pos = an + (uint32_t)__popc(bal & ((1u << lane) - 1u));
+          if (pos < M) sList[pos * ls + laneCol0 + a] = slot;
+        }
+        const uint32_t nn = min(M, an + (uint32_t)__popc(bal));
+        if (lane == a) n = nn;
+        if (nn >= M) open &= ~(1u << a);
+      }
+    }
+  }
+  // list entries were written by other lanes of the warp
+  __syncwarp();
+  return n;
+}
+
 // Home-agent context for the steering stages.
 struct AgentCtx {
   f3 pos, fwd;

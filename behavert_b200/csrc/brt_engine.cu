@@ -592,7 +592,7 @@ int brt_engine_set_option(brt_engine* e, const char* key, int64_t value) {
   } else if (k == "phase2_variant") {
     e->phase2Variant = value != 0 ? 1 : 0;
   } else if (k == "scan_variant") {
-    if (value < 0 || value > 3) { setLastError("scan_variant must be in [0, 3]"); return BRT_ERR_ARG; }
+    if (value < 0 || value > 4) { setLastError("scan_variant must be in [0, 4]"); return BRT_ERR_ARG; }
     e->scanVariant = (int)value;
   } else if (k == "block_size") {
     if (value < 32 || value > (int64_t)kFlockMaxThreads || value % 32) {
@@ -890,12 +890,14 @@ int brt_engine_autotune(brt_engine* e, float elapsedTime, uint32_t steps, char* 
   if (!twoPass) {
     bestMs = 1e30;
     const uint32_t blocks[3] = {64, 128, 256};
+    const int scans[3] = {0, 2, 4};  // per agent with / without cell culling, warp-cooperative
+    const char* names[3] = {"block_size/scan0", "block_size/scan2", "block_size/scan4"};
     for (uint32_t bs : blocks)
-      for (int sv = 0; sv < 3 && !rc; ++sv) {
+      for (int s = 0; s < 3 && !rc; ++s) {
         chk(brt_engine_set_option(e, "block_size", bs));
-        chk(brt_engine_set_option(e, "scan_variant", sv));
-        if (!rc) chk(trial(sv == 0 ? "block_size" : (sv == 1 ? "block_size/scan1" : "block_size/scan2"), bs, &ms));
-        if (!rc && ms < bestMs) { bestMs = ms; bestBlock = bs; bestScan = sv; }
+        chk(brt_engine_set_option(e, "scan_variant", scans[s]));
+        if (!rc) chk(trial(names[s], bs, &ms));
+        if (!rc && ms < bestMs) { bestMs = ms; bestBlock = bs; bestScan = scans[s]; }
       }
     if (!rc) { chk(brt_engine_set_option(e, "block_size", bestBlock)); chk(brt_engine_set_option(e, "scan_variant", bestScan)); }
     for (int p2 = 0; p2 < 2 && !rc; ++p2) {

@@ -37,8 +37,13 @@ __device__ __forceinline__ float shiftOf(uint32_t code, float L) {
 template <int FP, int P2, int MINB>
 __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs A) {
   extern __shared__ uint32_t sList[];
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= A.n) return;
+  const uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = i0 < A.n;
+  // The warp-cooperative scan needs every lane of the warp; inactive lanes
+  // take part read-only (mirroring the last agent) and leave after it.
+  const bool coop = A.scanVariant == 4;
+  if (!coop && !active) return;
+  const uint32_t i = active ? i0 : A.n - 1;
   const uint32_t f = A.nflocks == 1 ? 0u : flockOfSlot(A.agentBase, A.nflocks, i);
   const FlockDev& fl = A.flocks[f];
   const float4 p4 = __ldg(&A.posS[i]);
@@ -53,11 +58,18 @@ __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs 
 
   // Phase 1: the neighbour list in the reference's visit order.
   (void)M;
-  const uint32_t n =
-      A.scanVariant == 0 ? scanNeighborsPipelined<4, true>(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls)
-    : A.scanVariant == 1 ? scanNeighborsPipelined<2, true>(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls)
-    : A.scanVariant == 2 ? scanNeighborsPipelined<4, false>(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls)
-                         : scanNeighborsFlat(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls);
+  uint32_t n;
+  if (coop) {
+    const uint32_t key = fl.cellBase + ((uint32_t)gz * G + (uint32_t)gy) * G + (uint32_t)gx;
+    n = scanNeighborsCooperative(active, i, p, key, A.flocks, f, A.cellStart, A.cellEnd, A.posS, sList, ls,
+                                 threadIdx.x & ~31u);
+    if (!active) return;
+  } else {
+    n = A.scanVariant == 0 ? scanNeighborsPipelined<4, true>(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls)
+      : A.scanVariant == 1 ? scanNeighborsPipelined<2, true>(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls)
+      : A.scanVariant == 2 ? scanNeighborsPipelined<4, false>(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls)
+                           : scanNeighborsFlat(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls);
+  }
   if (A.lists) {
     uint32_t* out = A.lists + (size_t)i * A.listStride;
     out[0] = n;

@@ -87,13 +87,27 @@ __device__ __forceinline__ int gridCoord(float x, float cell, uint32_t G) {
 __device__ __forceinline__ int wrapCoord(int c, uint32_t G) {
   return c < 0 ? c + (int)G : (c >= (int)G ? c - (int)G : c);
 }
+// Image shift of the neighbour cell g + o (o in {-1, 0, 1}) seen from home
+// coordinate g: -L when it wraps below 0, +L when it wraps past G - 1.
+// Written on the unwrapped coordinate: the equivalent form
+// (o < 0 && g == 0) ? -L : ((o > 0 && g == G - 1) ? L : 0) was compiled
+// wrongly for sm_100a at -O3 (nvcc 12.9) when o came from lane arithmetic
+// (it returned +L for g = 0, o = +1); a probe checked this form over every
+// (g, o) at the seams and in the interior.
 __device__ __forceinline__ float imageShift(int g, int o, uint32_t G, float L) {
-  return (o < 0 && g == 0) ? -L : ((o > 0 && g == (int)G - 1) ? L : 0.0f);
+  const int c = g + o;
+  return c < 0 ? -L : (c >= (int)G ? L : 0.0f);
 }
 
-// Image shift of a listed neighbour from the two cell coordinates.
+// Image shift of a listed neighbour from the two cell coordinates (the
+// neighbour is at most one cell away modulo the wrap, and G >= 3): a cell
+// difference above 1 means the neighbour is across the lower seam, below -1
+// across the upper one.  Written on the difference for the same reason as
+// imageShift (the comparison form miscompiled in the same probe).
 __device__ __forceinline__ float imageShiftCells(int gi, int gj, uint32_t G, float L) {
-  return (gi == 0 && gj == (int)G - 1) ? -L : ((gi == (int)G - 1 && gj == 0) ? L : 0.0f);
+  (void)G;
+  const int d = gj - gi;
+  return d > 1 ? -L : (d < -1 ? L : 0.0f);
 }
 
 // Flock of a sorted slot (flocks own contiguous slot ranges).

@@ -55,7 +55,8 @@ struct FusedArgs {
   uint32_t listStride;
   uint32_t nflocks, n, Mmax, Fs;
   float dt;
-  int scanVariant;             // 0: pipelined x4 + cell culling, 1: x2 + culling, 2: x4, 3: flat loop
+  int scanVariant;             // 0: pipelined x4 + cell culling, 1: x2 + culling, 2: x4, 3: flat loop,
+                               // 4: warp-cooperative
   const uint32_t* stepCounter; // random-stream step of the Schooling move
 };
 

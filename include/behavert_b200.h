@@ -182,9 +182,11 @@ int brt_engine_set_params(brt_engine* e, uint32_t flock, const brt_params* p);
                               when the single-pass kernel applies (default 0)
      "block_size"       32..256, multiple of 32: threads per block of the
                               single-pass flock kernel (default 128)
-     "scan_variant"     0..3  neighbour-scan loop: 0 four candidates in flight
+     "scan_variant"     0..4  neighbour-scan loop: 0 four candidates in flight
                               with exact cell culling, 1 two in flight with
-                              culling, 2 four without culling, 3 one at a time
+                              culling, 2 four without culling, 3 one at a time,
+                              4 warp-cooperative (a warp tests 32 candidates of
+                              a home cell's neighbourhood per step)
      "phase2_variant"   0/1   list walk one or two neighbours at a time
      "wide_registers"   0/1   the flock kernel built for 128 registers a thread
                               (2 resident 256-thread blocks per SM) instead of 64

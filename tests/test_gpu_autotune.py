@@ -29,6 +29,43 @@ def test_block_sizes_are_bit_identical(block):
         assert np.array_equal(a, b)
 
 
+def _variant_workloads():
+    big = workloads.large(n=1 << 15, steps=2)
+    bat = workloads.batched(num_flocks=12, lo=128, hi=6000, steps=2)
+    cap = workloads.plain(n=4096, L=32.0, steps=2)
+    cap.params[0].maxBodiesPerCell = 3
+    seam = workloads.plain(n=1500, L=12.0, M=32, steps=2)   # 3 cells per side: every cell is on a seam
+    flat = workloads.plain(n=3000, L=32.0, steps=2)
+    flat.params[0].use2DProjection = 1
+    odd = workloads.plain(n=1000, L=32.0, steps=2)          # not a multiple of the warp size
+    return {"large": big, "batched": bat, "cap": cap, "seam": seam, "2d": flat, "odd": odd}
+
+
+@pytest.mark.parametrize("variant", [1, 2, 3, 4])
+@pytest.mark.parametrize("name", ["large", "batched", "cap", "seam", "2d", "odd"])
+def test_scan_variants_are_bit_identical(name, variant):
+    wl = _variant_workloads()[name]
+
+    def run(options):
+        with Engine(wl.params) as eng:
+            for k, v in options:
+                eng.set_option(k, v)
+            eng.record_lists(True)
+            eng.set_state(wl.pos, wl.fwd, wl.acc, wl.feat)
+            eng.step(DT, 2)
+            return eng.getNeighborLists(), eng.get_state()
+
+    ref_lists, ref = run([])
+    lists, out = run([("scan_variant", variant)])
+    assert np.array_equal(lists[:, 0], ref_lists[:, 0])
+    for i in range(len(lists)):
+        n = lists[i, 0]
+        assert np.array_equal(lists[i, 1:1 + n], ref_lists[i, 1:1 + n]), i
+    for a, b in zip(ref, out):
+        if a is not None:
+            assert np.array_equal(a, b)
+
+
 def test_sort_digit_widths_cap_at_four_passes():
     # 18-bit keys with 4-bit digits would need 5 passes; the plan widens them.
     wl = workloads.large(n=1 << 15, L=256.0, steps=2)
