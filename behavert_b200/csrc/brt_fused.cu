@@ -34,14 +34,17 @@ __device__ __forceinline__ float shiftOf(uint32_t code, float L) {
   return code == 1u ? -L : (code == 2u ? L : 0.0f);
 }
 
-template <int FP, int P2, int MINB>
+// SCAN: 0 the per-agent scans (variants 0-3, chosen at run time), 4 the
+// warp-cooperative scan, each its own instantiation so that it gets its own
+// register allocation.
+template <int FP, int P2, int MINB, int SCAN>
 __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs A) {
   extern __shared__ uint32_t sList[];
   const uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = i0 < A.n;
-  // The warp-cooperative scan needs every lane of the warp; inactive lanes
+  // The warp-cooperative scans need every lane of the warp; inactive lanes
   // take part read-only (mirroring the last agent) and leave after it.
-  const bool coop = A.scanVariant == 4;
+  constexpr bool coop = SCAN != 0;
   if (!coop && !active) return;
   const uint32_t i = active ? i0 : A.n - 1;
   const uint32_t f = A.nflocks == 1 ? 0u : flockOfSlot(A.agentBase, A.nflocks, i);
@@ -59,7 +62,7 @@ __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs 
   // Phase 1: the neighbour list in the reference's visit order.
   (void)M;
   uint32_t n;
-  if (coop) {
+  if (SCAN == 4) {
     const uint32_t key = fl.cellBase + ((uint32_t)gz * G + (uint32_t)gy) * G + (uint32_t)gx;
     n = scanNeighborsCooperative(active, i, p, key, A.flocks, f, A.cellStart, A.cellEnd, A.posS, sList, ls,
                                  threadIdx.x & ~31u);
@@ -220,22 +223,31 @@ __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs 
 }
 
 namespace {
+template <int FP, int SCAN>
+void launchFlockScan(const FusedArgs& A, uint32_t blocks, uint32_t block, size_t smem, int phase2, bool wideRegs,
+                     cudaStream_t st) {
+  if constexpr (SCAN == 0) {
+    if (phase2) {
+      if (wideRegs) flockKernel<FP, 1, 2, 0><<<blocks, block, smem, st>>>(A);
+      else flockKernel<FP, 1, 4, 0><<<blocks, block, smem, st>>>(A);
+      return;
+    }
+  }
+  if (wideRegs) flockKernel<FP, 0, 2, SCAN><<<blocks, block, smem, st>>>(A);
+  else flockKernel<FP, 0, 4, SCAN><<<blocks, block, smem, st>>>(A);
+}
 template <int FP>
 cudaError_t launchFlockFP(const FusedArgs& A, uint32_t blocks, uint32_t block, size_t smem, int phase2, bool wideRegs,
                           cudaStream_t st) {
-  if (wideRegs) {
-    if (phase2) flockKernel<FP, 1, 2><<<blocks, block, smem, st>>>(A);
-    else flockKernel<FP, 0, 2><<<blocks, block, smem, st>>>(A);
-  } else {
-    if (phase2) flockKernel<FP, 1, 4><<<blocks, block, smem, st>>>(A);
-    else flockKernel<FP, 0, 4><<<blocks, block, smem, st>>>(A);
-  }
+  if (A.scanVariant == 4) launchFlockScan<FP, 4>(A, blocks, block, smem, phase2, wideRegs, st);
+  else launchFlockScan<FP, 0>(A, blocks, block, smem, phase2, wideRegs, st);
   return cudaGetLastError();
 }
 template <int FP>
 cudaError_t configureFlockFP(int smem) {
-  const void* fns[4] = {(const void*)flockKernel<FP, 0, 4>, (const void*)flockKernel<FP, 1, 4>,
-                        (const void*)flockKernel<FP, 0, 2>, (const void*)flockKernel<FP, 1, 2>};
+  const void* fns[6] = {(const void*)flockKernel<FP, 0, 4, 0>, (const void*)flockKernel<FP, 1, 4, 0>,
+                        (const void*)flockKernel<FP, 0, 2, 0>, (const void*)flockKernel<FP, 1, 2, 0>,
+                        (const void*)flockKernel<FP, 0, 4, 4>, (const void*)flockKernel<FP, 0, 2, 4>};
   for (const void* fn : fns) {
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
@@ -245,9 +257,10 @@ cudaError_t configureFlockFP(int smem) {
 }  // namespace
 
 // phase2 != 0 walks the list two neighbours at a time with their loads issued
-// together.  block: threads per block, a multiple of 32 in [32, 256].
-// wideRegs: compiled for 2 resident 256-thread blocks per SM (up to 128
-// registers a thread) instead of 4 (64 registers).
+// together (per-agent scans only; the cooperative scan's instantiation keeps
+// the one-at-a-time walk, which measured faster for it).  block: threads per block, a multiple of 32
+// in [32, 256].  wideRegs: compiled for 2 resident 256-thread blocks per SM
+// (up to 128 registers a thread) instead of 4 (64 registers).
 cudaError_t launchFlock(const FusedArgs& A, int phase2, uint32_t block, bool wideRegs, cudaStream_t st) {
   if (A.n == 0) return cudaSuccess;
   if (block < 32 || block > kFlockMaxThreads || block % 32) return cudaErrorInvalidValue;

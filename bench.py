@@ -468,6 +468,8 @@ def main():
                     help="run W warm-up + this many single steps and exit (for ncu)")
     ap.add_argument("--profile-adjoint", type=int, default=0,
                     help="run this many config-3 adjoint iterations (taped forward + backward) and exit (for ncu)")
+    ap.add_argument("--profile-flocks", type=int, default=0,
+                    help="with --profile-steps: step the config-2 batched workload cut to this many flocks")
     ap.add_argument("--options", default="",
                     help="engine options key=value,... applied before stepping (replaces the autotuner)")
     args = ap.parse_args()
@@ -499,7 +501,7 @@ def main():
                 eng.adjoint_backward()
         return 0
 
-    w = workloads.large()
+    w = workloads.batched(num_flocks=args.profile_flocks) if args.profile_steps and args.profile_flocks else workloads.large()
     eng = Engine(w.params, device=local)
     options = [kv.split("=") for kv in args.options.split(",") if kv]
     for key, val in options:

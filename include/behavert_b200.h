@@ -188,6 +188,7 @@ int brt_engine_set_params(brt_engine* e, uint32_t flock, const brt_params* p);
                               4 warp-cooperative (a warp tests 32 candidates of
                               a home cell's neighbourhood per step)
      "phase2_variant"   0/1   list walk one or two neighbours at a time
+                              (per-agent scans 0..3 only)
      "wide_registers"   0/1   the flock kernel built for 128 registers a thread
                               (2 resident 256-thread blocks per SM) instead of 64
      "adjoint_graphs"   0/1   capture the adjoint forward/backward as graphs (default 1)
