@@ -142,7 +142,10 @@ __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs 
     }
     if (relaxOn) {
       // computeSimilarity's dot product, then acc += s * f_j, in the
-      // reference's sequential order.
+      // reference's sequential order.  Scalar on purpose: ptxas -O3 for
+      // sm_100a contracts a packed FP32 multiply feeding a packed add into a
+      // fused multiply-add even under --fmad=false and with explicit .rn,
+      // which would change the rounding.
       float dot = 0.0f;
 #pragma unroll
       for (int kk = 0; kk < FP; ++kk) dot += fi[kk] * fj[kk];
