@@ -278,7 +278,7 @@ int enqueueStep(brt_engine* e, float dt, bool record) {
   for (const FlockDev& d : e->flocksHost) twoPass = twoPass || (d.F > 0 && (d.clus != 0.0f || d.aclus != 0.0f));
   if (e->school) BRT_CUDA_TRY(launchSchool(F, e->stream));
   else if (twoPass) BRT_CUDA_TRY(launchFused(F, e->anyKnn, e->stream));
-  else BRT_CUDA_TRY(launchFlock(F, e->phase2Variant, e->fusedBlock, e->wideRegs, e->stream));
+  else BRT_CUDA_TRY(launchFlock(F, e->phase2Variant, e->fusedBlock, e->regBudget, e->stream));
   if (timed) {
     if ((rc = stageMark(e, 4))) return rc;
     e->pending[e->ringPos] = true;
@@ -607,7 +607,13 @@ int brt_engine_set_option(brt_engine* e, const char* key, int64_t value) {
     BRT_CUDA_TRY(cudaStreamSynchronize(e->stream));
     return BRT_OK;  // a value, not a launch configuration: graphs stay valid
   } else if (k == "wide_registers") {
-    e->wideRegs = value != 0;
+    e->regBudget = value != 0 ? 128 : 64;
+  } else if (k == "registers") {
+    if (value != 128 && value != 64 && value != 48 && value != 40) {
+      setLastError("registers must be 128, 64, 48 or 40");
+      return BRT_ERR_ARG;
+    }
+    e->regBudget = (int)value;
   } else if (k == "adjoint_graphs") {
     e->adjointGraphs = value != 0;
   } else if (k == "adjoint_export") {
@@ -886,7 +892,7 @@ int brt_engine_autotune(brt_engine* e, float elapsedTime, uint32_t steps, char* 
   if (!rc) chk(brt_engine_set_option(e, "sort_digit_bits", bestBits));
   uint32_t bestBlock = e->fusedBlock;
   int bestScan = e->scanVariant, bestP2 = e->phase2Variant;
-  bool bestWide = e->wideRegs;
+  int bestRegs = e->regBudget;
   if (!twoPass) {
     bestMs = 1e30;
     const uint32_t blocks[3] = {64, 128, 256};
@@ -906,14 +912,16 @@ int brt_engine_autotune(brt_engine* e, float elapsedTime, uint32_t steps, char* 
       if (!rc && ms <= bestMs) { bestMs = ms; bestP2 = p2; }
     }
     if (!rc) chk(brt_engine_set_option(e, "phase2_variant", bestP2));
-    double wideMs[2] = {1e30, 1e30};
-    for (int wr = 0; wr < 2 && !rc; ++wr) {
-      chk(brt_engine_set_option(e, "wide_registers", wr));
-      if (!rc) chk(trial("wide_registers", wr, &wideMs[wr]));
+    // 48 and 40 only change the cooperative scan's build
+    const int budgets[4] = {64, 128, 48, 40};
+    const int nBudgets = bestScan == 4 ? 4 : 2;
+    bestMs = 1e30;
+    for (int r = 0; r < nBudgets && !rc; ++r) {
+      chk(brt_engine_set_option(e, "registers", budgets[r]));
+      if (!rc) chk(trial("registers", (uint32_t)budgets[r], &ms));
+      if (!rc && ms < bestMs) { bestMs = ms; bestRegs = budgets[r]; }
     }
-    bestWide = wideMs[1] < wideMs[0];
-    bestMs = std::min(wideMs[0], wideMs[1]);
-    if (!rc) chk(brt_engine_set_option(e, "wide_registers", bestWide ? 1 : 0));
+    if (!rc) chk(brt_engine_set_option(e, "registers", bestRegs));
   }
   if (!rc && copyAll(false) != cudaSuccess) { setLastError("autotune restore failed"); rc = BRT_ERR_CUDA; }
   if (!rc) cudaStreamSynchronize(st);
@@ -927,8 +935,8 @@ int brt_engine_autotune(brt_engine* e, float elapsedTime, uint32_t steps, char* 
   if (report && report_len) {
     std::snprintf(buf, sizeof(buf),
                   "{\"sort_digit_bits\": %u, \"block_size\": %u, \"scan_variant\": %d, \"phase2_variant\": %d, "
-                  "\"wide_registers\": %d, \"ms_per_step\": %.6f, \"trials\": [",
-                  bestBits, bestBlock, bestScan, bestP2, bestWide ? 1 : 0, bestMs);
+                  "\"wide_registers\": %d, \"registers\": %d, \"ms_per_step\": %.6f, \"trials\": [",
+                  bestBits, bestBlock, bestScan, bestP2, bestRegs > 64 ? 1 : 0, bestRegs, bestMs);
     std::string out = std::string(buf) + log + "]}";
     std::snprintf(report, report_len, "%s", out.c_str());
   }

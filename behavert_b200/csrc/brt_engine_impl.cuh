@@ -34,7 +34,7 @@ struct brt_engine {
   int phase2Variant = 0;      // option "phase2_variant": list walk one or two neighbours at a time
   int scanVariant = 0;        // option "scan_variant": neighbour-scan loop shape
   uint32_t fusedBlock = 128;  // option "block_size": threads per block of the single-pass flock kernel
-  bool wideRegs = false;      // option "wide_registers": the 128-register build of that kernel
+  int regBudget = 64;         // option "registers" (or "wide_registers"): registers a thread of that kernel
   // state
   float4 *posA = nullptr, *fwdA = nullptr, *accA = nullptr, *posS = nullptr, *fwdS = nullptr, *accS = nullptr;
   float *featA = nullptr, *featS = nullptr, *featNormS = nullptr;

@@ -227,30 +227,35 @@ __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs 
 
 namespace {
 template <int FP, int SCAN>
-void launchFlockScan(const FusedArgs& A, uint32_t blocks, uint32_t block, size_t smem, int phase2, bool wideRegs,
+void launchFlockScan(const FusedArgs& A, uint32_t blocks, uint32_t block, size_t smem, int phase2, int regs,
                      cudaStream_t st) {
   if constexpr (SCAN == 0) {
     if (phase2) {
-      if (wideRegs) flockKernel<FP, 1, 2, 0><<<blocks, block, smem, st>>>(A);
+      if (regs > 64) flockKernel<FP, 1, 2, 0><<<blocks, block, smem, st>>>(A);
       else flockKernel<FP, 1, 4, 0><<<blocks, block, smem, st>>>(A);
       return;
     }
   }
-  if (wideRegs) flockKernel<FP, 0, 2, SCAN><<<blocks, block, smem, st>>>(A);
+  if constexpr (SCAN == 4) {
+    if (regs <= 40) { flockKernel<FP, 0, 6, 4><<<blocks, block, smem, st>>>(A); return; }
+    if (regs <= 48) { flockKernel<FP, 0, 5, 4><<<blocks, block, smem, st>>>(A); return; }
+  }
+  if (regs > 64) flockKernel<FP, 0, 2, SCAN><<<blocks, block, smem, st>>>(A);
   else flockKernel<FP, 0, 4, SCAN><<<blocks, block, smem, st>>>(A);
 }
 template <int FP>
-cudaError_t launchFlockFP(const FusedArgs& A, uint32_t blocks, uint32_t block, size_t smem, int phase2, bool wideRegs,
+cudaError_t launchFlockFP(const FusedArgs& A, uint32_t blocks, uint32_t block, size_t smem, int phase2, int regs,
                           cudaStream_t st) {
-  if (A.scanVariant == 4) launchFlockScan<FP, 4>(A, blocks, block, smem, phase2, wideRegs, st);
-  else launchFlockScan<FP, 0>(A, blocks, block, smem, phase2, wideRegs, st);
+  if (A.scanVariant == 4) launchFlockScan<FP, 4>(A, blocks, block, smem, phase2, regs, st);
+  else launchFlockScan<FP, 0>(A, blocks, block, smem, phase2, regs, st);
   return cudaGetLastError();
 }
 template <int FP>
 cudaError_t configureFlockFP(int smem) {
-  const void* fns[6] = {(const void*)flockKernel<FP, 0, 4, 0>, (const void*)flockKernel<FP, 1, 4, 0>,
+  const void* fns[8] = {(const void*)flockKernel<FP, 0, 4, 0>, (const void*)flockKernel<FP, 1, 4, 0>,
                         (const void*)flockKernel<FP, 0, 2, 0>, (const void*)flockKernel<FP, 1, 2, 0>,
-                        (const void*)flockKernel<FP, 0, 4, 4>, (const void*)flockKernel<FP, 0, 2, 4>};
+                        (const void*)flockKernel<FP, 0, 4, 4>, (const void*)flockKernel<FP, 0, 2, 4>,
+                        (const void*)flockKernel<FP, 0, 5, 4>, (const void*)flockKernel<FP, 0, 6, 4>};
   for (const void* fn : fns) {
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
@@ -262,19 +267,20 @@ cudaError_t configureFlockFP(int smem) {
 // phase2 != 0 walks the list two neighbours at a time with their loads issued
 // together (per-agent scans only; the cooperative scan's instantiation keeps
 // the one-at-a-time walk, which measured faster for it).  block: threads per block, a multiple of 32
-// in [32, 256].  wideRegs: compiled for 2 resident 256-thread blocks per SM
-// (up to 128 registers a thread) instead of 4 (64 registers).
-cudaError_t launchFlock(const FusedArgs& A, int phase2, uint32_t block, bool wideRegs, cudaStream_t st) {
+// in [32, 256].  regs: the register budget a thread is compiled for, 128 (2
+// resident 256-thread blocks per SM), 64 (4 blocks), or for the cooperative
+// scan also 48 and 40 (5 and 6 blocks, more resident warps for some spills).
+cudaError_t launchFlock(const FusedArgs& A, int phase2, uint32_t block, int regs, cudaStream_t st) {
   if (A.n == 0) return cudaSuccess;
   if (block < 32 || block > kFlockMaxThreads || block % 32) return cudaErrorInvalidValue;
   const uint32_t blocks = (A.n + block - 1) / block;
   const uint32_t fp = A.Fs;
   const size_t smem = (size_t)block * A.Mmax * 4;
-  if (fp == 0) return launchFlockFP<0>(A, blocks, block, smem, phase2, wideRegs, st);
-  if (fp <= 4) return launchFlockFP<4>(A, blocks, block, smem, phase2, wideRegs, st);
-  if (fp <= 8) return launchFlockFP<8>(A, blocks, block, smem, phase2, wideRegs, st);
-  if (fp <= 16) return launchFlockFP<16>(A, blocks, block, smem, phase2, wideRegs, st);
-  return launchFlockFP<32>(A, blocks, block, smem, phase2, wideRegs, st);
+  if (fp == 0) return launchFlockFP<0>(A, blocks, block, smem, phase2, regs, st);
+  if (fp <= 4) return launchFlockFP<4>(A, blocks, block, smem, phase2, regs, st);
+  if (fp <= 8) return launchFlockFP<8>(A, blocks, block, smem, phase2, regs, st);
+  if (fp <= 16) return launchFlockFP<16>(A, blocks, block, smem, phase2, regs, st);
+  return launchFlockFP<32>(A, blocks, block, smem, phase2, regs, st);
 }
 
 cudaError_t configureFlockKernels(uint32_t Mmax) {

@@ -127,8 +127,11 @@ struct SortPlan {
   uint32_t shift[4] = {0, 0, 0, 0};
 };
 constexpr uint32_t kSortThreads = 256;
-constexpr uint32_t kSortItems = 8;
-constexpr uint32_t kSortTile = kSortThreads * kSortItems;
+// Items a thread ranks per tile: 16, or 8 for 9-bit digits, whose per-warp
+// digit counters would not fit beside a 4096-item tile in shared memory.
+__host__ __device__ constexpr uint32_t sortItemsFor(uint32_t digitBits) { return digitBits >= 9 ? 8u : 16u; }
+__host__ __device__ constexpr uint32_t sortTileFor(uint32_t digitBits) { return kSortThreads * sortItemsFor(digitBits); }
+constexpr uint32_t kSortMinTile = kSortThreads * 8u;
 
 SortPlan makeSortPlan(uint32_t n, uint32_t bits, uint32_t maxDigitBits);
 // Scratch layout inside one allocation.

@@ -123,7 +123,7 @@ cudaError_t launchAdjointOut(const OutArgs& A, cudaStream_t st);
 cudaError_t launchHash(const HashArgs& A, uint32_t maxBlocks, cudaStream_t st);
 cudaError_t launchReorder(const ReorderArgs& A, cudaStream_t st);
 cudaError_t launchFused(const FusedArgs& A, bool knn, cudaStream_t st);
-cudaError_t launchFlock(const FusedArgs& A, int phase2, uint32_t block, bool wideRegs, cudaStream_t st);
+cudaError_t launchFlock(const FusedArgs& A, int phase2, uint32_t block, int regs, cudaStream_t st);
 cudaError_t launchLists(const StageArgs& A, bool knn, cudaStream_t st);
 cudaError_t launchSteerStage(const StageArgs& A, int which, cudaStream_t st);
 cudaError_t launchIntegrateStage(const StageArgs& A, float dt, cudaStream_t st);

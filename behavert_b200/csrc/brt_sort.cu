@@ -80,8 +80,8 @@ onesweepKernel(const uint2* __restrict__ in, uint2* __restrict__ out, uint32_t n
   constexpr int BINS = 1 << BITS;
   constexpr int T = kSortThreads;
   constexpr int WARPS = T / 32;
-  constexpr int IPT = kSortItems;
-  constexpr int TILE = kSortTile;
+  constexpr int IPT = (int)sortItemsFor(BITS);
+  constexpr int TILE = (int)sortTileFor(BITS);
   constexpr int DPT = (BINS + T - 1) / T;  // digits per thread (consecutive)
 
   __shared__ uint32_t sWarp[WARPS][BINS];
@@ -251,7 +251,7 @@ SortPlan makeSortPlan(uint32_t n, uint32_t bits, uint32_t maxDigitBits) {
   p.passes = std::min(4u, (p.bits + maxDigitBits - 1) / maxDigitBits);
   p.digitBits = std::max(4u, (p.bits + p.passes - 1) / p.passes);
   p.bins = 1u << p.digitBits;
-  p.tiles = (n + kSortTile - 1) / kSortTile;
+  p.tiles = (n + sortTileFor(p.digitBits) - 1) / sortTileFor(p.digitBits);
   for (uint32_t k = 0; k < p.passes; ++k) p.shift[k] = k * p.digitBits;
   return p;
 }
@@ -369,8 +369,9 @@ namespace {
 constexpr uint32_t kNoAllocMaxPairs = 1u << 20;
 constexpr size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
 // Worst case for n <= kNoAllocMaxPairs with 8-bit digits: 4 passes, 256 bins,
-// ceil(2^20 / tile) tiles; plus the ping-pong pairs and the error word.
-constexpr size_t kNoAllocTiles = (kNoAllocMaxPairs + brt::kSortTile - 1) / brt::kSortTile;
+// ceil(2^20 / tile) tiles of the smallest tile size; plus the ping-pong pairs
+// and the error word.
+constexpr size_t kNoAllocTiles = (kNoAllocMaxPairs + brt::kSortMinTile - 1) / brt::kSortMinTile;
 constexpr size_t kNoAllocScratchBytes = a256(4 * 256 * 4) + a256(4 * 4) + a256(4 * kNoAllocTiles * 256 * 4) +
                                         a256((size_t)kNoAllocMaxPairs * 8) + 256;
 

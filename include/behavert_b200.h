@@ -191,6 +191,9 @@ int brt_engine_set_params(brt_engine* e, uint32_t flock, const brt_params* p);
                               (per-agent scans 0..3 only)
      "wide_registers"   0/1   the flock kernel built for 128 registers a thread
                               (2 resident 256-thread blocks per SM) instead of 64
+     "registers"        128, 64, 48 or 40: the flock kernel's register budget
+                              a thread (64 default; 48 and 40 trade spills for
+                              resident warps and apply to scan_variant 4)
      "adjoint_graphs"   0/1   capture the adjoint forward/backward as graphs (default 1)
      "adjoint_export"   0/1   keep the frozen lists and branch flags (brt_adjoint_get_tape)
      "random_step"      uint32 the step counter of the Schooling random stream

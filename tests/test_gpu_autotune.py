@@ -66,6 +66,26 @@ def test_scan_variants_are_bit_identical(name, variant):
             assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("budget", [128, 48, 40])
+@pytest.mark.parametrize("name", ["large", "batched", "seam"])
+def test_register_budgets_are_bit_identical(name, budget):
+    wl = _variant_workloads()[name]
+    ref = _run(wl, 2, [("scan_variant", 4)])
+    out = _run(wl, 2, [("scan_variant", 4), ("registers", budget)])
+    for a, b in zip(ref, out):
+        if a is not None:
+            assert np.array_equal(a, b)
+
+
+def test_bad_register_budget_is_rejected():
+    from behavert_b200._abi import BrtError
+    wl = workloads.plain(n=512, L=32.0, steps=1)
+    with Engine(wl.params) as eng:
+        for bad in (0, 32, 96, 256):
+            with pytest.raises(BrtError):
+                eng.set_option("registers", bad)
+
+
 def test_sort_digit_widths_cap_at_four_passes():
     # 18-bit keys with 4-bit digits would need 5 passes; the plan widens them.
     wl = workloads.large(n=1 << 15, L=256.0, steps=2)
