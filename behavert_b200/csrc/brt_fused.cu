@@ -237,8 +237,8 @@ void launchFlockScan(const FusedArgs& A, uint32_t blocks, uint32_t block, size_t
     }
   }
   if constexpr (SCAN == 4) {
-    if (regs <= 40) { flockKernel<FP, 0, 6, 4><<<blocks, block, smem, st>>>(A); return; }
-    if (regs <= 48) { flockKernel<FP, 0, 5, 4><<<blocks, block, smem, st>>>(A); return; }
+    if (regs <= 40) { flockKernel<FP, 0, 6, SCAN><<<blocks, block, smem, st>>>(A); return; }
+    if (regs <= 48) { flockKernel<FP, 0, 5, SCAN><<<blocks, block, smem, st>>>(A); return; }
   }
   if (regs > 64) flockKernel<FP, 0, 2, SCAN><<<blocks, block, smem, st>>>(A);
   else flockKernel<FP, 0, 4, SCAN><<<blocks, block, smem, st>>>(A);
