@@ -130,6 +130,7 @@ _SIGS = {
     "brt_compute_cohesions": (C.c_int, [_vp]),
     "brt_steer_for_clustering": (C.c_int, [_vp]),
     "brt_compute_seekings_world_center": (C.c_int, [_vp]),
+    "brt_steer_and_slow_to_avoid_neighbors": (C.c_int, [_vp]),
     "brt_apply_steering_forces": (C.c_int, [_vp, C.c_float]),
     "brt_get_hash": (C.c_int, [_vp, _vp, _vp, C.c_int]),
     "brt_get_cell_ranges": (C.c_int, [_vp, _vp, _vp, C.c_int]),

@@ -433,6 +433,47 @@ __device__ __forceinline__ f3 flockingSteer(const AgentCtx& a, const FlockDev& f
   return steer;
 }
 
+// calcSeparation alone (OpenSteerWrapper_resources.cu:166-211): the
+// normalised mean of -offset / |offset|^2 over the listed neighbours inside
+// the separation neighbourhood, zero when there is none.  The per-neighbour
+// operations are those of flockingSteer's separation sum.
+__device__ __forceinline__ f3 separationDir(const AgentCtx& a, const FlockDev& fl, const uint32_t* list, uint32_t ls,
+                                            uint32_t n, const float4* __restrict__ posS) {
+  f3 s = mk3(0.f, 0.f, 0.f);
+  uint32_t c = 0;
+  for (uint32_t k = 0; k < n; ++k) {
+    const f3 other = neighborImage(a, __ldg(&posS[list[k * ls]]), fl);
+    const f3 offset = sub3(other, a.pos);
+    const float d2 = dot3(offset, offset);
+    const float dist = sqrtf(d2);
+    const f3 nrm = mul3(offset, 1.0f / dist);
+    const float cosAngle = dot3(a.fwd, nrm);
+    if (inBoid(dist, cosAngle, fl.minR, fl.sep[1], fl.sep[2])) {
+      s = add3(s, div3(offset, -d2));
+      ++c;
+    }
+  }
+  if (c > 0) s = normalize3(div3(s, (float)c));
+  return s;
+}
+
+// steerToAvoidNeighbors (OpenSteerWrapper_kernel.cu:110-154): the weighted
+// separation force, multiplied by (n - 16) * 0.5 when more than 16 neighbours
+// are listed, and the agent's speed scaled by 0.9 when the force points
+// against its heading (dot < -0.8) or by 1.02 when along it (dot > 0.5).  The
+// thresholds and factors are double literals in the reference, so the
+// comparison and the scaling are done in double.  Returns the force; *speed
+// is updated in place.
+__device__ __forceinline__ f3 avoidNeighbors(const AgentCtx& a, const FlockDev& fl, const uint32_t* list, uint32_t ls,
+                                             uint32_t n, const float4* __restrict__ posS, float* speed) {
+  f3 s = mul3(separationDir(a, fl, list, ls, n, posS), fl.sep[0]);
+  if (n > 16u) s = mul3(s, (float)(n - 16u) * 0.5f);
+  const double d = (double)dot3(s, a.fwd);
+  if (d < -0.8) *speed = (float)((double)*speed * 0.9);
+  else if (d > 0.5) *speed = (float)((double)*speed * 1.02);
+  return s;
+}
+
 // computeSimilarity (BehaviorClustering_resources.cu:156-180); the self norm
 // is the same for every pair and is passed in.
 __device__ __forceinline__ float similarity(const float* fi, float norm1, const float* __restrict__ fj, uint32_t F) {

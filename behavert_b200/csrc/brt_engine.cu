@@ -196,7 +196,7 @@ StageArgs stageArgs(brt_engine* e) {
   std::memset(&A, 0, sizeof(A));
   A.posS = e->posS; A.fwdS = e->fwdS; A.accS = e->accS; A.featS = e->featS; A.idS = e->idS;
   A.posA = e->posA; A.fwdA = e->fwdA; A.accA = e->accA; A.featA = e->featA; A.idA = e->idA;
-  A.statsById = e->statsById; A.steer = e->steer;
+  A.statsById = e->statsById; A.steer = e->steer; A.fwdW = e->fwdS;
   A.cellStart = e->cellStart; A.cellEnd = e->cellEnd;
   A.flocks = e->flocks; A.agentBase = e->agentBase; A.obstacles = e->obstacles; A.obsMask = e->obsMask;
   A.lists = e->lists; A.listStride = e->listStride;
@@ -988,6 +988,7 @@ int brt_steer_for_clustering(brt_engine* e) { return steerStage(e, 3); }
 // reference's seek-to-centre force is zero (OpenSteerWrapper_kernel.cu:236-246);
 // this stage applies the static obstacle field of the EnvGrid3D grid instead.
 int brt_compute_seekings_world_center(brt_engine* e) { return steerStage(e, 4); }
+int brt_steer_and_slow_to_avoid_neighbors(brt_engine* e) { return steerStage(e, 5); }
 
 // ---- on-disk state snapshot ----------------------------------------------------
 

@@ -202,6 +202,14 @@ __global__ void __launch_bounds__(128) steerStageKernel(StageArgs A, int which) 
     A.statsById[id] = st;
   }
   if (which == 4 && fl.numObstacles && fl.obsW != 0.0f) steer = obstacleSteer(a, fl, A.obstacles, A.obsMask, steer);
+  if (which == 5) {
+    // The new speed goes to this agent's own forward entry, which no other
+    // thread reads in this stage; blendIntoSteeringForce adds the force.
+    float speed = a.speed;
+    const f3 s = avoidNeighbors(a, fl, lst + 1, 1, n, A.posS, &speed);
+    A.fwdW[i] = make_float4(a.fwd.x, a.fwd.y, a.fwd.z, speed);
+    steer = add3(s, steer);
+  }
   A.steer[i] = make_float4(steer.x, steer.y, steer.z, 0.0f);
 }
 

@@ -66,6 +66,7 @@ struct StageArgs {
   float4* posA; float4* fwdA; float4* accA; float* featA; uint32_t* idA;
   float4* statsById;
   float4* steer;
+  float4* fwdW;                  // the sorted forwards again, written by the avoid-neighbours stage
   const uint32_t* cellStart; const uint32_t* cellEnd;
   const FlockDev* flocks; const uint32_t* agentBase;
   const float4* obstacles;

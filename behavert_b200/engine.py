@@ -159,8 +159,24 @@ class Engine:
     def computeSeekingsWorldCenter(self) -> None:
         check(lib().brt_compute_seekings_world_center(self._h), "computeSeekingsWorldCenter")
 
+    def steerAndSlowToAvoidNeighbors(self) -> None:
+        check(lib().brt_steer_and_slow_to_avoid_neighbors(self._h), "steerAndSlowToAvoidNeighbors")
+
     def applySteeringForces(self, dt: float) -> None:
         check(lib().brt_apply_steering_forces(self._h, dt), "applySteeringForces")
+
+    def update_crowd(self, dt: float) -> None:
+        """The crowd sample's per-frame sequence (Terrain.h:342-366) without
+        the terrain and camera plugins: separation replaced by
+        steerAndSlowToAvoidNeighbors."""
+        self.reorderSimData()
+        self.computeNeighborhoods()
+        self.resetSteerForce()
+        self.steerAndSlowToAvoidNeighbors()
+        self.computeAlignments()
+        self.computeCohesions()
+        self.computeSeekingsWorldCenter()
+        self.applySteeringForces(dt)
 
     def update_stagewise(self, dt: float) -> None:
         """The BehaveRT_Clustering per-frame sequence, stage by stage."""

@@ -413,6 +413,9 @@ class OpenSteerWrapperPlugIn : public Super {
   void computeAlignments() { check(brt_compute_alignments(m_CommonRes.engine()), "computeAlignments"); }
   void computeCohesions() { check(brt_compute_cohesions(m_CommonRes.engine()), "computeCohesions"); }
   void computeSeekingsWorldCenter() { check(brt_compute_seekings_world_center(m_CommonRes.engine()), "computeSeekingsWorldCenter"); }
+  void steerAndSlowToAvoidNeighbors() {
+    check(brt_steer_and_slow_to_avoid_neighbors(m_CommonRes.engine()), "steerAndSlowToAvoidNeighbors");
+  }
   void applySteeringForces(float elapsedTime) { check(brt_apply_steering_forces(m_CommonRes.engine(), elapsedTime), "applySteeringForces"); }
   DeviceArrayWrapper<float4v>* getForward() {
     if (!m_Forward) m_Forward.reset(new DeviceArrayWrapper<float4v>(Feature::Forward, (int)m_CommonRes.params().numBodies));

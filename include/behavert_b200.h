@@ -260,6 +260,12 @@ int brt_compute_alignments(brt_engine* e);            /* OpenSteerWrapperPlugIn.
 int brt_compute_cohesions(brt_engine* e);             /* OpenSteerWrapperPlugIn.h:350-366   */
 int brt_steer_for_clustering(brt_engine* e);          /* BehaviorClusteringPlugIn.h:740-822 */
 int brt_compute_seekings_world_center(brt_engine* e); /* OpenSteerWrapperPlugIn.h:380-393   */
+/* steerAndSlowToAvoidNeighbors (OpenSteerWrapperPlugIn.h:309-322, kernel
+   OpenSteerWrapper_kernel.cu:110-154): adds the weighted separation force,
+   times (n - 16) * 0.5 above 16 listed neighbours, and scales each agent's
+   speed by 0.9 / 1.02 when that force points against / along its heading
+   (the speed the next stages and brt_apply_steering_forces see). */
+int brt_steer_and_slow_to_avoid_neighbors(brt_engine* e);
 int brt_apply_steering_forces(brt_engine* e, float elapsedTime); /* OpenSteerWrapperPlugIn.h:400-418 */
 /* SchoolingPlugIn functionalities (engines whose flocks have schooling.mode
    1 or 2), after brt_compute_neighborhoods; the first two write the steering

@@ -382,7 +382,8 @@ template <class R> inline V3<R> v3(const R* a) { return mk<R>(a[0], a[1], a[2]);
 // BehaveRT_Clustering.cpp:209-222), obstacle avoidance, then the OpenSteer
 // integration (genericApplySteeringForceD, OpenSteerWrapper_kernel.cu:265-333).
 template <class R>
-void steerIntegrate(const Shared& S, const State<R>& st, R dt, State<R>& out, R* steerOut, int threads) {
+void steerIntegrate(const Shared& S, const State<R>& st, R dt, State<R>& out, R* steerOut, bool avoidNeighbors,
+                    int threads) {
   const uint32_t stride = S.Mmax + 1;
   const uint32_t Fd = S.Fmax;
   parallelFor(S.N, threads, [&](uint32_t b, uint32_t e) {
@@ -404,8 +405,33 @@ void steerIntegrate(const Shared& S, const State<R>& st, R dt, State<R>& out, R*
       }
       V3<R> steer = mk<R>(0, 0, 0);
       const R minR = R(p.commonSensingMinRadius);
+      // The crowd update order replaces computeSeparations by
+      // steerAndSlowToAvoidNeighbors (OpenSteerWrapper_kernel.cu:110-154):
+      // the weighted separation, times (n - 16) * 0.5f above 16 listed
+      // neighbours, and the speed scaled by the double literals 0.9 / 1.02
+      // when the force points against / along the heading.  The new speed is
+      // what every later stage and the integration read.
+      if (avoidNeighbors) {
+        V3<R> s = mk<R>(0, 0, 0);
+        uint32_t cnt = 0;
+        for (uint32_t k = 0; k < n; ++k) {
+          if (inBoidNeighborhood(myPos, img[k], minR, R(p.separationParams[1]), R(p.separationParams[2]), myFwd)) {
+            V3<R> offset = img[k] - myPos;
+            R d2 = dot(offset, offset);
+            s = s + offset / (-d2);
+            ++cnt;
+          }
+        }
+        if (cnt > 0) s = normalize(s / (R)cnt);
+        s = s * R(p.separationParams[0]);
+        if (n > 16u) s = s * R((float)(n - 16u) * 0.5f);
+        const double d = (double)dot(s, myFwd);
+        if (d < -0.8) mySpeed = R((double)mySpeed * 0.9);
+        else if (d > 0.5) mySpeed = R((double)mySpeed * 1.02);
+        steer = s + steer;
+      }
       // calcSeparation (OpenSteerWrapper_resources.cu:166-211), genericSeparationD (:86-105)
-      if (p.separationParams[0] != 0.0f) {
+      if (!avoidNeighbors && p.separationParams[0] != 0.0f) {
         V3<R> s = mk<R>(0, 0, 0);
         uint32_t cnt = 0;
         for (uint32_t k = 0; k < n; ++k) {
@@ -714,6 +740,7 @@ typedef struct oracle_io {
   void* steer4;                                    // N * 4, per sorted slot
   uint32_t* scanned;                               // N, candidates examined per sorted slot
   uint32_t random_step;                            // Schooling random-stream step of this step
+  uint32_t avoid_neighbors;                        // 1: crowd order, steerAndSlowToAvoidNeighbors for separation
 } oracle_io;
 }  // extern "C"
 
@@ -755,7 +782,7 @@ int stepImpl(uint32_t nflocks, const brt_params* params, R dt, const oracle_io* 
   if (params[0].schooling.mode != 0)
     schoolIntegrate<R>(S, st, out, io->steer4 ? steer.data() : nullptr, io->random_step, threads);
   else
-    steerIntegrate<R>(S, st, dt, out, io->steer4 ? steer.data() : nullptr, threads);
+    steerIntegrate<R>(S, st, dt, out, io->steer4 ? steer.data() : nullptr, io->avoid_neighbors != 0, threads);
 
   // scatter back to agent-id order (OpenSteerWrapper_kernel.cu:324-331)
   R* po = (R*)io->pos4_out; R* wo = (R*)io->fwd4_out; R* ao = (R*)io->acc4_out;

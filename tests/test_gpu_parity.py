@@ -169,6 +169,34 @@ def test_stagewise_equals_fused():
             assert np.array_equal(x, y)
 
 
+def test_crowd_order_steer_and_slow_to_avoid_neighbors():
+    """steerAndSlowToAvoidNeighbors in the crowd sample's order, stage by
+    stage through the C-ABI, against the oracle: lists bit-exact, the state
+    within the FP32 / FP64 tolerances (a flipped speed branch would move an
+    agent's speed by 2-10%)."""
+    w = workloads.plain(n=4096, L=40.0, M=32, seed=5, steps=1)
+    with make_engine(w) as eng:
+        pos, fwd, acc, _ = eng.get_state()
+        eng.update_crowd(w.dt)
+        lists = eng.getNeighborLists()
+        gpos, gfwd, gacc, _ = eng.get_state()
+    o = oracle.step(w.params, pos, fwd, acc, dt=w.dt, mode=0, avoid_neighbors=True)
+    cnt = lists[:, 0]
+    assert np.array_equal(cnt, o["lists"][:, 0])
+    assert (cnt > 18).sum() > 100 and (cnt <= 16).sum() > 100
+    mask = np.arange(lists.shape[1] - 1)[None, :] < cnt[:, None]
+    assert np.array_equal(np.where(mask, lists[:, 1:], 0), np.where(mask, o["lists"][:, 1:], 0))
+    assert _rel(gpos, o["pos"]) <= TOL_FP32 and _rel(_vel(gfwd), _vel(o["fwd"])) <= TOL_FP32
+    assert _rel(gacc, o["acc"]) <= 1e-4
+    plain = oracle.step(w.params, pos, fwd, acc, dt=w.dt, mode=0)
+    assert _rel(_vel(gfwd), _vel(plain["fwd"])) > 100 * TOL_FP32
+    o64 = oracle.step(w.params, *(x.astype(np.float64) for x in (pos, fwd, acc)), dt=w.dt, mode=1,
+                      want_intermediates=False, avoid_neighbors=True)
+    assert _rel(gpos, o64["pos"]) <= TOL_FP64
+    e = _fp64_errors("vel", _vel(gfwd), _vel(o64["fwd"]))
+    assert e["vel_l2"] <= TOL_FP64 and e["vel_p9999"] <= TOL_FP64, e
+
+
 def test_single_pass_equals_two_pass():
     """The single-pass fused kernel and the list-first kernel agree bit for bit."""
     w = workloads.large(n=40000)
