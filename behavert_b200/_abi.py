@@ -100,6 +100,24 @@ _vp = C.c_void_p
 _u32p = C.POINTER(C.c_uint32)
 _fp = C.POINTER(C.c_float)
 
+MAX_USER_ARRAYS = 8
+
+
+class BrtArrays(C.Structure):
+    """brt_arrays: a view of the engine's device arrays (raw addresses)."""
+    _fields_ = [
+        ("num_agents", C.c_uint32), ("num_cells", C.c_uint32), ("features_stride", C.c_uint32),
+        ("list_stride", C.c_uint32),
+        ("pos4", _vp), ("forward4", _vp), ("smooth_accel4", _vp), ("features", _vp), ("agent_id", _vp),
+        ("sorted_pos4", _vp), ("sorted_forward4", _vp), ("sorted_smooth_accel4", _vp), ("sorted_features", _vp),
+        ("sorted_agent_id", _vp), ("steer4", _vp), ("neighbor_lists", _vp), ("cell_start", _vp), ("cell_end", _vp),
+        ("num_user", C.c_uint32), ("user_bytes", C.c_uint32 * MAX_USER_ARRAYS), ("user", _vp * MAX_USER_ARRAYS),
+        ("user_agent_id", _vp),
+    ]
+
+
+LAUNCH_FN = C.CFUNCTYPE(None, _vp, _vp, C.POINTER(BrtArrays))
+
 _SIGS = {
     "brt_version": (C.c_char_p, []),
     "brt_error_string": (C.c_char_p, [C.c_int]),
@@ -131,6 +149,11 @@ _SIGS = {
     "brt_steer_for_clustering": (C.c_int, [_vp]),
     "brt_compute_seekings_world_center": (C.c_int, [_vp]),
     "brt_steer_and_slow_to_avoid_neighbors": (C.c_int, [_vp]),
+    "brt_engine_add_array": (C.c_int, [_vp, C.c_uint32, _u32p]),
+    "brt_engine_array_set": (C.c_int, [_vp, C.c_uint32, _vp, C.c_int]),
+    "brt_engine_array_get": (C.c_int, [_vp, C.c_uint32, _vp, C.c_int]),
+    "brt_engine_get_arrays": (C.c_int, [_vp, C.POINTER(BrtArrays)]),
+    "brt_engine_launch": (C.c_int, [_vp, LAUNCH_FN, _vp]),
     "brt_apply_steering_forces": (C.c_int, [_vp, C.c_float]),
     "brt_get_hash": (C.c_int, [_vp, _vp, _vp, C.c_int]),
     "brt_get_cell_ranges": (C.c_int, [_vp, _vp, _vp, C.c_int]),

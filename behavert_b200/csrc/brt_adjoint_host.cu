@@ -186,6 +186,10 @@ int enqueueRecompute(brt_engine* e, uint32_t steps) {
   const size_t n = e->N;
   float4 *posS = e->posS, *fwdS = e->fwdS, *accS = e->accS;
   uint32_t *idS = e->idS, *lists = e->lists;
+  // the engine returns to the forward's final state afterwards, so
+  // registered arrays (already at that state) are not permuted again
+  const bool wasFrozen = e->userFrozen;
+  e->userFrozen = true;
   int rc = BRT_OK;
   for (uint32_t s = 0; s < steps && !rc; ++s) {
     e->posS = a->tPos + s * n; e->fwdS = a->tFwd + s * n; e->accS = a->tAcc + s * n;
@@ -196,6 +200,7 @@ int enqueueRecompute(brt_engine* e, uint32_t steps) {
   }
   e->posS = posS; e->fwdS = fwdS; e->accS = accS; e->idS = idS; e->lists = lists;
   e->tapePrev = nullptr;
+  e->userFrozen = wasFrozen;
   return rc;
 }
 

@@ -173,6 +173,14 @@ void freeAll(brt_engine* e) {
                   e->membership[0], e->membership[1]};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  for (auto& u : e->user) {
+    cudaFree(u.a);
+    cudaFree(u.s);
+  }
+  e->user.clear();
+  if (e->userIds.a) cudaFree(e->userIds.a);
+  if (e->userIds.s) cudaFree(e->userIds.s);
+  if (e->userStage) cudaFree(e->userStage);
   if (e->stream) cudaStreamDestroy(e->stream);
 }
 
@@ -249,6 +257,18 @@ int enqueueReorder(brt_engine* e) {
   R.hist = e->ss.hist; R.histWords = e->plan.passes * e->plan.bins;
   R.n = e->N; R.numCells = e->C; R.errWord = e->errWord;
   BRT_CUDA_TRY(launchReorder(R, st));
+  // registered arrays move with their agents (slot i takes the previous slot
+  // pairs[i].y), the agent-id map with them
+  if (!e->user.empty() && !e->userFrozen) {
+    const uint32_t* prev = reinterpret_cast<const uint32_t*>(e->pairs[e->finalPairs]) + 1;
+    auto permute = [&](brt_engine::UserArray& u) -> cudaError_t {
+      cudaError_t err = launchGatherWords(u.a, prev, 2, u.s, u.words, e->N, st);
+      if (err != cudaSuccess) return err;
+      return cudaMemcpyAsync(u.a, u.s, (size_t)e->N * u.words * 4, cudaMemcpyDeviceToDevice, st);
+    };
+    BRT_CUDA_TRY(permute(e->userIds));
+    for (auto& u : e->user) BRT_CUDA_TRY(permute(u));
+  }
   return stageMark(e, 3);
 }
 
@@ -847,6 +867,11 @@ int brt_engine_autotune(brt_engine* e, float elapsedTime, uint32_t steps, char* 
     return c;
   };
   if (!rc && copyAll(true) != cudaSuccess) { setLastError("autotune snapshot failed"); rc = BRT_ERR_CUDA; }
+  // The trials' steps are undone, so registered arrays stay where they are;
+  // graphs captured while frozen are keyed apart from the others.
+  const bool wasFrozen = e->userFrozen;
+  e->userFrozen = true;
+  e->paramsVersion++;
   // One trial: the steps-step graph launched twice from the snapshot, the
   // faster launch counted.
   auto measure = [&](double* msPerStep) -> int {
@@ -925,6 +950,8 @@ int brt_engine_autotune(brt_engine* e, float elapsedTime, uint32_t steps, char* 
   }
   if (!rc && copyAll(false) != cudaSuccess) { setLastError("autotune restore failed"); rc = BRT_ERR_CUDA; }
   if (!rc) cudaStreamSynchronize(st);
+  e->userFrozen = wasFrozen;
+  e->paramsVersion++;
   e->reordered = false;
   e->listsValid = false;
   if (t0) cudaEventDestroy(t0);
@@ -1176,6 +1203,119 @@ int brt_get_steer_force(brt_engine* e, float* steer4, int where) {
   DeviceGuard guard(e->device);
   BRT_CUDA_TRY(cudaMemcpyAsync(steer4, e->steer, (size_t)e->N * 16, kindOut(where), e->stream));
   if (where == BRT_MEM_HOST) return syncAndCheck(e);
+  return BRT_OK;
+}
+
+// ---- plugin extension: registered arrays, the array view, user launches ----------
+
+int brt_engine_add_array(brt_engine* e, uint32_t bytes_per_agent, uint32_t* array_id) {
+  if (!e || !array_id) return BRT_ERR_ARG;
+  if (bytes_per_agent == 0 || bytes_per_agent % 4 || bytes_per_agent > 1024) {
+    setLastError("bytes_per_agent must be a multiple of 4 in [4, 1024]");
+    return BRT_ERR_ARG;
+  }
+  if (e->user.size() >= BRT_MAX_USER_ARRAYS) { setLastError("too many registered arrays"); return BRT_ERR_CAPACITY; }
+  DeviceGuard guard(e->device);
+  const size_t n = std::max<size_t>(e->N, 1);
+  const uint32_t words = bytes_per_agent / 4;
+  BRT_CUDA_TRY(cudaStreamSynchronize(e->stream));
+  if (!e->userIds.a) {
+    // the id map starts as the engine's current slot order
+    BRT_CUDA_TRY(cudaMalloc(&e->userIds.a, n * 4));
+    BRT_CUDA_TRY(cudaMalloc(&e->userIds.s, n * 4));
+    e->userIds.words = 1;
+    if (e->N) BRT_CUDA_TRY(cudaMemcpyAsync(e->userIds.a, e->idA, (size_t)e->N * 4, cudaMemcpyDeviceToDevice, e->stream));
+  }
+  brt_engine::UserArray u;
+  u.words = words;
+  BRT_CUDA_TRY(cudaMalloc(&u.a, n * words * 4));
+  if (cudaMalloc(&u.s, n * words * 4) != cudaSuccess) {
+    cudaFree(u.a);
+    setLastError("out of device memory");
+    return BRT_ERR_CUDA;
+  }
+  BRT_CUDA_TRY(cudaMemsetAsync(u.a, 0, n * words * 4, e->stream));
+  if (words > e->userStageWords) {
+    if (e->userStage) cudaFree(e->userStage);
+    e->userStage = nullptr;
+    e->userStageWords = 0;
+    BRT_CUDA_TRY(cudaMalloc(&e->userStage, n * words * 4));
+    e->userStageWords = words;
+  }
+  e->user.push_back(u);
+  *array_id = (uint32_t)e->user.size() - 1;
+  e->paramsVersion++;  // captured step graphs must now include the permutation
+  BRT_CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return BRT_OK;
+}
+
+int brt_engine_array_set(brt_engine* e, uint32_t array_id, const void* src, int where) {
+  if (!e || !src || array_id >= e->user.size()) return BRT_ERR_ARG;
+  if (where != BRT_MEM_HOST && where != BRT_MEM_DEVICE) return BRT_ERR_ARG;
+  DeviceGuard guard(e->device);
+  const brt_engine::UserArray& u = e->user[array_id];
+  const size_t bytes = (size_t)e->N * u.words * 4;
+  if (!bytes) return BRT_OK;
+  const uint32_t* s = (const uint32_t*)src;
+  if (where == BRT_MEM_HOST) {
+    BRT_CUDA_TRY(cudaMemcpyAsync(e->userStage, src, bytes, cudaMemcpyHostToDevice, e->stream));
+    s = e->userStage;
+  }
+  // slot i holds agent userIds[i]
+  BRT_CUDA_TRY(launchGatherWords(s, e->userIds.a, 1, u.a, u.words, e->N, e->stream));
+  if (where == BRT_MEM_HOST) return syncAndCheck(e);
+  return BRT_OK;
+}
+
+int brt_engine_array_get(brt_engine* e, uint32_t array_id, void* dst, int where) {
+  if (!e || !dst || array_id >= e->user.size()) return BRT_ERR_ARG;
+  if (where != BRT_MEM_HOST && where != BRT_MEM_DEVICE) return BRT_ERR_ARG;
+  DeviceGuard guard(e->device);
+  const brt_engine::UserArray& u = e->user[array_id];
+  const size_t bytes = (size_t)e->N * u.words * 4;
+  if (!bytes) return BRT_OK;
+  uint32_t* d = where == BRT_MEM_HOST ? e->userStage : (uint32_t*)dst;
+  BRT_CUDA_TRY(launchScatterWords(u.a, e->userIds.a, d, u.words, e->N, e->stream));
+  if (where == BRT_MEM_HOST) {
+    BRT_CUDA_TRY(cudaMemcpyAsync(dst, e->userStage, bytes, cudaMemcpyDeviceToHost, e->stream));
+    return syncAndCheck(e);
+  }
+  return BRT_OK;
+}
+
+int brt_engine_get_arrays(brt_engine* e, brt_arrays* out) {
+  if (!e || !out) return BRT_ERR_ARG;
+  std::memset(out, 0, sizeof(*out));
+  out->num_agents = e->N;
+  out->num_cells = e->C;
+  out->features_stride = e->Fs;
+  out->list_stride = e->listStride;
+  out->pos4 = (float*)e->posA; out->forward4 = (float*)e->fwdA; out->smooth_accel4 = (float*)e->accA;
+  out->features = e->featA;
+  out->agent_id = e->idA;
+  out->sorted_pos4 = (float*)e->posS; out->sorted_forward4 = (float*)e->fwdS;
+  out->sorted_smooth_accel4 = (float*)e->accS; out->sorted_features = e->featS;
+  out->sorted_agent_id = e->idS;
+  out->steer4 = (float*)e->steer;
+  out->neighbor_lists = e->lists;
+  out->cell_start = e->cellStart; out->cell_end = e->cellEnd;
+  out->num_user = (uint32_t)e->user.size();
+  for (size_t k = 0; k < e->user.size(); ++k) {
+    out->user[k] = e->user[k].a;
+    out->user_bytes[k] = e->user[k].words * 4;
+  }
+  out->user_agent_id = e->userIds.a;
+  return BRT_OK;
+}
+
+int brt_engine_launch(brt_engine* e, brt_launch_fn fn, void* user_data) {
+  if (!e || !fn) return BRT_ERR_ARG;
+  DeviceGuard guard(e->device);
+  brt_arrays view;
+  int rc = brt_engine_get_arrays(e, &view);
+  if (rc) return rc;
+  fn(user_data, (void*)e->stream, &view);
+  BRT_CUDA_TRY(cudaGetLastError());
   return BRT_OK;
 }
 

@@ -71,6 +71,19 @@ struct brt_engine {
   bool adjointGraphs = true;  // option "adjoint_graphs"
   bool adjointExport = false; // option "adjoint_export"
   uint32_t weightsVersion = 0; // bumped by brt_set_steering_weights
+  // registered per-agent arrays (brt_engine_add_array): `a` holds the array in
+  // the engine's slot order, `s` is the gather target of each reorder (copied
+  // back to `a`, so captured graphs always read and write the same buffers);
+  // userIds is the agent id of each slot, permuted the same way.
+  struct UserArray {
+    uint32_t words = 0;
+    uint32_t *a = nullptr, *s = nullptr;
+  };
+  std::vector<UserArray> user;
+  UserArray userIds;
+  uint32_t* userStage = nullptr;  // id-order staging, N * max words
+  uint32_t userStageWords = 0;
+  bool userFrozen = false;        // steps whose state is restored afterwards leave the arrays alone
 };
 
 namespace brt {

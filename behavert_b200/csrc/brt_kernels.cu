@@ -311,6 +311,38 @@ cudaError_t launchLists(const StageArgs& A, bool knn, cudaStream_t st) {
   else listsKernel<false><<<blocksFor(A.n, 128), 128, 0, st>>>(A);
   return cudaGetLastError();
 }
+// Registered per-agent arrays of `words` 32-bit words: slot i of dst takes
+// slot index[i * stride] of src (gather), or slot i of src goes to slot
+// index[i] of dst (scatter); one thread per word.
+__global__ void gatherWordsKernel(const uint32_t* __restrict__ src, const uint32_t* __restrict__ index, uint32_t stride,
+                                  uint32_t* __restrict__ dst, uint32_t words, uint32_t n) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (size_t)n * words) return;
+  const size_t i = t / words, k = t - i * words;
+  dst[t] = src[(size_t)__ldg(&index[i * stride]) * words + k];
+}
+__global__ void scatterWordsKernel(const uint32_t* __restrict__ src, const uint32_t* __restrict__ index,
+                                   uint32_t* __restrict__ dst, uint32_t words, uint32_t n) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (size_t)n * words) return;
+  const size_t i = t / words, k = t - i * words;
+  dst[(size_t)__ldg(&index[i]) * words + k] = src[t];
+}
+cudaError_t launchGatherWords(const uint32_t* src, const uint32_t* index, uint32_t stride, uint32_t* dst, uint32_t words,
+                              uint32_t n, cudaStream_t st) {
+  const size_t total = (size_t)n * words;
+  if (total == 0) return cudaSuccess;
+  gatherWordsKernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(src, index, stride, dst, words, n);
+  return cudaGetLastError();
+}
+cudaError_t launchScatterWords(const uint32_t* src, const uint32_t* index, uint32_t* dst, uint32_t words, uint32_t n,
+                               cudaStream_t st) {
+  const size_t total = (size_t)n * words;
+  if (total == 0) return cudaSuccess;
+  scatterWordsKernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(src, index, dst, words, n);
+  return cudaGetLastError();
+}
+
 cudaError_t launchSteerStage(const StageArgs& A, int which, cudaStream_t st) {
   if (A.n == 0) return cudaSuccess;
   steerStageKernel<<<blocksFor(A.n, 128), 128, 0, st>>>(A, which);

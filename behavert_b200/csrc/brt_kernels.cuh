@@ -152,6 +152,12 @@ cudaError_t configureFusedKernels(uint32_t Mmax);
 cudaError_t configureFlockKernels(uint32_t Mmax);
 cudaError_t launchGatherFeatFromId(const float* src, uint32_t F, const uint32_t* id, float* dst, uint32_t Fs, uint32_t n, cudaStream_t st);
 cudaError_t launchHashPairsOut(const uint2* pairs, const uint32_t* idS, uint32_t* keys, uint32_t* ids, uint32_t n, cudaStream_t st);
+// dst[i] = src[index[i * stride]] and dst[index[i]] = src[i] for arrays of
+// `words` 32-bit words per agent.
+cudaError_t launchGatherWords(const uint32_t* src, const uint32_t* index, uint32_t stride, uint32_t* dst, uint32_t words,
+                              uint32_t n, cudaStream_t st);
+cudaError_t launchScatterWords(const uint32_t* src, const uint32_t* index, uint32_t* dst, uint32_t words, uint32_t n,
+                               cudaStream_t st);
 
 uint32_t sortPassMask(const SortPlan& p, uint32_t pass);
 

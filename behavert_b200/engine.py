@@ -116,6 +116,55 @@ class Engine:
         check(lib().brt_get_similarity_stats(self._h, ptr(out), BRT_MEM_HOST), "get_similarity_stats")
         return out
 
+    # -- plugin extension: registered per-agent arrays and user kernels ----------------
+    def add_array(self, bytes_per_agent: int) -> int:
+        """Registers a zero-filled per-agent array that moves with its agents
+        (brt_engine_add_array); returns its id."""
+        out = C.c_uint32(0)
+        check(lib().brt_engine_add_array(self._h, int(bytes_per_agent), C.byref(out)), "brt_engine_add_array")
+        return int(out.value)
+
+    def array_set(self, array_id: int, values) -> None:
+        """Loads a registered array from agent-id order (a host array, or a
+        CUDA tensor)."""
+        nbytes = int(self.get_arrays().user_bytes[int(array_id)]) * self.num_agents
+        have = values.nbytes if isinstance(values, np.ndarray) else values.numel() * values.element_size()
+        if have != nbytes:
+            raise ValueError("array %d holds %d bytes, got %d" % (array_id, nbytes, have))
+        check(lib().brt_engine_array_set(self._h, int(array_id), ptr(values), self._where(values)),
+              "brt_engine_array_set")
+
+    def array_get(self, array_id: int, dtype=np.uint32, shape=None) -> np.ndarray:
+        """A registered array in agent-id order."""
+        nbytes = int(self.get_arrays().user_bytes[int(array_id)])
+        out = np.empty(self.num_agents * nbytes // np.dtype(dtype).itemsize, dtype)
+        check(lib().brt_engine_array_get(self._h, int(array_id), ptr(out), BRT_MEM_HOST), "brt_engine_array_get")
+        return out.reshape(shape if shape is not None else (self.num_agents, -1))
+
+    def get_arrays(self):
+        """The brt_arrays view of the engine's device arrays (raw addresses)."""
+        from ._abi import BrtArrays
+        view = BrtArrays()
+        check(lib().brt_engine_get_arrays(self._h, C.byref(view)), "brt_engine_get_arrays")
+        return view
+
+    def launch(self, fn) -> None:
+        """Calls fn(stream_handle, view) in stream order (brt_engine_launch);
+        fn enqueues its own work on the engine's stream."""
+        from ._abi import LAUNCH_FN
+        errors = []
+
+        def tramp(_user, stream, view):
+            try:
+                fn(int(stream or 0), view.contents)
+            except Exception as exc:  # re-raised once the C call has returned
+                errors.append(exc)
+
+        cb = LAUNCH_FN(tramp)
+        check(lib().brt_engine_launch(self._h, cb, None), "brt_engine_launch")
+        if errors:
+            raise errors[0]
+
     # -- the fused step ---------------------------------------------------------------
     def step(self, dt: float, nsteps: int = 1) -> None:
         check(lib().brt_step(self._h, dt, nsteps), "brt_step")

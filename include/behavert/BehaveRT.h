@@ -23,6 +23,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <fstream>
+#include <functional>
 #include <map>
 #include <memory>
 #include <random>
@@ -119,6 +120,22 @@ class DeviceInterface {
   void threadSync() {
     if (m_Engine) check(brt_sync(m_Engine), "brt_sync");
   }
+  // kernelCall (Core/DeviceInterface.cu:380-458): the before hook, the
+  // caller's launches on the engine stream over the engine's arrays, the
+  // after hook, and an optional synchronisation.  `launch` receives the
+  // stream (a cudaStream_t) and the brt_arrays view.
+  using Launch = std::function<void(void* stream, const brt_arrays& arrays)>;
+  void kernelCall(const Launch& launch, const std::function<void()>& before = {},
+                  const std::function<void()>& after = {}, bool sync = false) {
+    if (!m_Engine) throw std::runtime_error("kernelCall before the engine exists");
+    if (before) before();
+    struct Ctx { const Launch* fn; } ctx{&launch};
+    check(brt_engine_launch(
+              m_Engine, [](void* u, void* s, const brt_arrays* a) { (*static_cast<Ctx*>(u)->fn)(s, *a); }, &ctx),
+          "kernelCall");
+    if (after) after();
+    if (sync) threadSync();
+  }
 
  private:
   int m_Device;
@@ -169,13 +186,21 @@ inline CommonResources m_CommonRes;
 // DeviceArrayWrapper<T>: host image of one engine feature.  The device image
 // is the engine's own array; copyArrayFromDevice / copyArrayToDevice move
 // the whole feature in agent-id order.
-enum class Feature { Position, Forward, SmoothAccel, Features, SimilarityStats, Hash, CellStart, NeighList, SteerForce };
+// Feature::User is a plugin's own per-agent array: registered with the engine
+// (brt_engine_add_array), which moves it with the agents at every reorder;
+// kernels find it as brt_arrays::user[getUserArrayId()].
+enum class Feature { Position, Forward, SmoothAccel, Features, SimilarityStats, Hash, CellStart, NeighList, SteerForce, User };
 
 template <class Type>
 class DeviceArrayWrapper {
  public:
   DeviceArrayWrapper(Feature feature, int size, int dimension = 1)
-      : m_Feature(feature), m_Size(size), m_Dimension(dimension), m_Host((size_t)size * dimension) {}
+      : m_Feature(feature), m_Size(size), m_Dimension(dimension), m_Host((size_t)size * dimension) {
+    if (feature == Feature::User)
+      check(brt_engine_add_array(m_CommonRes.engine(), (uint32_t)(sizeof(Type) * dimension), &m_ArrayId),
+            "brt_engine_add_array");
+  }
+  uint32_t getUserArrayId() const { return m_ArrayId; }
   Type* getHostArray() { return m_Host.data(); }
   int getSize() const { return m_Size; }
   int getElementBytesCount() const { return (int)sizeof(Type) * m_Dimension; }
@@ -208,6 +233,7 @@ class DeviceArrayWrapper {
       case Feature::CellStart: check(brt_get_cell_ranges(e, (uint32_t*)h, nullptr, BRT_MEM_HOST), "getCellStart"); break;
       case Feature::NeighList: check(brt_get_neighbor_lists(e, (uint32_t*)h, BRT_MEM_HOST), "neighList"); break;
       case Feature::SteerForce: check(brt_get_steer_force(e, (float*)h, BRT_MEM_HOST), "steerForce"); break;
+      case Feature::User: check(brt_engine_array_get(e, m_ArrayId, h, BRT_MEM_HOST), "getUserArray"); break;
     }
   }
   void copyArrayToDevice() {
@@ -219,6 +245,7 @@ class DeviceArrayWrapper {
       case Feature::SmoothAccel: check(brt_set_state(e, nullptr, nullptr, h, nullptr, BRT_MEM_HOST), "setSmoothAccel"); break;
       case Feature::Features: check(brt_set_state(e, nullptr, nullptr, nullptr, h, BRT_MEM_HOST), "setFeatures"); break;
       case Feature::SimilarityStats: check(brt_set_similarity_stats(e, h, BRT_MEM_HOST), "setSimilarityStats"); break;
+      case Feature::User: check(brt_engine_array_set(e, m_ArrayId, h, BRT_MEM_HOST), "setUserArray"); break;
       default: throw std::runtime_error("feature is computed by the engine and cannot be written");
     }
   }
@@ -229,6 +256,7 @@ class DeviceArrayWrapper {
   Feature m_Feature;
   int m_Size, m_Dimension;
   std::vector<Type> m_Host;
+  uint32_t m_ArrayId = 0;
 };
 
 // ---------------------------------------------------------------------------

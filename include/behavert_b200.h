@@ -316,6 +316,51 @@ int brt_engine_record_lists(brt_engine* e, int enable);
    fired inside a kernel; cleared by this call. */
 int brt_engine_check_device_error(brt_engine* e, uint32_t* word);
 
+/* ---- plugin extension: per-agent arrays and user kernels -------------------
+   A reference plugin keeps per-agent features in the device data repository
+   (DataInfo table, devicedata.cuh:51-70, through DeviceArrayWrapper,
+   DeviceArrayWrapper.h:74-168) and launches its own kernels over them with
+   DeviceInterface::kernelCall (Core/DeviceInterface.cu:380-458).
+
+   brt_engine_add_array registers a per-agent array of bytes_per_agent bytes
+   (a multiple of 4, at most 1024; at most BRT_MAX_USER_ARRAYS arrays),
+   zero-filled.  The engine permutes it with the agents at every reorder, as
+   the reference reorders registered features, so slot i always belongs to
+   agent user_agent_id[i] of brt_arrays.  brt_engine_array_set / _get copy it
+   from / to agent-id order.
+
+   brt_engine_get_arrays fills a view of the engine's device arrays (borrowed:
+   valid until the engine is destroyed or its parameters change).
+   brt_engine_launch calls fn(user_data, stream, &view) on the calling thread;
+   fn enqueues its kernels on `stream`, the engine's stream, so they run in
+   order with the engine's stages (the before / after hooks of kernelCall are
+   the code around its launches).  The state arrays are in the engine's slot
+   order (agent_id maps slot to agent); the sorted_* arrays, steer4 and
+   neighbor_lists are those of the current step, valid after
+   brt_reorder_sim_data / brt_compute_neighborhoods, and the state arrays and
+   the registered arrays share the sorted order once a step completes. */
+#define BRT_MAX_USER_ARRAYS 8
+typedef struct brt_arrays {
+  uint32_t num_agents, num_cells, features_stride, list_stride;
+  float* pos4; float* forward4; float* smooth_accel4; float* features;
+  const uint32_t* agent_id;
+  float* sorted_pos4; float* sorted_forward4; float* sorted_smooth_accel4; float* sorted_features;
+  const uint32_t* sorted_agent_id;
+  float* steer4;
+  const uint32_t* neighbor_lists;  /* [n, slot...] per sorted slot, stride list_stride */
+  const uint32_t* cell_start; const uint32_t* cell_end;
+  uint32_t num_user;
+  uint32_t user_bytes[BRT_MAX_USER_ARRAYS];
+  void* user[BRT_MAX_USER_ARRAYS];
+  const uint32_t* user_agent_id;
+} brt_arrays;
+typedef void (*brt_launch_fn)(void* user_data, void* stream, const brt_arrays* arrays);
+int brt_engine_add_array(brt_engine* e, uint32_t bytes_per_agent, uint32_t* array_id);
+int brt_engine_array_set(brt_engine* e, uint32_t array_id, const void* src, int where);
+int brt_engine_array_get(brt_engine* e, uint32_t array_id, void* dst, int where);
+int brt_engine_get_arrays(brt_engine* e, brt_arrays* out);
+int brt_engine_launch(brt_engine* e, brt_launch_fn fn, void* user_data);
+
 /* ---- differentiable rollout ---------------------------------------------------
    No counterpart in the reference (BehaveRT has no differentiation).
    Neighbour sets and branch decisions (inBoidNeighborhood memberships, the

@@ -11,9 +11,14 @@ LIB_DIR = ROOT / "behavert_b200"
 APPS = [("flocking_facade", "flocking.cfg"), ("schooling_facade", "schooling.cfg")]
 
 
-def _build(name: str, out: Path):
+CUDA = Path("/usr/local/cuda")
+
+
+def _build(name: str, out: Path, cuda: bool = False):
     cmd = ["g++", "-std=c++17", "-O2", "-I", str(ROOT / "include"), str(ROOT / "tests" / "cpp" / (name + ".cpp")),
            "-o", str(out), "-L", str(LIB_DIR), "-lbehavert_b200", "-Wl,-rpath," + str(LIB_DIR)]
+    if cuda:
+        cmd += ["-I", str(CUDA / "include"), "-L", str(CUDA / "lib64"), "-lcudart", "-Wl,-rpath," + str(CUDA / "lib64")]
     subprocess.run(cmd, check=True, capture_output=True, text=True)
 
 
@@ -34,3 +39,20 @@ def test_facade_stagewise_equals_fused(tmp_path, name, cfg):
     print(res.stdout, res.stderr)
     assert res.returncode == 0, res.stdout + res.stderr
     assert "stage-wise == fused: yes" in res.stdout
+
+
+def test_plugin_application_builds(tmp_path):
+    _build("plugin_facade", tmp_path / "plugin_facade", cuda=True)
+
+
+@pytest.mark.gpu
+def test_plugin_arrays_and_kernel_call(tmp_path):
+    """A user plugin's own per-agent arrays (Feature::User) follow their agents
+    through fused and stage-wise steps, and kernelCall runs its device work in
+    stream order with the before / after hooks."""
+    exe = tmp_path / "plugin_facade"
+    _build("plugin_facade", exe, cuda=True)
+    res = subprocess.run([str(exe), str(ROOT / "tests" / "cpp" / "flocking.cfg")], capture_output=True, text=True)
+    print(res.stdout, res.stderr)
+    assert res.returncode == 0, res.stdout + res.stderr
+    assert "snapshot follows its agents: yes" in res.stdout
