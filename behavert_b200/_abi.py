@@ -149,6 +149,7 @@ _SIGS = {
     "brt_steer_for_clustering": (C.c_int, [_vp]),
     "brt_compute_seekings_world_center": (C.c_int, [_vp]),
     "brt_steer_and_slow_to_avoid_neighbors": (C.c_int, [_vp]),
+    "brt_steer_for_move_away_base_target": (C.c_int, [_vp, _vp, _vp]),
     "brt_engine_add_array": (C.c_int, [_vp, C.c_uint32, _u32p]),
     "brt_engine_array_set": (C.c_int, [_vp, C.c_uint32, _vp, C.c_int]),
     "brt_engine_array_get": (C.c_int, [_vp, C.c_uint32, _vp, C.c_int]),

@@ -1016,6 +1016,21 @@ int brt_steer_for_clustering(brt_engine* e) { return steerStage(e, 3); }
 // this stage applies the static obstacle field of the EnvGrid3D grid instead.
 int brt_compute_seekings_world_center(brt_engine* e) { return steerStage(e, 4); }
 int brt_steer_and_slow_to_avoid_neighbors(brt_engine* e) { return steerStage(e, 5); }
+int brt_steer_for_move_away_base_target(brt_engine* e, const float* base3, const float* params3) {
+  if (!e || !base3) return BRT_ERR_ARG;
+  if (!e->reordered || !e->listsValid) { setLastError("steering stage before computeNeighborhoods"); return BRT_ERR_STATE; }
+  DeviceGuard guard(e->device);
+  StageArgs A = stageArgs(e);
+  // OpenSteerWrapperPlugIn.h:144-150: (500, 500, 1000) when the weight is 0
+  const float defaults[3] = {500.0f, 500.0f, 1000.0f};
+  const float* p = (params3 && params3[0] != 0.0f) ? params3 : defaults;
+  for (int k = 0; k < 3; ++k) {
+    A.avoidBase[k] = base3[k];
+    A.avoidBaseParams[k] = p[k];
+  }
+  BRT_CUDA_TRY(launchSteerStage(A, 6, e->stream));
+  return BRT_OK;
+}
 
 // ---- on-disk state snapshot ----------------------------------------------------
 

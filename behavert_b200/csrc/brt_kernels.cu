@@ -210,6 +210,18 @@ __global__ void __launch_bounds__(128) steerStageKernel(StageArgs A, int which) 
     A.fwdW[i] = make_float4(a.fwd.x, a.fwd.y, a.fwd.z, speed);
     steer = add3(s, steer);
   }
+  if (which == 6) {
+    // moveAwayFromTarget_kernel (OpenSteerWrapper_kernel.cu:185-212): flee the
+    // base point, (weight * offset) / distance, nothing beyond twice the
+    // radius.  The kernel's acceleration write is overwritten by its own copy
+    // of the old value, so the smoothed acceleration is left as it is.  As in
+    // the reference: the direct offset (no periodic image), and 0/0 for an
+    // agent exactly at the base point.
+    f3 s = sub3(a.pos, mk3(A.avoidBase[0], A.avoidBase[1], A.avoidBase[2]));
+    const float d = len3(s);
+    if (d > A.avoidBaseParams[2] * 2.0f) s = mk3(0.f, 0.f, 0.f);
+    steer = add3(div3(mul3(s, A.avoidBaseParams[0]), d), steer);
+  }
   A.steer[i] = make_float4(steer.x, steer.y, steer.z, 0.0f);
 }
 

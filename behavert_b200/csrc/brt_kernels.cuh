@@ -67,6 +67,8 @@ struct StageArgs {
   float4* statsById;
   float4* steer;
   float4* fwdW;                  // the sorted forwards again, written by the avoid-neighbours stage
+  float avoidBase[3];            // move-away stage: the point to flee
+  float avoidBaseParams[3];      //   (steering weight, acceleration factor, radius)
   const uint32_t* cellStart; const uint32_t* cellEnd;
   const FlockDev* flocks; const uint32_t* agentBase;
   const float4* obstacles;

@@ -214,16 +214,26 @@ class Engine:
     def applySteeringForces(self, dt: float) -> None:
         check(lib().brt_apply_steering_forces(self._h, dt), "applySteeringForces")
 
-    def update_crowd(self, dt: float) -> None:
+    def steerForMoveAwayBaseTarget(self, base, params=None) -> None:
+        """Flee the point `base` (avoidBase); params = avoidBaseParams
+        (weight, acceleration factor, radius), None for the defaults."""
+        b = np.ascontiguousarray(base, np.float32).reshape(3)
+        p = None if params is None else np.ascontiguousarray(params, np.float32).reshape(3)
+        check(lib().brt_steer_for_move_away_base_target(self._h, ptr(b), ptr(p)), "steerForMoveAwayBaseTarget")
+
+    def update_crowd(self, dt: float, avoid_base=None, avoid_base_params=None) -> None:
         """The crowd sample's per-frame sequence (Terrain.h:342-366) without
-        the terrain and camera plugins: separation replaced by
-        steerAndSlowToAvoidNeighbors."""
+        the terrain plugin: separation replaced by steerAndSlowToAvoidNeighbors,
+        and, when avoid_base is given, the move-away-from-base stage after
+        cohesion."""
         self.reorderSimData()
         self.computeNeighborhoods()
         self.resetSteerForce()
         self.steerAndSlowToAvoidNeighbors()
         self.computeAlignments()
         self.computeCohesions()
+        if avoid_base is not None:
+            self.steerForMoveAwayBaseTarget(avoid_base, avoid_base_params)
         self.computeSeekingsWorldCenter()
         self.applySteeringForces(dt)
 

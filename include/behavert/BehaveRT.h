@@ -413,8 +413,19 @@ class OpenSteerWrapperPlugIn : public Super {
     BRT_READ_PARAM(s, "commonMaxSpeed", p.commonMaxSpeed, parseFloat);
     BRT_READ_PARAM(s, "commonMaxForce", p.commonMaxForce, parseFloat);
     BRT_READ_PARAM(s, "commonSensingMinRadius", p.commonSensingMinRadius, parseFloat);
+    // avoidBaseParams with the defaults of OpenSteerWrapperPlugIn.h:141-150
+    if (c->has("avoidBaseParams", s)) parseFloat3(c->getSetting("avoidBaseParams", s), avoidBaseParams);
+    if (avoidBaseParams[0] == 0.0f) {
+      avoidBaseParams[0] = 500.0f;
+      avoidBaseParams[1] = 500.0f;
+      avoidBaseParams[2] = 1000.0f;
+    }
     SimEnginePlugIn::installPlugIn();
   }
+  // hOpenSteerWrapperParams.avoidBase / avoidBaseParams: set by the
+  // application before steerForMoveAwayBaseTarget, as the reference's do.
+  float avoidBase[3] = {0.0f, 0.0f, 0.0f};
+  float avoidBaseParams[3] = {0.0f, 0.0f, 0.0f};
   const std::string name() override { return "OpenSteerWrapperPlugIn"; }
   const DependenciesList plugInDependencies() override { return {"EnvGrid3DPlugIn", "Proximity3DPlugIn"}; }
   // OpenSteerWrapperPlugIn::reset (:195-263): random unit forward, w = maxSpeed.
@@ -443,6 +454,10 @@ class OpenSteerWrapperPlugIn : public Super {
   void computeSeekingsWorldCenter() { check(brt_compute_seekings_world_center(m_CommonRes.engine()), "computeSeekingsWorldCenter"); }
   void steerAndSlowToAvoidNeighbors() {
     check(brt_steer_and_slow_to_avoid_neighbors(m_CommonRes.engine()), "steerAndSlowToAvoidNeighbors");
+  }
+  void steerForMoveAwayBaseTarget() {
+    check(brt_steer_for_move_away_base_target(m_CommonRes.engine(), avoidBase, avoidBaseParams),
+          "steerForMoveAwayBaseTarget");
   }
   void applySteeringForces(float elapsedTime) { check(brt_apply_steering_forces(m_CommonRes.engine(), elapsedTime), "applySteeringForces"); }
   DeviceArrayWrapper<float4v>* getForward() {

@@ -266,6 +266,15 @@ int brt_compute_seekings_world_center(brt_engine* e); /* OpenSteerWrapperPlugIn.
    speed by 0.9 / 1.02 when that force points against / along its heading
    (the speed the next stages and brt_apply_steering_forces see). */
 int brt_steer_and_slow_to_avoid_neighbors(brt_engine* e);
+/* steerForMoveAwayBaseTarget (OpenSteerWrapperPlugIn.h:428-440, kernel
+   OpenSteerWrapper_kernel.cu:185-212): adds (w * (p - base)) / |p - base|, and
+   nothing beyond twice the radius, to every agent's steering force.
+   base3 = avoidBase; params3 = avoidBaseParams (steering weight w,
+   acceleration factor, radius), NULL or w = 0 for the reference's defaults
+   (500, 500, 1000).  As in the reference: the direct offset (no periodic
+   image), the smoothed acceleration left unchanged (the kernel's own write
+   of it is overwritten), and 0/0 for an agent exactly at the base point. */
+int brt_steer_for_move_away_base_target(brt_engine* e, const float* base3, const float* params3);
 int brt_apply_steering_forces(brt_engine* e, float elapsedTime); /* OpenSteerWrapperPlugIn.h:400-418 */
 /* SchoolingPlugIn functionalities (engines whose flocks have schooling.mode
    1 or 2), after brt_compute_neighborhoods; the first two write the steering

@@ -383,7 +383,7 @@ template <class R> inline V3<R> v3(const R* a) { return mk<R>(a[0], a[1], a[2]);
 // integration (genericApplySteeringForceD, OpenSteerWrapper_kernel.cu:265-333).
 template <class R>
 void steerIntegrate(const Shared& S, const State<R>& st, R dt, State<R>& out, R* steerOut, bool avoidNeighbors,
-                    int threads) {
+                    const float* moveAway, int threads) {
   const uint32_t stride = S.Mmax + 1;
   const uint32_t Fd = S.Fmax;
   parallelFor(S.N, threads, [&](uint32_t b, uint32_t e) {
@@ -505,6 +505,16 @@ void steerIntegrate(const Shared& S, const State<R>& st, R dt, State<R>& out, R*
           if (n > 0) s = normalize((s / (R)n) - myFwd) * R(p.alignmentClusteringForceParams[0]);
           steer = s + steer;
         }
+      }
+      // moveAwayFromTarget_kernel (OpenSteerWrapper_kernel.cu:185-212), in the
+      // crowd order after cohesion: (w * (p - base)) / |p - base|, zero beyond
+      // twice the radius; the direct offset, as in the reference.  Its
+      // acceleration write is overwritten by the old value (no effect).
+      if (moveAway) {
+        V3<R> s = myPos - mk<R>(R(moveAway[0]), R(moveAway[1]), R(moveAway[2]));
+        R d = length(s);
+        if (d > R(moveAway[5]) * R(2)) s = mk<R>(0, 0, 0);
+        steer = ((s * R(moveAway[3])) / d) + steer;
       }
       // Static sphere obstacles: flee every sphere whose centre is closer
       // than radius + commonSearchRadius, with a linear falloff to zero at
@@ -741,6 +751,9 @@ typedef struct oracle_io {
   uint32_t* scanned;                               // N, candidates examined per sorted slot
   uint32_t random_step;                            // Schooling random-stream step of this step
   uint32_t avoid_neighbors;                        // 1: crowd order, steerAndSlowToAvoidNeighbors for separation
+  uint32_t move_away;                              // 1: the move-away-from-base stage after cohesion
+  float avoid_base[3];                             // its base point
+  float avoid_base_params[3];                      // (steering weight, acceleration factor, radius)
 } oracle_io;
 }  // extern "C"
 
@@ -781,8 +794,12 @@ int stepImpl(uint32_t nflocks, const brt_params* params, R dt, const oracle_io* 
   if (io->steer4) steer.resize(4 * (size_t)N);
   if (params[0].schooling.mode != 0)
     schoolIntegrate<R>(S, st, out, io->steer4 ? steer.data() : nullptr, io->random_step, threads);
-  else
-    steerIntegrate<R>(S, st, dt, out, io->steer4 ? steer.data() : nullptr, io->avoid_neighbors != 0, threads);
+  else {
+    const float moveAway[6] = {io->avoid_base[0], io->avoid_base[1], io->avoid_base[2],
+                               io->avoid_base_params[0], io->avoid_base_params[1], io->avoid_base_params[2]};
+    steerIntegrate<R>(S, st, dt, out, io->steer4 ? steer.data() : nullptr, io->avoid_neighbors != 0,
+                      io->move_away ? moveAway : nullptr, threads);
+  }
 
   // scatter back to agent-id order (OpenSteerWrapper_kernel.cu:324-331)
   R* po = (R*)io->pos4_out; R* wo = (R*)io->fwd4_out; R* ao = (R*)io->acc4_out;

@@ -25,7 +25,8 @@ class OracleIO(C.Structure):
         ("pos4_out", _vp), ("fwd4_out", _vp), ("acc4_out", _vp), ("feat_out", _vp), ("stats4_out", _vp),
         ("sorted_keys", _vp), ("sorted_ids", _vp), ("cell_start", _vp), ("cell_end", _vp),
         ("lists", _vp), ("steer4", _vp), ("scanned", _vp), ("random_step", C.c_uint32),
-        ("avoid_neighbors", C.c_uint32),
+        ("avoid_neighbors", C.c_uint32), ("move_away", C.c_uint32),
+        ("avoid_base", C.c_float * 3), ("avoid_base_params", C.c_float * 3),
     ]
 
 
@@ -75,11 +76,13 @@ def num_cells(params: Sequence) -> int:
 
 def step(params: Sequence, pos, fwd, acc, feat=None, stats=None, dt: float = 0.1, mode: int = 0,
          threads: int = 0, want_intermediates: bool = True, random_step: int = 0,
-         avoid_neighbors: bool = False) -> dict:
+         avoid_neighbors: bool = False, move_away=None) -> dict:
     """One oracle step.  mode 0: float32 in/out; mode 1: float64 in/out.
     random_step: the step of the Schooling random stream (schooling.mode 2).
     avoid_neighbors: the crowd sample's order (Terrain.h:342-366), with
     steerAndSlowToAvoidNeighbors in place of computeSeparations.
+    move_away: (base xyz, (weight, acceleration factor, radius)) for the
+    steerForMoveAwayBaseTarget stage after cohesion, or None.
 
     Returns the id-ordered new state and, when asked, the sorted keys/ids,
     cell ranges, neighbour lists (stride Mmax+1) and the steering force per
@@ -111,7 +114,9 @@ def step(params: Sequence, pos, fwd, acc, feat=None, stats=None, dt: float = 0.1
                   _p(out["pos"]), _p(out["fwd"]), _p(out["acc"]), _p(out["feat"]), _p(out["stats"]),
                   _p(out.get("keys")), _p(out.get("ids")), _p(out.get("cell_start")), _p(out.get("cell_end")),
                   _p(out.get("lists")), _p(out.get("steer")), _p(out.get("scanned")), int(random_step),
-                  int(bool(avoid_neighbors)))
+                  int(bool(avoid_neighbors)), int(move_away is not None),
+                  (C.c_float * 3)(*([0.0] * 3 if move_away is None else [float(x) for x in move_away[0]])),
+                  (C.c_float * 3)(*([0.0] * 3 if move_away is None else [float(x) for x in move_away[1]])))
     arr = (BrtParams * len(params))(*params)
     if threads <= 0:
         threads = min(hardware_threads(), int(os.environ.get("BRT_ORACLE_THREADS", "64")))

@@ -197,6 +197,29 @@ def test_crowd_order_steer_and_slow_to_avoid_neighbors():
     assert e["vel_l2"] <= TOL_FP64 and e["vel_p9999"] <= TOL_FP64, e
 
 
+def test_crowd_order_with_move_away_from_base():
+    """The crowd order with steerForMoveAwayBaseTarget after cohesion, stage
+    by stage through the C-ABI, against the oracle."""
+    w = workloads.plain(n=4096, L=40.0, M=32, seed=6, steps=1)
+    base, prm = (20.0, 15.0, 25.0), (2.0, 500.0, 8.0)
+    with make_engine(w) as eng:
+        pos, fwd, acc, _ = eng.get_state()
+        eng.update_crowd(w.dt, avoid_base=base, avoid_base_params=prm)
+        lists = eng.getNeighborLists()
+        gpos, gfwd, gacc, _ = eng.get_state()
+    o = oracle.step(w.params, pos, fwd, acc, dt=w.dt, mode=0, avoid_neighbors=True, move_away=(base, prm))
+    assert np.array_equal(lists[:, 0], o["lists"][:, 0])
+    assert _rel(gpos, o["pos"]) <= TOL_FP32 and _rel(_vel(gfwd), _vel(o["fwd"])) <= TOL_FP32
+    assert _rel(gacc, o["acc"]) <= 1e-4
+    without = oracle.step(w.params, pos, fwd, acc, dt=w.dt, mode=0, avoid_neighbors=True)
+    assert _rel(_vel(gfwd), _vel(without["fwd"])) > 100 * TOL_FP32
+    o64 = oracle.step(w.params, *(x.astype(np.float64) for x in (pos, fwd, acc)), dt=w.dt, mode=1,
+                      want_intermediates=False, avoid_neighbors=True, move_away=(base, prm))
+    assert _rel(gpos, o64["pos"]) <= TOL_FP64
+    e = _fp64_errors("vel", _vel(gfwd), _vel(o64["fwd"]))
+    assert e["vel_l2"] <= TOL_FP64 and e["vel_p9999"] <= TOL_FP64, e
+
+
 def test_single_pass_equals_two_pass():
     """The single-pass fused kernel and the list-first kernel agree bit for bit."""
     w = workloads.large(n=40000)

@@ -66,3 +66,21 @@ def test_fp32_close_to_fp64():
     va = a["fwd"][:, :3] * a["fwd"][:, 3:4]
     vb = b["fwd"][:, :3] * b["fwd"][:, 3:4]
     assert np.linalg.norm(va - vb) / np.linalg.norm(vb) < 1e-5
+
+
+def test_move_away_from_base_force():
+    """steerForMoveAwayBaseTarget alone: (w * (p - base)) / |p - base| within
+    twice the radius, zero beyond (OpenSteerWrapper_kernel.cu:185-212)."""
+    w = _crowd()
+    w.params[0].separationParams[0] = 0.0
+    base, prm = (20.0, 15.0, 25.0), (2.0, 500.0, 8.0)
+    f64 = [a.astype(np.float64) for a in (w.pos, w.fwd, w.acc)]
+    o = oracle.step(w.params, *f64, dt=0.1, mode=1, move_away=(base, prm))
+    p = f64[0][o["ids"], :3]
+    off = p - np.array(base)
+    d = np.linalg.norm(off, axis=1)
+    expect = np.where((d > 2 * prm[2])[:, None], 0.0, prm[0] * off / d[:, None])
+    assert (d <= 2 * prm[2]).sum() > 100 and (d > 2 * prm[2]).sum() > 100
+    assert np.allclose(o["steer"][:, :3], expect, rtol=1e-12, atol=1e-12)
+    plain = oracle.step(w.params, *f64, dt=0.1, mode=1)
+    assert np.all(plain["steer"][:, :3] == 0.0)
