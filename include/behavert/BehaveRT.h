@@ -321,7 +321,16 @@ class EnvGrid3DPlugIn : public Super {
     const std::string cs = m_CommonRes.getConfig()->getSetting("cellSize", s);
     if (!cs.empty()) { parseFloat3(cs, cell); p.cellSize = cell[0]; }
     BRT_READ_PARAM(s, "worldSize", p.worldSize, parseFloat);
-    BRT_READ_PARAM(s, "maxBodiesPerCell", p.maxBodiesPerCell, parseInt);
+    // setupMaxBodiesPerCell (EnvGrid3DPlugIn.h:537-562): the configured cap,
+    // or with useAutomaticMaxBodiesPerCell the upper bound
+    // 1 + cellVolume / bodyVolume, bodyVolume = 4.1866 r^3 of the body radius
+    if (parseBool(m_CommonRes.getConfig()->getSetting("useAutomaticMaxBodiesPerCell", s))) {
+      const float cellVolume = cell[0] * cell[1] * cell[2];
+      const float bodyVolume = 4.1866f * p.commonRadius * p.commonRadius * p.commonRadius;
+      if (bodyVolume > 0.0f) p.maxBodiesPerCell = (uint32_t)(int)(1.0f + cellVolume / bodyVolume);
+    } else {
+      BRT_READ_PARAM(s, "maxBodiesPerCell", p.maxBodiesPerCell, parseInt);
+    }
     SimEnginePlugIn::installPlugIn();
   }
   const std::string name() override { return "EnvGrid3DPlugIn"; }

@@ -56,3 +56,19 @@ def test_plugin_arrays_and_kernel_call(tmp_path):
     print(res.stdout, res.stderr)
     assert res.returncode == 0, res.stdout + res.stderr
     assert "snapshot follows its agents: yes" in res.stdout
+
+
+@pytest.mark.parametrize("cfg,cap", [("automatic_cap.cfg", 16), ("flocking.cfg", 0)])
+def test_configuration_mapping(tmp_path, cfg, cap):
+    """The reference's key names reach the engine parameters; with
+    useAutomaticMaxBodiesPerCell the per-cell cap is the reference's upper
+    bound 1 + cellVolume / bodyVolume (EnvGrid3DPlugIn.h:537-562).  CPU only:
+    the engine is created lazily and no functionality is called."""
+    exe = tmp_path / "config_facade"
+    _build("config_facade", exe)
+    res = subprocess.run([str(exe), str(ROOT / "tests" / "cpp" / cfg)], capture_output=True, text=True)
+    assert res.returncode == 0, res.stdout + res.stderr
+    fields = res.stdout.split()
+    got = dict(zip(fields[0::2], fields[1::2]))
+    assert int(got["maxBodiesPerCell"]) == cap
+    assert int(got["numBodies"]) == (1 << 10 if cfg == "automatic_cap.cfg" else 1 << 12)
