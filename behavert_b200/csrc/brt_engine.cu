@@ -168,7 +168,7 @@ void freeAll(brt_engine* e) {
     for (int k = 0; k < 5; ++k)
       if (e->ev[r][k]) cudaEventDestroy(e->ev[r][k]);
   void* ptrs[] = {e->flocks, e->agentBase, e->obstacles, e->obsMask, e->posA, e->fwdA, e->accA, e->posS, e->fwdS, e->accS,
-                  e->featA, e->featS, e->featNormS, e->idA, e->idS, e->statsById, e->steer, e->lists, e->pairs[0], e->pairs[1],
+                  e->featA, e->featS, e->idA, e->idS, e->statsById, e->steer, e->lists, e->pairs[0], e->pairs[1],
                   e->cellStart, e->cellEnd, e->sortMem, e->errWord, e->stage4, e->stageF, e->stepCounter,
                   e->membership[0], e->membership[1]};
   for (void* p : ptrs)
@@ -250,7 +250,6 @@ int enqueueReorder(brt_engine* e) {
   R.pairs = e->pairs[e->finalPairs];
   R.posA = e->posA; R.fwdA = e->fwdA; R.accA = e->accA; R.featA = e->featA; R.idA = e->idA;
   R.posS = e->posS; R.fwdS = e->fwdS; R.accS = e->accS; R.featS = e->featS; R.idS = e->idS;
-  R.featNormS = e->featNormS;
   R.prevOut = e->tapePrev;
   R.fs4 = e->Fs / 4;
   R.cellStart = e->cellStart; R.cellEnd = e->cellEnd;
@@ -283,7 +282,6 @@ int enqueueStep(brt_engine* e, float dt, bool record) {
   FusedArgs F;
   std::memset(&F, 0, sizeof(F));
   F.posS = e->posS; F.fwdS = e->fwdS; F.accS = e->accS; F.featS = e->featS; F.idS = e->idS;
-  F.featNormS = e->featNormS;
   F.posA = e->posA; F.fwdA = e->fwdA; F.accA = e->accA; F.featA = e->featA; F.idA = e->idA;
   F.statsById = e->statsById;
   F.cellStart = e->cellStart; F.cellEnd = e->cellEnd;
@@ -490,7 +488,6 @@ int brt_engine_create(const brt_params* flocks, uint32_t num_flocks, int device,
   chk(devAlloc(&e->posA, n)); chk(devAlloc(&e->fwdA, n)); chk(devAlloc(&e->accA, n));
   chk(devAlloc(&e->posS, n)); chk(devAlloc(&e->fwdS, n)); chk(devAlloc(&e->accS, n));
   chk(devAlloc(&e->featA, n * e->Fs)); chk(devAlloc(&e->featS, n * e->Fs));
-  if (e->Fs) chk(devAlloc(&e->featNormS, n));
   chk(devAlloc(&e->idA, n)); chk(devAlloc(&e->idS, n));
   chk(devAlloc(&e->statsById, n));
   chk(devAlloc(&e->steer, n));

@@ -37,7 +37,7 @@ struct brt_engine {
   int regBudget = 64;         // option "registers" (or "wide_registers"): registers a thread of that kernel
   // state
   float4 *posA = nullptr, *fwdA = nullptr, *accA = nullptr, *posS = nullptr, *fwdS = nullptr, *accS = nullptr;
-  float *featA = nullptr, *featS = nullptr, *featNormS = nullptr;
+  float *featA = nullptr, *featS = nullptr;
   uint32_t *idA = nullptr, *idS = nullptr;
   float4* statsById = nullptr;
   float4* steer = nullptr;

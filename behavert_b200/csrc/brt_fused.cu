@@ -6,7 +6,8 @@
 // list; phase 2 walks the list once, in list order, accumulating separation,
 // alignment, cohesion (OpenSteerWrapper_resources.cu:166-290) and the
 // feature-relaxation sums with the features held in registers and each
-// neighbour's feature norm precomputed by the reorder kernel.  (Folding the
+// neighbour's feature norm precomputed by the reorder kernel (carried in the w
+// of its sorted position).  (Folding the
 // sums into the scan itself makes every scan iteration pay for the warp's
 // accepting lanes, which measured slower.)
 //
@@ -100,7 +101,7 @@ __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs 
     }
 #pragma unroll
     for (int k = 0; k < FP; ++k) facc[k] = 0.0f;
-    n1 = __ldg(&A.featNormS[i]);
+    n1 = p4.w;  // the reorder stores each agent's feature norm in its sorted position's w
   }
   f3 sSep = mk3(0.f, 0.f, 0.f), sAli = mk3(0.f, 0.f, 0.f), sCoh = mk3(0.f, 0.f, 0.f);
   uint32_t cSep = 0, cAli = 0, cCoh = 0;
@@ -155,7 +156,7 @@ __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs 
       for (int kk = 0; kk < FP; ++kk) facc[kk] += s * fj[kk];
     }
   };
-  auto loadFeat = [&](uint32_t j, float* fj, float& n2) {
+  auto loadFeat = [&](uint32_t j, float* fj) {
     if (relaxOn) {
       const float4* src = reinterpret_cast<const float4*>(A.featS) + (size_t)j * fs4;
 #pragma unroll
@@ -163,17 +164,17 @@ __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs 
         const float4 v = (uint32_t)qq < fs4 ? __ldg(&src[qq]) : make_float4(0.f, 0.f, 0.f, 0.f);
         fj[4 * qq + 0] = v.x; fj[4 * qq + 1] = v.y; fj[4 * qq + 2] = v.z; fj[4 * qq + 3] = v.w;
       }
-      n2 = __ldg(&A.featNormS[j]);
     }
   };
   const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
   if (P2 == 0) {
     for (uint32_t k = 0; k < n; ++k) {
       const uint32_t j = list[k * ls] & kSlotMask;
+      const float4 q = __ldg(&A.posS[j]);
       float fj[FP > 0 ? FP : 1];
-      float n2 = 0.0f;
-      loadFeat(j, fj, n2);
-      visit(__ldg(&A.posS[j]), aliOn ? __ldg(&A.fwdS[j]) : zero4, fj, n2);
+      float n2 = q.w;  // the neighbour's feature norm
+      loadFeat(j, fj);
+      visit(q, aliOn ? __ldg(&A.fwdS[j]) : zero4, fj, n2);
     }
   } else {
     for (uint32_t k = 0; k < n; k += 2) {
@@ -183,9 +184,9 @@ __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs 
       const float4 q0 = __ldg(&A.posS[j0]), q1 = __ldg(&A.posS[j1]);
       const float4 w0 = aliOn ? __ldg(&A.fwdS[j0]) : zero4, w1 = aliOn ? __ldg(&A.fwdS[j1]) : zero4;
       float f0[FP > 0 ? FP : 1], f1[FP > 0 ? FP : 1];
-      float n20 = 0.0f, n21 = 0.0f;
-      loadFeat(j0, f0, n20);
-      loadFeat(j1, f1, n21);
+      float n20 = q0.w, n21 = q1.w;
+      loadFeat(j0, f0);
+      loadFeat(j1, f1);
       visit(q0, w0, f0, n20);
       if (two) visit(q1, w1, f1, n21);
     }

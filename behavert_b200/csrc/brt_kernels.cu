@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(256) reorderKernel(ReorderArgs A) {
     if (ps >= A.n || key >= A.numCells) { atomicOr(A.errWord, kDevErrOrder); continue; }
     const uint32_t prev = i > 0 ? A.pairs[i - 1].x : kEmpty;
     const uint32_t next = i + 1 < A.n ? A.pairs[i + 1].x : kEmpty;
-    A.posS[i] = __ldg(&A.posA[ps]);
+    float4 pos = __ldg(&A.posA[ps]);
     A.fwdS[i] = __ldg(&A.fwdA[ps]);
     A.accS[i] = __ldg(&A.accA[ps]);
     A.idS[i] = __ldg(&A.idA[ps]);
@@ -78,6 +78,9 @@ __global__ void __launch_bounds__(256) reorderKernel(ReorderArgs A) {
       // The feature norm sqrtf(sum f^2) (computeSimilarity's norma,
       // BehaviorClustering_resources.cu:164-175) is the same for every pair
       // an agent takes part in: compute it once here, in the same order.
+      // It also goes into the sorted position's w (no kernel reads the w
+      // of a position; integration always writes 1), so the list walk gets
+      // a neighbour's norm with the neighbour's position.
       const float4* src = reinterpret_cast<const float4*>(A.featA) + (size_t)ps * A.fs4;
       float4* dst = reinterpret_cast<float4*>(A.featS) + (size_t)i * A.fs4;
       float nn = 0.0f;
@@ -89,8 +92,9 @@ __global__ void __launch_bounds__(256) reorderKernel(ReorderArgs A) {
         nn += v.z * v.z;
         nn += v.w * v.w;
       }
-      if (A.featNormS) A.featNormS[i] = sqrtf(nn);
+      pos.w = sqrtf(nn);
     }
+    A.posS[i] = pos;
     if (key != prev) A.cellStart[key] = i;
     if (key != next) A.cellEnd[key] = i + 1;
   }

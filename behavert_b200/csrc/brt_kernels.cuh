@@ -32,7 +32,6 @@ struct ReorderArgs {
   const float4* posA; const float4* fwdA; const float4* accA;
   const float* featA; const uint32_t* idA;
   float4* posS; float4* fwdS; float4* accS; float* featS; uint32_t* idS;
-  float* featNormS;            // sqrtf(sum f^2) per sorted slot (optional)
   uint32_t* prevOut;           // source slot per sorted slot (optional, adjoint tape)
   uint32_t fs4;                // feature float4s per agent
   uint32_t* cellStart; uint32_t* cellEnd;
@@ -44,7 +43,6 @@ struct ReorderArgs {
 struct FusedArgs {
   const float4* posS; const float4* fwdS; const float4* accS;
   const float* featS; const uint32_t* idS;
-  const float* featNormS;
   float4* posA; float4* fwdA; float4* accA; float* featA; uint32_t* idA;
   float4* statsById;
   const uint32_t* cellStart; const uint32_t* cellEnd;

@@ -347,7 +347,9 @@ int brt_engine_check_device_error(brt_engine* e, uint32_t* word);
    order (agent_id maps slot to agent); the sorted_* arrays, steer4 and
    neighbor_lists are those of the current step, valid after
    brt_reorder_sim_data / brt_compute_neighborhoods, and the state arrays and
-   the registered arrays share the sorted order once a step completes. */
+   the registered arrays share the sorted order once a step completes.  In an
+   engine with features, sorted_pos4's w holds each agent's feature norm
+   (the state's pos4 keeps w = 1). */
 #define BRT_MAX_USER_ARRAYS 8
 typedef struct brt_arrays {
   uint32_t num_agents, num_cells, features_stride, list_stride;
