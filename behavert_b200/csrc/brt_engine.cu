@@ -607,7 +607,8 @@ int brt_engine_set_option(brt_engine* e, const char* key, int64_t value) {
   if (k == "two_pass") {
     e->forceTwoPass = value != 0;
   } else if (k == "phase2_variant") {
-    e->phase2Variant = value != 0 ? 1 : 0;
+    if (value < 0 || value > 2) { setLastError("phase2_variant must be in [0, 2]"); return BRT_ERR_ARG; }
+    e->phase2Variant = (int)value;
   } else if (k == "scan_variant") {
     if (value < 0 || value > 4) { setLastError("scan_variant must be in [0, 4]"); return BRT_ERR_ARG; }
     e->scanVariant = (int)value;
@@ -928,7 +929,7 @@ int brt_engine_autotune(brt_engine* e, float elapsedTime, uint32_t steps, char* 
         if (!rc && ms < bestMs) { bestMs = ms; bestBlock = bs; bestScan = scans[s]; }
       }
     if (!rc) { chk(brt_engine_set_option(e, "block_size", bestBlock)); chk(brt_engine_set_option(e, "scan_variant", bestScan)); }
-    for (int p2 = 0; p2 < 2 && !rc; ++p2) {
+    for (int p2 = 0; p2 < 3 && !rc; ++p2) {
       chk(brt_engine_set_option(e, "phase2_variant", p2));
       if (!rc) chk(trial("phase2_variant", p2, &ms));
       if (!rc && ms <= bestMs) { bestMs = ms; bestP2 = p2; }

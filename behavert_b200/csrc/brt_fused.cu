@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs 
   (void)interior;
   // One listed neighbour: its image position, forward and features are
   // loaded by the caller so that several neighbours' loads can be in flight.
-  auto visit = [&](const float4 q4, const float4 wj, const float* fj, float n2) {
+  auto visitGeom = [&](const float4 q4, const float4 wj) {
     const f3 img = neighborImage(a, q4, fl);
     const float qx = img.x, qy = img.y, qz = img.z;
     const float dx = qx - p.x, dy = qy - p.y, dz = qz - p.z;
@@ -141,6 +141,8 @@ __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs 
       sCoh = add3(sCoh, mk3(qx, qy, qz));
       ++cCoh;
     }
+  };
+  auto visitFeat = [&](const float* fj, float n2) {
     if (relaxOn) {
       // computeSimilarity's dot product, then acc += s * f_j, in the
       // reference's sequential order.  Scalar on purpose: ptxas -O3 for
@@ -155,6 +157,10 @@ __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs 
 #pragma unroll
       for (int kk = 0; kk < FP; ++kk) facc[kk] += s * fj[kk];
     }
+  };
+  auto visit = [&](const float4 q4, const float4 wj, const float* fj, float n2) {
+    visitGeom(q4, wj);
+    visitFeat(fj, n2);
   };
   auto loadFeat = [&](uint32_t j, float* fj) {
     if (relaxOn) {
@@ -175,6 +181,22 @@ __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs 
       float n2 = q.w;  // the neighbour's feature norm
       loadFeat(j, fj);
       visit(q, aliOn ? __ldg(&A.fwdS[j]) : zero4, fj, n2);
+    }
+  } else if (P2 == 2) {
+    // Two walks over the list, geometry first, then the feature sums: every
+    // accumulator still sees the neighbours in list order, and each walk
+    // keeps only its own accumulators live.
+    for (uint32_t k = 0; k < n; ++k) {
+      const uint32_t j = list[k * ls] & kSlotMask;
+      visitGeom(__ldg(&A.posS[j]), aliOn ? __ldg(&A.fwdS[j]) : zero4);
+    }
+    if (relaxOn) {
+      for (uint32_t k = 0; k < n; ++k) {
+        const uint32_t j = list[k * ls] & kSlotMask;
+        float fj[FP > 0 ? FP : 1];
+        loadFeat(j, fj);
+        visitFeat(fj, __ldg(&A.posS[j]).w);
+      }
     }
   } else {
     for (uint32_t k = 0; k < n; k += 2) {
@@ -231,9 +253,16 @@ template <int FP, int SCAN>
 void launchFlockScan(const FusedArgs& A, uint32_t blocks, uint32_t block, size_t smem, int phase2, int regs,
                      cudaStream_t st) {
   if constexpr (SCAN == 0) {
-    if (phase2) {
+    if (phase2 == 1) {
       if (regs > 64) flockKernel<FP, 1, 2, 0><<<blocks, block, smem, st>>>(A);
       else flockKernel<FP, 1, 4, 0><<<blocks, block, smem, st>>>(A);
+      return;
+    }
+  }
+  if constexpr (SCAN == 4 && FP > 0) {
+    if (phase2 == 2) {
+      if (regs <= 48) flockKernel<FP, 2, 5, 4><<<blocks, block, smem, st>>>(A);
+      else flockKernel<FP, 2, 4, 4><<<blocks, block, smem, st>>>(A);
       return;
     }
   }
@@ -261,13 +290,21 @@ cudaError_t configureFlockFP(int smem) {
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
   }
+  if constexpr (FP > 0) {
+    const void* split[2] = {(const void*)flockKernel<FP, 2, 4, 4>, (const void*)flockKernel<FP, 2, 5, 4>};
+    for (const void* fn : split) {
+      cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      if (e != cudaSuccess) return e;
+    }
+  }
   return cudaSuccess;
 }
 }  // namespace
 
-// phase2 != 0 walks the list two neighbours at a time with their loads issued
-// together (per-agent scans only; the cooperative scan's instantiation keeps
-// the one-at-a-time walk, which measured faster for it).  block: threads per block, a multiple of 32
+// phase2 1 walks the list two neighbours at a time with their loads issued
+// together (per-agent scans only); phase2 2 walks it twice, geometry then
+// feature sums (cooperative scan with features only); otherwise one walk,
+// one neighbour at a time.  block: threads per block, a multiple of 32
 // in [32, 256].  regs: the register budget a thread is compiled for, 128 (2
 // resident 256-thread blocks per SM), 64 (4 blocks), or for the cooperative
 // scan also 48 and 40 (5 and 6 blocks, more resident warps for some spills).

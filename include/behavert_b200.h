@@ -187,7 +187,9 @@ int brt_engine_set_params(brt_engine* e, uint32_t flock, const brt_params* p);
                               culling, 2 four without culling, 3 one at a time,
                               4 warp-cooperative (a warp tests 32 candidates of
                               a home cell's neighbourhood per step)
-     "phase2_variant"   0/1   list walk one or two neighbours at a time
+     "phase2_variant"   0..2  list walk one or two neighbours at a time, or
+                              (2, scan_variant 4 with features) two walks,
+                              geometry then feature sums
                               (per-agent scans 0..3 only)
      "wide_registers"   0/1   the flock kernel built for 128 registers a thread
                               (2 resident 256-thread blocks per SM) instead of 64

@@ -66,6 +66,18 @@ def test_scan_variants_are_bit_identical(name, variant):
             assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("scan,phase2", [(0, 1), (4, 2), (4, 1)])
+@pytest.mark.parametrize("name", ["large", "batched", "seam"])
+def test_list_walk_variants_are_bit_identical(name, scan, phase2):
+    wl = _variant_workloads()[name]
+    ref = _run(wl, 2, [("scan_variant", scan)])
+    for regs in (64, 48):
+        out = _run(wl, 2, [("scan_variant", scan), ("phase2_variant", phase2), ("registers", regs)])
+        for a, b in zip(ref, out):
+            if a is not None:
+                assert np.array_equal(a, b)
+
+
 @pytest.mark.parametrize("budget", [128, 48, 40])
 @pytest.mark.parametrize("name", ["large", "batched", "seam"])
 def test_register_budgets_are_bit_identical(name, budget):
