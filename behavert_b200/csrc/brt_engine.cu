@@ -918,23 +918,33 @@ int brt_engine_autotune(brt_engine* e, float elapsedTime, uint32_t steps, char* 
   int bestRegs = e->regBudget;
   if (!twoPass) {
     bestMs = 1e30;
+    // block size x scan loop x list walk, jointly: the best block depends on
+    // the walk.  Walk 1 (two neighbours at a time) only exists for the
+    // per-agent scans, walk 2 (geometry, then feature sums) for the
+    // cooperative scan of flocks with features.
     const uint32_t blocks[3] = {64, 128, 256};
     const int scans[3] = {0, 2, 4};  // per agent with / without cell culling, warp-cooperative
-    const char* names[3] = {"block_size/scan0", "block_size/scan2", "block_size/scan4"};
+    const char* names[3][2] = {{"block_size/scan0/walk0", "block_size/scan0/walk1"},
+                               {"block_size/scan2/walk0", "block_size/scan2/walk1"},
+                               {"block_size/scan4/walk0", "block_size/scan4/walk2"}};
+    bool anyFeatures = false;
+    for (const FlockDev& d : e->flocksHost) anyFeatures = anyFeatures || (d.F > 0 && d.relax != 0.0f);
     for (uint32_t bs : blocks)
-      for (int s = 0; s < 3 && !rc; ++s) {
-        chk(brt_engine_set_option(e, "block_size", bs));
-        chk(brt_engine_set_option(e, "scan_variant", scans[s]));
-        if (!rc) chk(trial(names[s], bs, &ms));
-        if (!rc && ms < bestMs) { bestMs = ms; bestBlock = bs; bestScan = scans[s]; }
-      }
-    if (!rc) { chk(brt_engine_set_option(e, "block_size", bestBlock)); chk(brt_engine_set_option(e, "scan_variant", bestScan)); }
-    for (int p2 = 0; p2 < 3 && !rc; ++p2) {
-      chk(brt_engine_set_option(e, "phase2_variant", p2));
-      if (!rc) chk(trial("phase2_variant", p2, &ms));
-      if (!rc && ms <= bestMs) { bestMs = ms; bestP2 = p2; }
+      for (int s = 0; s < 3 && !rc; ++s)
+        for (int w = 0; w < 2 && !rc; ++w) {
+          const int p2 = w == 0 ? 0 : (scans[s] == 4 ? 2 : 1);
+          if (p2 == 2 && !anyFeatures) continue;
+          chk(brt_engine_set_option(e, "block_size", bs));
+          chk(brt_engine_set_option(e, "scan_variant", scans[s]));
+          chk(brt_engine_set_option(e, "phase2_variant", p2));
+          if (!rc) chk(trial(names[s][w], bs, &ms));
+          if (!rc && ms < bestMs) { bestMs = ms; bestBlock = bs; bestScan = scans[s]; bestP2 = p2; }
+        }
+    if (!rc) {
+      chk(brt_engine_set_option(e, "block_size", bestBlock));
+      chk(brt_engine_set_option(e, "scan_variant", bestScan));
+      chk(brt_engine_set_option(e, "phase2_variant", bestP2));
     }
-    if (!rc) chk(brt_engine_set_option(e, "phase2_variant", bestP2));
     // 48 and 40 only change the cooperative scan's build
     const int budgets[4] = {64, 128, 48, 40};
     const int nBudgets = bestScan == 4 ? 4 : 2;
