@@ -3,13 +3,13 @@
 //
 // One thread per sorted slot.  Phase 1 scans the 27 neighbour cells in the
 // reference's visit order (Proximity3D_kernel.cu:108-115) into a shared-memory
-// list; phase 2 walks the list once, in list order, accumulating separation,
-// alignment, cohesion (OpenSteerWrapper_resources.cu:166-290) and the
-// feature-relaxation sums with the features held in registers and each
-// neighbour's feature norm precomputed by the reorder kernel (carried in the w
-// of its sorted position).  (Folding the
-// sums into the scan itself makes every scan iteration pay for the warp's
-// accepting lanes, which measured slower.)
+// list; phase 2 walks the list in list order (once, or with walk 2 twice:
+// geometry, then features), accumulating separation, alignment, cohesion
+// (OpenSteerWrapper_resources.cu:166-290) and the feature-relaxation sums with
+// the features held in registers and each neighbour's feature norm
+// precomputed by the reorder kernel (carried in the w of its sorted
+// position).  (Folding the sums into the scan itself makes every scan
+// iteration pay for the warp's accepting lanes, which measured slower.)
 //
 // inBoidNeighborhood (OpenSteerWrapper_resources.cu:67-92) is evaluated with
 // exact squared-distance thresholds (sqrtf is monotone and correctly rounded):
@@ -23,17 +23,8 @@
 
 namespace brt {
 
-// List entries carry the neighbour's image shift in their top bits:
-// 2 bits per axis (0: none, 1: -L, 2: +L) above a 26-bit sorted slot.
-constexpr uint32_t kSlotBits = 26;
-constexpr uint32_t kSlotMask = (1u << kSlotBits) - 1u;
-
-__device__ __forceinline__ uint32_t shiftCode(int g, int o, uint32_t G) {
-  return (o < 0 && g == 0) ? 1u : ((o > 0 && g == (int)G - 1) ? 2u : 0u);
-}
-__device__ __forceinline__ float shiftOf(uint32_t code, float L) {
-  return code == 1u ? -L : (code == 2u ? L : 0.0f);
-}
+// List entries are plain sorted slots; the walk recomputes each neighbour's
+// periodic image from its position (neighborImage).
 
 // SCAN: 0 the per-agent scans (variants 0-3, chosen at run time), 4 the
 // warp-cooperative scan, each its own instantiation so that it gets its own
@@ -77,7 +68,7 @@ __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs 
   if (A.lists) {
     uint32_t* out = A.lists + (size_t)i * A.listStride;
     out[0] = n;
-    for (uint32_t k = 0; k < n; ++k) out[1 + k] = list[k * ls] & kSlotMask;
+    for (uint32_t k = 0; k < n; ++k) out[1 + k] = list[k * ls];
   }
 
   // Phase 2: steering and feature sums over the list, in list order.
@@ -175,7 +166,7 @@ __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs 
   const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
   if (P2 == 0) {
     for (uint32_t k = 0; k < n; ++k) {
-      const uint32_t j = list[k * ls] & kSlotMask;
+      const uint32_t j = list[k * ls];
       const float4 q = __ldg(&A.posS[j]);
       float fj[FP > 0 ? FP : 1];
       float n2 = q.w;  // the neighbour's feature norm
@@ -187,12 +178,12 @@ __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs 
     // accumulator still sees the neighbours in list order, and each walk
     // keeps only its own accumulators live.
     for (uint32_t k = 0; k < n; ++k) {
-      const uint32_t j = list[k * ls] & kSlotMask;
+      const uint32_t j = list[k * ls];
       visitGeom(__ldg(&A.posS[j]), aliOn ? __ldg(&A.fwdS[j]) : zero4);
     }
     if (relaxOn) {
       for (uint32_t k = 0; k < n; ++k) {
-        const uint32_t j = list[k * ls] & kSlotMask;
+        const uint32_t j = list[k * ls];
         float fj[FP > 0 ? FP : 1];
         loadFeat(j, fj);
         visitFeat(fj, __ldg(&A.posS[j]).w);
@@ -201,8 +192,8 @@ __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs 
   } else {
     for (uint32_t k = 0; k < n; k += 2) {
       const bool two = k + 1 < n;
-      const uint32_t j0 = list[k * ls] & kSlotMask;
-      const uint32_t j1 = two ? (list[(k + 1) * ls] & kSlotMask) : j0;
+      const uint32_t j0 = list[k * ls];
+      const uint32_t j1 = two ? (list[(k + 1) * ls]) : j0;
       const float4 q0 = __ldg(&A.posS[j0]), q1 = __ldg(&A.posS[j1]);
       const float4 w0 = aliOn ? __ldg(&A.fwdS[j0]) : zero4, w1 = aliOn ? __ldg(&A.fwdS[j1]) : zero4;
       float f0[FP > 0 ? FP : 1], f1[FP > 0 ? FP : 1];
