@@ -31,9 +31,11 @@ struct brt_engine {
   float4* membership[2] = {nullptr, nullptr};  // clusterMembership by agent id (ping-pong)
   int membershipCur = 0;
   bool forceTwoPass = false;  // option "two_pass": run the list-first kernel even when not needed
-  int phase2Variant = 0;      // option "phase2_variant": list walk one or two neighbours at a time
-  int scanVariant = 0;        // option "scan_variant": neighbour-scan loop shape
-  uint32_t fusedBlock = 128;  // option "block_size": threads per block of the single-pass flock kernel
+  // Launch options; the defaults are the autotuner's choice on both the
+  // 1M-agent flock and the 1,024-flock batch.
+  int phase2Variant = 2;      // option "phase2_variant": list walk shape (2: geometry, then features)
+  int scanVariant = 4;        // option "scan_variant": neighbour-scan loop shape (4: warp-cooperative)
+  uint32_t fusedBlock = 64;   // option "block_size": threads per block of the single-pass flock kernel
   int regBudget = 64;         // option "registers" (or "wide_registers"): registers a thread of that kernel
   // state
   float4 *posA = nullptr, *fwdA = nullptr, *accA = nullptr, *posS = nullptr, *fwdS = nullptr, *accS = nullptr;

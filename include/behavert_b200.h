@@ -181,16 +181,16 @@ int brt_engine_set_params(brt_engine* e, uint32_t flock, const brt_params* p);
      "two_pass"         0/1   build each neighbour list before steering even
                               when the single-pass kernel applies (default 0)
      "block_size"       32..256, multiple of 32: threads per block of the
-                              single-pass flock kernel (default 128)
+                              single-pass flock kernel (default 64)
      "scan_variant"     0..4  neighbour-scan loop: 0 four candidates in flight
                               with exact cell culling, 1 two in flight with
                               culling, 2 four without culling, 3 one at a time,
                               4 warp-cooperative (a warp tests 32 candidates of
-                              a home cell's neighbourhood per step)
-     "phase2_variant"   0..2  list walk one or two neighbours at a time, or
-                              (2, scan_variant 4 with features) two walks,
-                              geometry then feature sums
-                              (per-agent scans 0..3 only)
+                              a home cell's neighbourhood per step; default)
+     "phase2_variant"   0..2  list walk: 0 one neighbour at a time, 1 two at a
+                              time (per-agent scans 0..3 only), 2 (default)
+                              two walks, geometry then feature sums (with
+                              scan_variant 4 and features; otherwise as 0)
      "wide_registers"   0/1   the flock kernel built for 128 registers a thread
                               (2 resident 256-thread blocks per SM) instead of 64
      "registers"        128, 64, 48 or 40: the flock kernel's register budget
