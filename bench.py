@@ -415,7 +415,7 @@ def fitting_leg(device: int, iters: int = 200):
         loss.sum().backward()
         opt.step()
         if it in (0, iters - 1):
-            losses.append(float(loss.sum()))
+            losses.append(float(loss.detach().sum()))
     torch.cuda.synchronize()
     t_fit = time.perf_counter() - t0
     eng.close()

@@ -76,7 +76,7 @@ def test_adam_fit_reduces_loss_toward_hidden_weights():
             loss = flock_loss(eng, w, pos0, vel_h, tgt, DT, T, k).sum()
             loss.backward()
             opt.step()
-            losses.append(float(loss))
+            losses.append(float(loss.detach()))
     hidden = np.asarray(wl.meta["hidden"])
     err0 = np.linalg.norm(np.asarray(wl.meta["trial"]) - hidden)
     err = np.linalg.norm(w.detach().cpu().numpy()[0] - hidden)
