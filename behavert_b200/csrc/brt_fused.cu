@@ -29,6 +29,13 @@ namespace brt {
 // SCAN: 0 the per-agent scans (variants 0-3, chosen at run time), 4 the
 // warp-cooperative scan, each its own instantiation so that it gets its own
 // register allocation.
+//
+// Rounds of 32 candidates the cooperative scan holds in registers: 96
+// candidates cover most home cells' 27-cell neighbourhoods at densities of 3
+// to 4 agents a cell (72 to 108 candidates).  Holding 4 measured the same on
+// the batched workload and 3% slower on config 1; 2 was slower on both.
+constexpr int kCoopCachedRounds = 3;
+
 template <int FP, int P2, int MINB, int SCAN>
 __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs A) {
   extern __shared__ uint32_t sList[];
@@ -49,14 +56,16 @@ __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs 
   const bool interior = gx > 0 && gx < hi && gy > 0 && gy < hi && gz > 0 && gz < hi;
   const uint32_t M = fl.M;
   uint32_t* list = sList + threadIdx.x;
-  const uint32_t ls = blockDim.x;
+  // The cooperative scan stores 32 rows of one agent's column per vote: an
+  // odd stride puts those rows in distinct shared-memory banks.
+  const uint32_t ls = blockDim.x + (SCAN == 4 ? 1u : 0u);
 
   // Phase 1: the neighbour list in the reference's visit order.
   (void)M;
   uint32_t n;
   if (SCAN == 4) {
     const uint32_t key = fl.cellBase + ((uint32_t)gz * G + (uint32_t)gy) * G + (uint32_t)gx;
-    n = scanNeighborsCooperative(active, i, p, key, A.flocks, f, A.cellStart, A.cellEnd, A.posS, sList, ls,
+    n = scanNeighborsCooperative<kCoopCachedRounds>(active, i, p, key, A.flocks, f, A.cellStart, A.cellEnd, A.posS, sList, ls,
                                  threadIdx.x & ~31u);
     if (!active) return;
   } else {
@@ -252,8 +261,8 @@ void launchFlockScan(const FusedArgs& A, uint32_t blocks, uint32_t block, size_t
   }
   if constexpr (SCAN == 4 && FP > 0) {
     if (phase2 == 2) {
-      if (regs <= 48) flockKernel<FP, 2, 5, 4><<<blocks, block, smem, st>>>(A);
-      else flockKernel<FP, 2, 4, 4><<<blocks, block, smem, st>>>(A);
+      if (regs <= 48) flockKernel<FP, 2, 5, SCAN><<<blocks, block, smem, st>>>(A);
+      else flockKernel<FP, 2, 4, SCAN><<<blocks, block, smem, st>>>(A);
       return;
     }
   }
@@ -304,7 +313,7 @@ cudaError_t launchFlock(const FusedArgs& A, int phase2, uint32_t block, int regs
   if (block < 32 || block > kFlockMaxThreads || block % 32) return cudaErrorInvalidValue;
   const uint32_t blocks = (A.n + block - 1) / block;
   const uint32_t fp = A.Fs;
-  const size_t smem = (size_t)block * A.Mmax * 4;
+  const size_t smem = (size_t)(block + (A.scanVariant == 4 ? 1u : 0u)) * A.Mmax * 4;
   if (fp == 0) return launchFlockFP<0>(A, blocks, block, smem, phase2, regs, st);
   if (fp <= 4) return launchFlockFP<4>(A, blocks, block, smem, phase2, regs, st);
   if (fp <= 8) return launchFlockFP<8>(A, blocks, block, smem, phase2, regs, st);
@@ -313,7 +322,7 @@ cudaError_t launchFlock(const FusedArgs& A, int phase2, uint32_t block, int regs
 }
 
 cudaError_t configureFlockKernels(uint32_t Mmax) {
-  const int smem = (int)((size_t)kFlockMaxThreads * Mmax * 4);
+  const int smem = (int)((size_t)(kFlockMaxThreads + 1) * Mmax * 4);
   cudaError_t e = cudaSuccess;
   if ((e = configureFlockFP<0>(smem))) return e;
   if ((e = configureFlockFP<4>(smem))) return e;
