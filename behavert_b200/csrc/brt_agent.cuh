@@ -251,15 +251,16 @@ __device__ __forceinline__ uint32_t scanNeighborsPipelined(uint32_t self, f3 p, 
 // With R > 0 the run's first R rounds of candidates are loaded into registers
 // up front and each agent then goes through them alone (agent-major): its
 // position, slot and count are broadcast once instead of once a round, and
-// it stops at the round that fills its list.  Rounds after the first R, for
-// agents still open, go round-major as with R = 0.  Each agent's list gets
-// the same candidates in the same order either way.
+// it stops at the round that fills its list.  With WINT > 0 the next R
+// rounds go the same way while at least WINT of the run's agents are still
+// open; rounds after that go round-major as with R = 0.  Each agent's list
+// gets the same candidates in the same order either way.
 //
 // Called by all 32 lanes of a warp; `active` lanes own an agent (sorted slot
 // `self`, position p, home cell key `key`, flock `flock`).  Each agent's list
 // goes to column laneCol0 + lane of the shared array sList (stride ls).
 // Returns the lane's list length.
-template <int R>
+template <int R, int WINT = 0>
 __device__ __forceinline__ uint32_t scanNeighborsCooperative(bool active, uint32_t self, f3 p, uint32_t key,
                                                              const FlockDev* __restrict__ flocks, uint32_t flock,
                                                              const uint32_t* __restrict__ cellStart,
@@ -318,58 +319,61 @@ __device__ __forceinline__ uint32_t scanNeighborsCooperative(bool active, uint32
     uint32_t base0 = 0;
     if constexpr (R > 0) {
       constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
-      float cqx[R], cqy[R], cqz[R];
-      uint32_t cslot[R];
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        cqx[r] = cqy[r] = cqz[r] = 0.0f;
-        cslot[r] = kNoSlot;
-        if ((uint32_t)r * 32u < total) {
-          const uint32_t t = (uint32_t)r * 32u + lane;
-          uint32_t c = 0;
-#pragma unroll
-          for (int step = 16; step > 0; step >>= 1) {
-            const uint32_t cand = c + (uint32_t)step;
-            const uint32_t e = __shfl_sync(full, excl, cand & 31u);
-            if (cand < 27u && e <= t) c = cand;
-          }
-          const uint32_t cStart = __shfl_sync(full, segStart, c), cExcl = __shfl_sync(full, excl, c);
-          const float csx = __shfl_sync(full, sx, c), csy = __shfl_sync(full, sy, c), csz = __shfl_sync(full, sz, c);
-          if (t < total) {
-            cslot[r] = cStart + (t - cExcl);
-            const float4 q = __ldg(&posS[cslot[r]]);
-            cqx[r] = q.x + csx;
-            cqy[r] = q.y + csy;
-            cqz[r] = q.z + csz;
-          }
-        }
-      }
       const uint32_t below = (1u << lane) - 1u;
-      for (uint32_t todo = groupMask; todo; todo &= todo - 1u) {
-        const uint32_t a = __ffs(todo) - 1u;
-        const float ax = __shfl_sync(full, p.x, a), ay = __shfl_sync(full, p.y, a), az = __shfl_sync(full, p.z, a);
-        const uint32_t aSelf = __shfl_sync(full, self, a);
-        uint32_t an = 0;
-        uint32_t* col = sList + laneCol0 + a;
+      for (;;) {
+        float cqx[R], cqy[R], cqz[R];
+        uint32_t cslot[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          if ((uint32_t)r * 32u >= total) break;
-          const float dx = cqx[r] - ax, dy = cqy[r] - ay, dz = cqz[r] - az;
-          const float d2 = dx * dx + dy * dy + dz * dz;
-          const bool acc = cslot[r] != kNoSlot && !(d2 > thr) && cslot[r] != aSelf;
-          const uint32_t bal = __ballot_sync(full, acc);
-          if (acc) {
-            const uint32_t pos = an + (uint32_t)__popc(bal & below);
-            if (pos < M) col[pos * ls] = cslot[r];
+          cqx[r] = cqy[r] = cqz[r] = 0.0f;
+          cslot[r] = kNoSlot;
+          if (base0 + (uint32_t)r * 32u < total) {
+            const uint32_t t = base0 + (uint32_t)r * 32u + lane;
+            uint32_t c = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1) {
+              const uint32_t cand = c + (uint32_t)step;
+              const uint32_t e = __shfl_sync(full, excl, cand & 31u);
+              if (cand < 27u && e <= t) c = cand;
+            }
+            const uint32_t cStart = __shfl_sync(full, segStart, c), cExcl = __shfl_sync(full, excl, c);
+            const float csx = __shfl_sync(full, sx, c), csy = __shfl_sync(full, sy, c), csz = __shfl_sync(full, sz, c);
+            if (t < total) {
+              cslot[r] = cStart + (t - cExcl);
+              const float4 q = __ldg(&posS[cslot[r]]);
+              cqx[r] = q.x + csx;
+              cqy[r] = q.y + csy;
+              cqz[r] = q.z + csz;
+            }
           }
-          an += (uint32_t)__popc(bal);
-          if (an >= M) break;
         }
-        an = min(an, M);
-        if (lane == a) n = an;
-        if (an >= M) open &= ~(1u << a);
+        for (uint32_t todo = open; todo; todo &= todo - 1u) {
+          const uint32_t a = __ffs(todo) - 1u;
+          const float ax = __shfl_sync(full, p.x, a), ay = __shfl_sync(full, p.y, a), az = __shfl_sync(full, p.z, a);
+          const uint32_t aSelf = __shfl_sync(full, self, a);
+          uint32_t an = __shfl_sync(full, n, a);
+          uint32_t* col = sList + laneCol0 + a;
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            if (base0 + (uint32_t)r * 32u >= total) break;
+            const float dx = cqx[r] - ax, dy = cqy[r] - ay, dz = cqz[r] - az;
+            const float d2 = dx * dx + dy * dy + dz * dz;
+            const bool acc = cslot[r] != kNoSlot && !(d2 > thr) && cslot[r] != aSelf;
+            const uint32_t bal = __ballot_sync(full, acc);
+            if (acc) {
+              const uint32_t pos = an + (uint32_t)__popc(bal & below);
+              if (pos < M) col[pos * ls] = cslot[r];
+            }
+            an += (uint32_t)__popc(bal);
+            if (an >= M) break;
+          }
+          an = min(an, M);
+          if (lane == a) n = an;
+          if (an >= M) open &= ~(1u << a);
+        }
+        base0 += (uint32_t)R * 32u;
+        if (WINT == 0 || base0 >= total || __popc(open) < WINT) break;
       }
-      base0 = (uint32_t)R * 32u;
     }
     for (uint32_t base = base0; base < total && open; base += 32u) {
       const uint32_t t = base + lane;

@@ -610,7 +610,7 @@ int brt_engine_set_option(brt_engine* e, const char* key, int64_t value) {
     if (value < 0 || value > 2) { setLastError("phase2_variant must be in [0, 2]"); return BRT_ERR_ARG; }
     e->phase2Variant = (int)value;
   } else if (k == "scan_variant") {
-    if (value < 0 || value > 4) { setLastError("scan_variant must be in [0, 4]"); return BRT_ERR_ARG; }
+    if (value < 0 || value > 5) { setLastError("scan_variant must be in [0, 5]"); return BRT_ERR_ARG; }
     e->scanVariant = (int)value;
   } else if (k == "block_size") {
     if (value < 32 || value > (int64_t)kFlockMaxThreads || value % 32) {
@@ -923,16 +923,18 @@ int brt_engine_autotune(brt_engine* e, float elapsedTime, uint32_t steps, char* 
     // per-agent scans, walk 2 (geometry, then feature sums) for the
     // cooperative scan of flocks with features.
     const uint32_t blocks[3] = {64, 128, 256};
-    const int scans[3] = {0, 2, 4};  // per agent with / without cell culling, warp-cooperative
-    const char* names[3][2] = {{"block_size/scan0/walk0", "block_size/scan0/walk1"},
+    // per agent with / without cell culling, warp-cooperative, cooperative with windows
+    const int scans[4] = {0, 2, 4, 5};
+    const char* names[4][2] = {{"block_size/scan0/walk0", "block_size/scan0/walk1"},
                                {"block_size/scan2/walk0", "block_size/scan2/walk1"},
-                               {"block_size/scan4/walk0", "block_size/scan4/walk2"}};
+                               {"block_size/scan4/walk0", "block_size/scan4/walk2"},
+                               {"block_size/scan5/walk0", "block_size/scan5/walk2"}};
     bool anyFeatures = false;
     for (const FlockDev& d : e->flocksHost) anyFeatures = anyFeatures || (d.F > 0 && d.relax != 0.0f);
     for (uint32_t bs : blocks)
-      for (int s = 0; s < 3 && !rc; ++s)
+      for (int s = 0; s < 4 && !rc; ++s)
         for (int w = 0; w < 2 && !rc; ++w) {
-          const int p2 = w == 0 ? 0 : (scans[s] == 4 ? 2 : 1);
+          const int p2 = w == 0 ? 0 : (scans[s] >= 4 ? 2 : 1);
           if (p2 == 2 && !anyFeatures) continue;
           chk(brt_engine_set_option(e, "block_size", bs));
           chk(brt_engine_set_option(e, "scan_variant", scans[s]));
@@ -947,7 +949,7 @@ int brt_engine_autotune(brt_engine* e, float elapsedTime, uint32_t steps, char* 
     }
     // 48 and 40 only change the cooperative scan's build
     const int budgets[4] = {64, 128, 48, 40};
-    const int nBudgets = bestScan == 4 ? 4 : 2;
+    const int nBudgets = bestScan >= 4 ? 4 : 2;
     bestMs = 1e30;
     for (int r = 0; r < nBudgets && !rc; ++r) {
       chk(brt_engine_set_option(e, "registers", budgets[r]));

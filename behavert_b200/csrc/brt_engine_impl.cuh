@@ -34,7 +34,7 @@ struct brt_engine {
   // Launch options; the defaults are the autotuner's choice on both the
   // 1M-agent flock and the 1,024-flock batch.
   int phase2Variant = 2;      // option "phase2_variant": list walk shape (2: geometry, then features)
-  int scanVariant = 4;        // option "scan_variant": neighbour-scan loop shape (4: warp-cooperative)
+  int scanVariant = 5;        // option "scan_variant": neighbour-scan loop shape (5: warp-cooperative, windowed)
   uint32_t fusedBlock = 64;   // option "block_size": threads per block of the single-pass flock kernel
   int regBudget = 64;         // option "registers" (or "wide_registers"): registers a thread of that kernel
   // state

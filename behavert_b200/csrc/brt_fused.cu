@@ -27,14 +27,20 @@ namespace brt {
 // periodic image from its position (neighborImage).
 
 // SCAN: 0 the per-agent scans (variants 0-3, chosen at run time), 4 the
-// warp-cooperative scan, each its own instantiation so that it gets its own
-// register allocation.
+// warp-cooperative scan, 5 the cooperative scan that keeps going agent-major
+// in windows of register-held rounds while a run has many open agents; each
+// its own instantiation so that it gets its own register allocation.
 //
 // Rounds of 32 candidates the cooperative scan holds in registers: 96
 // candidates cover most home cells' 27-cell neighbourhoods at densities of 3
 // to 4 agents a cell (72 to 108 candidates).  Holding 4 measured the same on
 // the batched workload and 3% slower on config 1; 2 was slower on both.
 constexpr int kCoopCachedRounds = 3;
+// Scan 5 takes further windows while at least this many of a run's agents
+// still need candidates (dense cells, e.g. config 1's Gaussian blobs): 4%
+// faster on config 1, 1% slower on the uniform batched workload, where runs
+// are short.  16 measured between the two.
+constexpr int kCoopWindowAgents = 8;
 
 template <int FP, int P2, int MINB, int SCAN>
 __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs A) {
@@ -58,14 +64,14 @@ __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs 
   uint32_t* list = sList + threadIdx.x;
   // The cooperative scan stores 32 rows of one agent's column per vote: an
   // odd stride puts those rows in distinct shared-memory banks.
-  const uint32_t ls = blockDim.x + (SCAN == 4 ? 1u : 0u);
+  const uint32_t ls = blockDim.x + (SCAN >= 4 ? 1u : 0u);
 
   // Phase 1: the neighbour list in the reference's visit order.
   (void)M;
   uint32_t n;
-  if (SCAN == 4) {
+  if (SCAN >= 4) {
     const uint32_t key = fl.cellBase + ((uint32_t)gz * G + (uint32_t)gy) * G + (uint32_t)gx;
-    n = scanNeighborsCooperative<kCoopCachedRounds>(active, i, p, key, A.flocks, f, A.cellStart, A.cellEnd, A.posS, sList, ls,
+    n = scanNeighborsCooperative<kCoopCachedRounds, SCAN == 5 ? kCoopWindowAgents : 0>(active, i, p, key, A.flocks, f, A.cellStart, A.cellEnd, A.posS, sList, ls,
                                  threadIdx.x & ~31u);
     if (!active) return;
   } else {
@@ -259,14 +265,14 @@ void launchFlockScan(const FusedArgs& A, uint32_t blocks, uint32_t block, size_t
       return;
     }
   }
-  if constexpr (SCAN == 4 && FP > 0) {
+  if constexpr (SCAN >= 4 && FP > 0) {
     if (phase2 == 2) {
       if (regs <= 48) flockKernel<FP, 2, 5, SCAN><<<blocks, block, smem, st>>>(A);
       else flockKernel<FP, 2, 4, SCAN><<<blocks, block, smem, st>>>(A);
       return;
     }
   }
-  if constexpr (SCAN == 4) {
+  if constexpr (SCAN >= 4) {
     if (regs <= 40) { flockKernel<FP, 0, 6, SCAN><<<blocks, block, smem, st>>>(A); return; }
     if (regs <= 48) { flockKernel<FP, 0, 5, SCAN><<<blocks, block, smem, st>>>(A); return; }
   }
@@ -277,27 +283,37 @@ template <int FP>
 cudaError_t launchFlockFP(const FusedArgs& A, uint32_t blocks, uint32_t block, size_t smem, int phase2, int regs,
                           cudaStream_t st) {
   if (A.scanVariant == 4) launchFlockScan<FP, 4>(A, blocks, block, smem, phase2, regs, st);
+  else if (A.scanVariant == 5) launchFlockScan<FP, 5>(A, blocks, block, smem, phase2, regs, st);
   else launchFlockScan<FP, 0>(A, blocks, block, smem, phase2, regs, st);
   return cudaGetLastError();
 }
-template <int FP>
-cudaError_t configureFlockFP(int smem) {
-  const void* fns[8] = {(const void*)flockKernel<FP, 0, 4, 0>, (const void*)flockKernel<FP, 1, 4, 0>,
-                        (const void*)flockKernel<FP, 0, 2, 0>, (const void*)flockKernel<FP, 1, 2, 0>,
-                        (const void*)flockKernel<FP, 0, 4, 4>, (const void*)flockKernel<FP, 0, 2, 4>,
-                        (const void*)flockKernel<FP, 0, 5, 4>, (const void*)flockKernel<FP, 0, 6, 4>};
+template <int FP, int SCAN>
+cudaError_t configureCoopScan(int smem) {
+  const void* fns[4] = {(const void*)flockKernel<FP, 0, 4, SCAN>, (const void*)flockKernel<FP, 0, 2, SCAN>,
+                        (const void*)flockKernel<FP, 0, 5, SCAN>, (const void*)flockKernel<FP, 0, 6, SCAN>};
   for (const void* fn : fns) {
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
   }
   if constexpr (FP > 0) {
-    const void* split[2] = {(const void*)flockKernel<FP, 2, 4, 4>, (const void*)flockKernel<FP, 2, 5, 4>};
+    const void* split[2] = {(const void*)flockKernel<FP, 2, 4, SCAN>, (const void*)flockKernel<FP, 2, 5, SCAN>};
     for (const void* fn : split) {
       cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
       if (e != cudaSuccess) return e;
     }
   }
   return cudaSuccess;
+}
+template <int FP>
+cudaError_t configureFlockFP(int smem) {
+  const void* fns[4] = {(const void*)flockKernel<FP, 0, 4, 0>, (const void*)flockKernel<FP, 1, 4, 0>,
+                        (const void*)flockKernel<FP, 0, 2, 0>, (const void*)flockKernel<FP, 1, 2, 0>};
+  for (const void* fn : fns) {
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+  }
+  cudaError_t e = configureCoopScan<FP, 4>(smem);
+  return e == cudaSuccess ? configureCoopScan<FP, 5>(smem) : e;
 }
 }  // namespace
 
@@ -313,7 +329,7 @@ cudaError_t launchFlock(const FusedArgs& A, int phase2, uint32_t block, int regs
   if (block < 32 || block > kFlockMaxThreads || block % 32) return cudaErrorInvalidValue;
   const uint32_t blocks = (A.n + block - 1) / block;
   const uint32_t fp = A.Fs;
-  const size_t smem = (size_t)(block + (A.scanVariant == 4 ? 1u : 0u)) * A.Mmax * 4;
+  const size_t smem = (size_t)(block + (A.scanVariant >= 4 ? 1u : 0u)) * A.Mmax * 4;
   if (fp == 0) return launchFlockFP<0>(A, blocks, block, smem, phase2, regs, st);
   if (fp <= 4) return launchFlockFP<4>(A, blocks, block, smem, phase2, regs, st);
   if (fp <= 8) return launchFlockFP<8>(A, blocks, block, smem, phase2, regs, st);

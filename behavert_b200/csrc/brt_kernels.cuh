@@ -54,7 +54,7 @@ struct FusedArgs {
   uint32_t nflocks, n, Mmax, Fs;
   float dt;
   int scanVariant;             // 0: pipelined x4 + cell culling, 1: x2 + culling, 2: x4, 3: flat loop,
-                               // 4: warp-cooperative
+                               // 4: warp-cooperative, 5: warp-cooperative with windows
   const uint32_t* stepCounter; // random-stream step of the Schooling move
 };
 

@@ -41,7 +41,7 @@ def _variant_workloads():
     return {"large": big, "batched": bat, "cap": cap, "seam": seam, "2d": flat, "odd": odd}
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3, 4])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5])
 @pytest.mark.parametrize("name", ["large", "batched", "cap", "seam", "2d", "odd"])
 def test_scan_variants_are_bit_identical(name, variant):
     wl = _variant_workloads()[name]
@@ -66,7 +66,7 @@ def test_scan_variants_are_bit_identical(name, variant):
             assert np.array_equal(a, b)
 
 
-@pytest.mark.parametrize("scan,phase2", [(0, 1), (4, 2), (4, 1)])
+@pytest.mark.parametrize("scan,phase2", [(0, 1), (4, 2), (4, 1), (5, 2)])
 @pytest.mark.parametrize("name", ["large", "batched", "seam"])
 def test_list_walk_variants_are_bit_identical(name, scan, phase2):
     wl = _variant_workloads()[name]
