@@ -15,8 +15,8 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libbehavert_b200.so"
-SOURCES = ["brt_sort.cu", "brt_kernels.cu", "brt_fused.cu", "brt_school.cu", "brt_cluster.cu", "brt_adjoint.cu",
-           "brt_engine.cu", "brt_adjoint_host.cu"]
+SOURCES = ["brt_sort.cu", "brt_kernels.cu", "brt_fused.cu", "brt_resort.cu", "brt_school.cu", "brt_cluster.cu",
+           "brt_adjoint.cu", "brt_engine.cu", "brt_adjoint_host.cu"]
 HEADERS = ["brt_internal.cuh", "brt_kernels.cuh", "brt_agent.cuh", "brt_engine_impl.cuh"]
 
 NVCC_FLAGS = [

@@ -151,6 +151,8 @@ int copyState(brt_engine* e, float4* pos, float4* fwd, float4* acc, uint32_t* id
   BRT_CUDA_TRY(cudaMemcpyAsync(fwd, sfwd, n * 16, cudaMemcpyDeviceToDevice, e->stream));
   BRT_CUDA_TRY(cudaMemcpyAsync(acc, sacc, n * 16, cudaMemcpyDeviceToDevice, e->stream));
   BRT_CUDA_TRY(cudaMemcpyAsync(id, sid, n * 4, cudaMemcpyDeviceToDevice, e->stream));
+  // a checkpoint restored into the engine: its order is not the last step's
+  if (pos == e->posA) BRT_CUDA_TRY(engineInvalidateResort(e));
   return BRT_OK;
 }
 

@@ -170,7 +170,7 @@ void freeAll(brt_engine* e) {
   void* ptrs[] = {e->flocks, e->agentBase, e->obstacles, e->obsMask, e->posA, e->fwdA, e->accA, e->posS, e->fwdS, e->accS,
                   e->featA, e->featS, e->idA, e->idS, e->statsById, e->steer, e->lists, e->pairs[0], e->pairs[1],
                   e->cellStart, e->cellEnd, e->sortMem, e->errWord, e->stage4, e->stageF, e->stepCounter,
-                  e->membership[0], e->membership[1]};
+                  e->membership[0], e->membership[1], e->resortMem};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto& u : e->user) {
@@ -235,14 +235,52 @@ int stageMark(brt_engine* e, int k) {
 }
 
 // hash -> sort -> reorder + cell ranges
-int enqueueReorder(brt_engine* e) {
+ResortArgs resortArgs(brt_engine* e) {
+  ResortArgs A;
+  std::memset(&A, 0, sizeof(A));
+  A.pos = e->posA; A.id = e->idA; A.prevPairs = e->pairs[e->plan.passes & 1];
+  A.cellStart = e->cellStart; A.cellEnd = e->cellEnd;
+  A.flocks = e->flocks; A.agentBase = e->agentBase;
+  A.nflocks = e->nflocks; A.n = e->N; A.numCells = e->C;
+  A.maxMovers = e->N / 8;
+  A.newKey = e->rsNewKey; A.prefix = e->rsPrefix; A.blockStay = e->rsBlockStay;
+  A.moverCount = e->rsCount; A.moverHead = e->rsHead; A.moverNext = e->rsNext;
+  A.newStart = e->rsNewStart; A.stayBase = e->rsStayBase; A.tileStatus = e->rsTiles; A.tileCounter = e->rsCounter; A.words = e->rsWords;
+  A.stepCounter = e->stepCounter;
+  A.out = e->pairs[e->plan.passes & 1];
+  A.errWord = e->errWord;
+  return A;
+}
+
+// The next fused step cannot take its order from the current one (the
+// canonical arrays or the sort plan were replaced): it runs the full sort.
+cudaError_t invalidateResort(brt_engine* e) {
+  return cudaMemsetAsync(e->rsWords + kResortWordValid, 0, 4, e->stream);
+}
+
+// Hash, sort and reorder.  From the fused step (incremental) the order comes
+// from the incremental re-sort when the previous step's order allows it, the
+// hash and radix passes running only otherwise (decided on the device).
+int enqueueReorder(brt_engine* e, bool incremental = false) {
   cudaStream_t st = e->stream;
   int rc = stageMark(e, 0);
   if (rc) return rc;
-  BRT_CUDA_TRY(launchHash(hashArgs(e), e->smCount * 8, st));
+  const bool rs = incremental && e->resortOn;
+  HashArgs H = hashArgs(e);
+  H.resortValid = e->rsWords + kResortWordValid;
+  const uint32_t* gate = nullptr;
+  ResortArgs RS;
+  if (rs) {
+    RS = resortArgs(e);
+    BRT_CUDA_TRY(launchResortMark(RS, st));
+    gate = e->rsWords + kResortWordMode;
+    H.gate = gate;
+  }
+  BRT_CUDA_TRY(launchHash(H, e->smCount * 8, st));
   if ((rc = stageMark(e, 1))) return rc;
   for (uint32_t k = 0; k < e->plan.passes; ++k)
-    BRT_CUDA_TRY(launchOnesweepPass(e->plan, k, e->pairs[k & 1], e->pairs[(k + 1) & 1], e->ss, e->errWord, st));
+    BRT_CUDA_TRY(launchOnesweepPass(e->plan, k, e->pairs[k & 1], e->pairs[(k + 1) & 1], e->ss, e->errWord, st, gate));
+  if (rs) BRT_CUDA_TRY(launchResortPlace(RS, st));
   if ((rc = stageMark(e, 2))) return rc;
   e->finalPairs = e->plan.passes & 1;
   ReorderArgs R;
@@ -255,6 +293,12 @@ int enqueueReorder(brt_engine* e) {
   R.cellStart = e->cellStart; R.cellEnd = e->cellEnd;
   R.hist = e->ss.hist; R.histWords = e->plan.passes * e->plan.bins;
   R.n = e->N; R.numCells = e->C; R.errWord = e->errWord;
+  if (rs) {
+    R.resortMode = e->rsWords + kResortWordMode;
+    R.newStart = e->rsNewStart;
+    R.moverCount = e->rsCount; R.moverHead = e->rsHead;
+    R.resortValid = e->rsWords + kResortWordValid;
+  }
   BRT_CUDA_TRY(launchReorder(R, st));
   // registered arrays move with their agents (slot i takes the previous slot
   // pairs[i].y), the agent-id map with them
@@ -277,7 +321,7 @@ int enqueueStep(brt_engine* e, float dt, bool record) {
     int rc = drainSlot(e, e->ringPos);
     if (rc) return rc;
   }
-  int rc = enqueueReorder(e);
+  int rc = enqueueReorder(e, true);
   if (rc) return rc;
   FusedArgs F;
   std::memset(&F, 0, sizeof(F));
@@ -353,6 +397,7 @@ int configureKernels(brt_engine* e);
 
 namespace brt {
 int engineEnqueueStep(brt_engine* e, float dt, bool record) { return enqueueStep(e, dt, record); }
+cudaError_t engineInvalidateResort(brt_engine* e) { return invalidateResort(e); }
 int engineSyncAndCheck(brt_engine* e) { return syncAndCheck(e); }
 }  // namespace brt
 
@@ -500,7 +545,20 @@ int brt_engine_create(const brt_params* flocks, uint32_t num_flocks, int device,
   chk(devAlloc(&e->stageF, std::max<size_t>(1, n * e->Fmax)));
   const size_t sortBytes = sortScratchBytes(e->plan, false);
   if (!rc && cudaMalloc(&e->sortMem, sortBytes) != cudaSuccess) { setLastError("sort scratch allocation failed"); rc = BRT_ERR_CUDA; }
+  // incremental re-sort arrays, each on a 16-byte boundary
+  auto words4 = [](size_t w) { return (w + 3) & ~(size_t)3; };
+  const size_t rsSizes[11] = {n, n, n, (size_t)resortBlocks(e->N) + 1, e->C, e->C, e->C,
+                              std::max<size_t>(1, resortCellTiles(e->C)), 1, kResortWords, e->C};
+  size_t rsWordsTotal = 0;
+  for (size_t w : rsSizes) rsWordsTotal += words4(w);
+  if (!rc && cudaMalloc(&e->resortMem, rsWordsTotal * 4) != cudaSuccess) { setLastError("re-sort allocation failed"); rc = BRT_ERR_CUDA; }
   if (rc) { freeAll(e); delete e; return rc; }
+  {
+    uint32_t** rsPtrs[11] = {&e->rsNewKey, &e->rsPrefix, &e->rsNext, &e->rsBlockStay, &e->rsCount, &e->rsHead,
+                             &e->rsNewStart, &e->rsTiles, &e->rsCounter, &e->rsWords, &e->rsStayBase};
+    size_t off = 0;
+    for (int k = 0; k < 11; ++k) { *rsPtrs[k] = e->resortMem + off; off += words4(rsSizes[k]); }
+  }
   e->ss = carveSortScratch(e->plan, e->sortMem, false);
   cudaStream_t st = e->stream;
   BRT_CUDA_TRY(cudaMemcpyAsync(e->flocks, e->flocksHost.data(), sizeof(FlockDev) * num_flocks, cudaMemcpyHostToDevice, st));
@@ -513,6 +571,8 @@ int brt_engine_create(const brt_params* flocks, uint32_t num_flocks, int device,
     BRT_CUDA_TRY(cudaStreamSynchronize(st));
   }
   BRT_CUDA_TRY(cudaMemsetAsync(e->sortMem, 0, sortBytes, st));
+  BRT_CUDA_TRY(cudaMemsetAsync(e->resortMem, 0, rsWordsTotal * 4, st));
+  if (e->C) BRT_CUDA_TRY(cudaMemsetAsync(e->rsHead, 0xFF, (size_t)e->C * 4, st));  // kNoMover
   BRT_CUDA_TRY(cudaMemsetAsync(e->errWord, 0, 4, st));
   BRT_CUDA_TRY(cudaMemsetAsync(e->stepCounter, 0, 4, st));
   if (n) {
@@ -593,6 +653,7 @@ int brt_engine_set_params(brt_engine* e, uint32_t flock, const brt_params* p) {
     BRT_CUDA_TRY(cudaMemcpyAsync(e->obsMask + d.cellBase, field.data() + d.cellBase, sizeof(uint2) * d.C,
                                  cudaMemcpyHostToDevice, e->stream));
   }
+  BRT_CUDA_TRY(invalidateResort(e));
   BRT_CUDA_TRY(cudaStreamSynchronize(e->stream));
   for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second);
   e->graphs.clear();
@@ -612,6 +673,9 @@ int brt_engine_set_option(brt_engine* e, const char* key, int64_t value) {
   } else if (k == "scan_variant") {
     if (value < 0 || value > 5) { setLastError("scan_variant must be in [0, 5]"); return BRT_ERR_ARG; }
     e->scanVariant = (int)value;
+  } else if (k == "incremental_sort") {
+    e->resortOn = value != 0;
+    BRT_CUDA_TRY(invalidateResort(e));
   } else if (k == "block_size") {
     if (value < 32 || value > (int64_t)kFlockMaxThreads || value % 32) {
       setLastError("block_size must be a multiple of 32 in [32, 256]");
@@ -650,6 +714,7 @@ int brt_engine_set_option(brt_engine* e, const char* key, int64_t value) {
     e->ss = carveSortScratch(plan, mem, false);
     e->reordered = false;
     e->listsValid = false;
+    BRT_CUDA_TRY(invalidateResort(e));
   } else {
     setLastError("unknown option " + k);
     return BRT_ERR_ARG;
@@ -716,6 +781,7 @@ int brt_set_state(brt_engine* e, const float* pos4, const float* fwd4, const flo
   }
   e->reordered = false;
   e->listsValid = false;
+  BRT_CUDA_TRY(invalidateResort(e));
   if (where == BRT_MEM_HOST) BRT_CUDA_TRY(cudaStreamSynchronize(st));
   return BRT_OK;
 }
@@ -861,6 +927,7 @@ int brt_engine_autotune(brt_engine* e, float elapsedTime, uint32_t steps, char* 
     } else {
       cp(e->posA, sp, n * 16); cp(e->fwdA, sf, n * 16); cp(e->accA, sa, n * 16); cp(e->statsById, ss, n * 16);
       cp(e->idA, si, n * 4); cp(e->featA, sx, n * e->Fs * 4);
+      if (c == cudaSuccess) c = invalidateResort(e);
     }
     return c;
   };
@@ -907,11 +974,16 @@ int brt_engine_autotune(brt_engine* e, float elapsedTime, uint32_t steps, char* 
   // single-pass kernel runs).
   uint32_t bestBits = e->plan.digitBits;
   double bestMs = 1e30, ms = 0.0;
+  // digit widths are timed with the full sort every step (the incremental
+  // re-sort would hide them)
+  const bool resortWas = e->resortOn;
+  e->resortOn = false;
   for (uint32_t b = 4; b <= 8 && !rc; ++b) {
     chk(brt_engine_set_option(e, "sort_digit_bits", b));
     if (!rc) chk(trial("sort_digit_bits", b, &ms));
     if (!rc && ms < bestMs) { bestMs = ms; bestBits = b; }
   }
+  e->resortOn = resortWas;
   if (!rc) chk(brt_engine_set_option(e, "sort_digit_bits", bestBits));
   uint32_t bestBlock = e->fusedBlock;
   int bestScan = e->scanVariant, bestP2 = e->phase2Variant;
@@ -958,6 +1030,19 @@ int brt_engine_autotune(brt_engine* e, float elapsedTime, uint32_t steps, char* 
     }
     if (!rc) chk(brt_engine_set_option(e, "registers", bestRegs));
   }
+  // the incremental re-sort against the full sort every step
+  {
+    const int start = e->resortOn ? 1 : 0;
+    int bestResort = start;
+    bestMs = 1e30;
+    for (int k = 0; k < 2 && !rc; ++k) {
+      const int v = k == 0 ? start : 1 - start;
+      chk(brt_engine_set_option(e, "incremental_sort", v));
+      if (!rc) chk(trial("incremental_sort", (uint32_t)v, &ms));
+      if (!rc && ms < bestMs) { bestMs = ms; bestResort = v; }
+    }
+    if (!rc) chk(brt_engine_set_option(e, "incremental_sort", bestResort));
+  }
   if (!rc && copyAll(false) != cudaSuccess) { setLastError("autotune restore failed"); rc = BRT_ERR_CUDA; }
   if (!rc) cudaStreamSynchronize(st);
   e->userFrozen = wasFrozen;
@@ -972,8 +1057,9 @@ int brt_engine_autotune(brt_engine* e, float elapsedTime, uint32_t steps, char* 
   if (report && report_len) {
     std::snprintf(buf, sizeof(buf),
                   "{\"sort_digit_bits\": %u, \"block_size\": %u, \"scan_variant\": %d, \"phase2_variant\": %d, "
-                  "\"wide_registers\": %d, \"registers\": %d, \"ms_per_step\": %.6f, \"trials\": [",
-                  bestBits, bestBlock, bestScan, bestP2, bestRegs > 64 ? 1 : 0, bestRegs, bestMs);
+                  "\"wide_registers\": %d, \"registers\": %d, \"incremental_sort\": %d, \"ms_per_step\": %.6f, "
+                  "\"trials\": [",
+                  bestBits, bestBlock, bestScan, bestP2, bestRegs > 64 ? 1 : 0, bestRegs, e->resortOn ? 1 : 0, bestMs);
     std::string out = std::string(buf) + log + "]}";
     std::snprintf(report, report_len, "%s", out.c_str());
   }

@@ -51,6 +51,12 @@ struct brt_engine {
   void* sortMem = nullptr;
   brt::SortScratch ss;
   uint32_t* errWord = nullptr;
+  // incremental re-sort (brt_resort.cu); option "incremental_sort"
+  bool resortOn = true;
+  uint32_t* resortMem = nullptr;   // one allocation carved into the arrays below
+  uint32_t *rsNewKey = nullptr, *rsPrefix = nullptr, *rsNext = nullptr, *rsBlockStay = nullptr;
+  uint32_t *rsCount = nullptr, *rsHead = nullptr, *rsNewStart = nullptr, *rsTiles = nullptr;
+  uint32_t *rsCounter = nullptr, *rsWords = nullptr, *rsStayBase = nullptr;
   float4* stage4 = nullptr;  // id-order staging (N float4)
   float* stageF = nullptr;   // id-order staging (N * Fmax)
   // pipeline state
@@ -113,6 +119,8 @@ inline int devAlloc(T** p, size_t count) {
 
 // Defined in brt_engine.cu.
 int engineEnqueueStep(brt_engine* e, float dt, bool record);
+// The canonical arrays were overwritten: the next step runs the full sort.
+cudaError_t engineInvalidateResort(brt_engine* e);
 int engineSyncAndCheck(brt_engine* e);
 
 }  // namespace brt

@@ -18,6 +18,9 @@
 namespace brt {
 
 constexpr uint32_t kEmpty = 0xFFFFFFFFu;
+// Sort mode of a fused step (the incremental re-sort's decision word): the
+// hash and radix passes run only in the full-sort mode.
+constexpr uint32_t kResortFullSort = 1u, kResortIncremental = 2u;
 
 // Device error word bits (set by kernels, read by brt_engine_check_device_error).
 constexpr uint32_t kDevErrLookback = 1u;   // onesweep look-back spin limit hit
@@ -146,8 +149,10 @@ size_t sortScratchBytes(const SortPlan& p, bool withTmp);
 SortScratch carveSortScratch(const SortPlan& p, void* base, bool withTmp);
 
 // Launch one onesweep pass.
+// gate (optional): the pass runs only if *gate == kResortFullSort.
 cudaError_t launchOnesweepPass(const SortPlan& p, uint32_t pass, const uint2* in, uint2* out,
-                               const SortScratch& s, uint32_t* errWord, cudaStream_t st);
+                               const SortScratch& s, uint32_t* errWord, cudaStream_t st,
+                               const uint32_t* gate = nullptr);
 // Histogram of all passes' digits (standalone sort only; the engine fuses it
 // into the hash kernel).
 cudaError_t launchSortHistogram(const SortPlan& p, const uint2* in, const SortScratch& s, cudaStream_t st);

@@ -27,6 +27,7 @@ namespace brt {
 // cell ranges and resets the sort's look-back state.
 __global__ void __launch_bounds__(256) hashKernel(HashArgs A) {
   extern __shared__ uint32_t sHist[];
+  if (A.gate && *A.gate != kResortFullSort) return;  // the incremental re-sort ordered this step
   const uint32_t histWords = A.passes * A.bins;
   for (uint32_t k = threadIdx.x; k < histWords; k += blockDim.x) sHist[k] = 0u;
   __syncthreads();
@@ -50,6 +51,7 @@ __global__ void __launch_bounds__(256) hashKernel(HashArgs A) {
   for (uint32_t k = gtid; k < A.statusWords; k += gstride) A.status[k] = 0u;
   if (gtid < A.passes) A.counters[gtid] = 0u;
   if (gtid == 0 && A.stepCounter) *A.stepCounter += 1u;
+  if (gtid == 0 && A.resortValid) *A.resortValid = 0u;
   __syncthreads();
   for (uint32_t k = threadIdx.x; k < histWords; k += blockDim.x)
     if (sHist[k]) atomicAdd(&A.hist[k], sHist[k]);
@@ -63,6 +65,15 @@ __global__ void __launch_bounds__(256) reorderKernel(ReorderArgs A) {
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t gstride = gridDim.x * blockDim.x;
   for (uint32_t k = gtid; k < A.histWords; k += gstride) A.hist[k] = 0u;
+  if (A.resortMode && *A.resortMode == kResortIncremental) {
+    // the hash kernel did not clear the ranges: clear those of cells that
+    // are empty now (the others are written below)
+    for (uint32_t c = gtid; c < A.numCells; c += gstride) {
+      const uint32_t next = c + 1 < A.numCells ? A.newStart[c + 1] : A.n;
+      if (A.newStart[c] == next) { A.cellStart[c] = kEmpty; A.cellEnd[c] = kEmpty; }
+    }
+  }
+  if (gtid == 0 && A.resortValid) *A.resortValid = 1u;
   for (uint32_t i = gtid; i < A.n; i += gstride) {
     const uint2 kv = A.pairs[i];
     const uint32_t key = kv.x, ps = kv.y;
@@ -95,7 +106,10 @@ __global__ void __launch_bounds__(256) reorderKernel(ReorderArgs A) {
       pos.w = sqrtf(nn);
     }
     A.posS[i] = pos;
-    if (key != prev) A.cellStart[key] = i;
+    if (key != prev) {
+      A.cellStart[key] = i;
+      if (A.moverHead) { A.moverHead[key] = kNoMover; A.moverCount[key] = 0u; }
+    }
     if (key != next) A.cellEnd[key] = i + 1;
   }
 }

@@ -25,6 +25,8 @@ struct HashArgs {
   uint32_t statusWords;
   uint32_t* counters;          // sort tile counters to clear
   uint32_t* stepCounter;       // random-stream step counter, incremented once per step
+  const uint32_t* gate;        // optional: run only when *gate == kResortFullSort
+  uint32_t* resortValid;       // optional: cleared (the cell ranges are cleared here)
 };
 
 struct ReorderArgs {
@@ -38,6 +40,11 @@ struct ReorderArgs {
   uint32_t* hist; uint32_t histWords;
   uint32_t n, numCells;
   uint32_t* errWord;
+  // incremental re-sort (all null outside the fused step)
+  const uint32_t* resortMode;  // the step's sort mode
+  const uint32_t* newStart;    // per cell, from the re-sort's cell scan
+  uint32_t* moverCount; uint32_t* moverHead;  // reset for every cell seen
+  uint32_t* resortValid;       // set: the next step may re-sort from this order
 };
 
 struct FusedArgs {
@@ -76,6 +83,44 @@ struct StageArgs {
   uint32_t nflocks, n, Fs;
   const uint32_t* stepCounter;
 };
+
+// Incremental re-sort (brt_resort.cu).  words[]: mode of the current step,
+// previous order valid (set by the fused step's reorder, cleared by the hash
+// kernel and by the host whenever the canonical order may have changed),
+// movers counted, a cell's mover list overflowed.
+constexpr uint32_t kResortChunk = 1024;   // slots per stayer-count block
+constexpr uint32_t kMaxMoversPerCell = 32;
+constexpr uint32_t kNoMover = 0xFFFFFFFFu;
+constexpr uint32_t kResortWordMode = 0, kResortWordValid = 1, kResortWordMovers = 2, kResortWordOverflow = 3;
+constexpr uint32_t kResortWordDone = 4;  // blocks of the mark kernel finished
+constexpr uint32_t kResortWords = 8;
+struct ResortArgs {
+  const float4* pos;             // canonical positions (previous sorted order)
+  const uint32_t* id;            // agent id per canonical slot
+  const uint2* prevPairs;        // previous step's sorted pairs: the previous key of each slot
+  const uint32_t* cellStart; const uint32_t* cellEnd;  // previous step's cell ranges
+  const FlockDev* flocks; const uint32_t* agentBase;
+  uint32_t nflocks, n, numCells;
+  uint32_t maxMovers;            // the full sort runs above this many movers
+  uint32_t* newKey;              // [n]
+  uint32_t* prefix;              // [n] stayers before the slot in its block, stay flag in bit 31
+  uint32_t* blockStay;           // [blocks + 1] stayer counts, then their exclusive scan
+  uint32_t* moverCount;          // [numCells], zero between steps
+  uint32_t* moverHead;           // [numCells], kNoMover between steps
+  uint32_t* moverNext;           // [n]
+  uint32_t* newStart;            // [numCells] first sorted position of each cell
+  uint32_t* stayBase;            // [numCells] newStart minus the stayers before the cell's previous range
+  uint32_t* tileStatus;          // [cell tiles] look-back state of the cell scan
+  uint32_t* tileCounter;
+  uint32_t* words;               // [kResortWords]
+  uint32_t* stepCounter;         // random-stream step (advanced here when the hash does not run)
+  uint2* out;                    // sorted pairs: the sort's final buffer
+  uint32_t* errWord;
+};
+uint32_t resortBlocks(uint32_t n);
+uint32_t resortCellTiles(uint32_t numCells);
+cudaError_t launchResortMark(const ResortArgs& A, cudaStream_t st);
+cudaError_t launchResortPlace(const ResortArgs& A, cudaStream_t st);
 
 // Reverse of one taped step (brt_adjoint.cu).
 constexpr uint32_t kAdjointThreads = 128;

@@ -76,7 +76,7 @@ template <int BITS>
 __global__ void __launch_bounds__(kSortThreads)
 onesweepKernel(const uint2* __restrict__ in, uint2* __restrict__ out, uint32_t n, uint32_t shift,
                uint32_t mask, const uint32_t* __restrict__ hist, uint32_t* __restrict__ status,
-               uint32_t* __restrict__ counter, uint32_t* __restrict__ errWord) {
+               uint32_t* __restrict__ counter, uint32_t* __restrict__ errWord, const uint32_t* gate) {
   constexpr int BINS = 1 << BITS;
   constexpr int T = kSortThreads;
   constexpr int WARPS = T / 32;
@@ -92,6 +92,7 @@ onesweepKernel(const uint2* __restrict__ in, uint2* __restrict__ out, uint32_t n
   __shared__ uint32_t sTile;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (gate && *gate != kResortFullSort) return;  // this step's order came from the incremental re-sort
   if (tid == 0) sTile = atomicAdd(counter, 1u);
   for (int k = tid; k < WARPS * BINS; k += T) (&sWarp[0][0])[k] = 0u;
   __syncthreads();
@@ -280,7 +281,7 @@ SortScratch carveSortScratch(const SortPlan& p, void* base, bool withTmp) {
 }
 
 cudaError_t launchOnesweepPass(const SortPlan& p, uint32_t pass, const uint2* in, uint2* out,
-                               const SortScratch& s, uint32_t* errWord, cudaStream_t st) {
+                               const SortScratch& s, uint32_t* errWord, cudaStream_t st, const uint32_t* gate) {
   if (p.n == 0) return cudaSuccess;
   const uint32_t shift = p.shift[pass], mask = passMask(p, pass);
   const uint32_t* hist = s.hist + (size_t)pass * p.bins;
@@ -288,12 +289,12 @@ cudaError_t launchOnesweepPass(const SortPlan& p, uint32_t pass, const uint2* in
   uint32_t* counter = s.counters + pass;
   dim3 grid(p.tiles), block(kSortThreads);
   switch (p.digitBits) {
-    case 4: onesweepKernel<4><<<grid, block, 0, st>>>(in, out, p.n, shift, mask, hist, status, counter, errWord); break;
-    case 5: onesweepKernel<5><<<grid, block, 0, st>>>(in, out, p.n, shift, mask, hist, status, counter, errWord); break;
-    case 6: onesweepKernel<6><<<grid, block, 0, st>>>(in, out, p.n, shift, mask, hist, status, counter, errWord); break;
-    case 7: onesweepKernel<7><<<grid, block, 0, st>>>(in, out, p.n, shift, mask, hist, status, counter, errWord); break;
-    case 8: onesweepKernel<8><<<grid, block, 0, st>>>(in, out, p.n, shift, mask, hist, status, counter, errWord); break;
-    case 9: onesweepKernel<9><<<grid, block, 0, st>>>(in, out, p.n, shift, mask, hist, status, counter, errWord); break;
+    case 4: onesweepKernel<4><<<grid, block, 0, st>>>(in, out, p.n, shift, mask, hist, status, counter, errWord, gate); break;
+    case 5: onesweepKernel<5><<<grid, block, 0, st>>>(in, out, p.n, shift, mask, hist, status, counter, errWord, gate); break;
+    case 6: onesweepKernel<6><<<grid, block, 0, st>>>(in, out, p.n, shift, mask, hist, status, counter, errWord, gate); break;
+    case 7: onesweepKernel<7><<<grid, block, 0, st>>>(in, out, p.n, shift, mask, hist, status, counter, errWord, gate); break;
+    case 8: onesweepKernel<8><<<grid, block, 0, st>>>(in, out, p.n, shift, mask, hist, status, counter, errWord, gate); break;
+    case 9: onesweepKernel<9><<<grid, block, 0, st>>>(in, out, p.n, shift, mask, hist, status, counter, errWord, gate); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

@@ -178,6 +178,13 @@ int brt_engine_set_params(brt_engine* e, uint32_t flock, const brt_params* p);
    knobs, Core/src/CommonResources.cpp:78-82, generalised):
      "sort_digit_bits"  4..9  radix digit width of the onesweep passes (default 8;
                               at most 4 passes, so narrow digits on wide keys widen)
+     "incremental_sort" 0/1   derive a fused step's sorted order from the
+                              previous step's when few agents changed cell
+                              (default 1); the device falls back to the full
+                              radix sort after a state change, when more
+                              than one agent in 8 moved, or when a cell
+                              received more than 32 movers.  The order is
+                              the same either way.
      "two_pass"         0/1   build each neighbour list before steering even
                               when the single-pass kernel applies (default 0)
      "block_size"       32..256, multiple of 32: threads per block of the
@@ -354,7 +361,9 @@ int brt_engine_check_device_error(brt_engine* e, uint32_t* word);
    brt_reorder_sim_data / brt_compute_neighborhoods, and the state arrays and
    the registered arrays share the sorted order once a step completes.  In an
    engine with features, sorted_pos4's w holds each agent's feature norm
-   (the state's pos4 keeps w = 1). */
+   (the state's pos4 keeps w = 1).  Kernels may change any value of the
+   state arrays but must not move agents between slots or rewrite agent_id:
+   the next step's incremental re-sort starts from the current slot order. */
 #define BRT_MAX_USER_ARRAYS 8
 typedef struct brt_arrays {
   uint32_t num_agents, num_cells, features_stride, list_stride;
