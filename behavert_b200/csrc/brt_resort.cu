@@ -37,9 +37,12 @@ namespace brt {
 namespace {
 
 constexpr uint32_t kStayBit = 0x80000000u;
-// fat tiles: few tiles keep the look-back short when every tile reaches it at once
-constexpr uint32_t kCellScanThreads = 1024;
-constexpr uint32_t kCellScanItems = 8;
+// Cell-scan tiles: THREADS threads of ITEMS consecutive cells, chosen per grid
+// (cellScanShape) for about kCellScanTilesTarget tiles: enough to fill the
+// GPU, few enough that the look-back stays short when every tile reaches it
+// at once.  Small grids take 256-thread tiles of 1 to 4 cells a thread, large
+// ones 1024-thread tiles of 8 (measured faster than 256 threads of 32).
+constexpr uint32_t kCellScanTilesTarget = 4 * 148;
 constexpr uint32_t kLookAgg = 1u << 30;
 constexpr uint32_t kLookInc = 2u << 30;
 constexpr uint32_t kLookMask = 3u << 30;
@@ -125,26 +128,41 @@ __global__ void __launch_bounds__(kMarkThreads) resortMarkKernel(ResortArgs A, u
   bool stay[kMarkItems], mover[kMarkItems];
   uint32_t bal[kMarkItems];
   uint32_t moving = 0;
+  // every load before any store: the arrays are not declared disjoint, so a
+  // store between them would keep the next item's loads waiting
+  float4 p[kMarkItems];
+  uint32_t prevKey[kMarkItems];
 #pragma unroll
   for (uint32_t k = 0; k < kMarkItems; ++k) {
     slot[k] = blockIdx.x * kResortChunk + k * kMarkThreads + threadIdx.x;
+    p[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+    prevKey[k] = 0;
+    if (slot[k] < A.n) {
+      p[k] = __ldg(&A.pos[slot[k]]);
+      prevKey[k] = __ldg(&A.prevPairs[slot[k]].x);
+    }
+  }
+#pragma unroll
+  for (uint32_t k = 0; k < kMarkItems; ++k) {
     stay[k] = false;
     mover[k] = false;
     key[k] = 0;
     if (slot[k] < A.n) {
       const uint32_t f = A.nflocks == 1 ? 0u : flockOfSlot(A.agentBase, A.nflocks, slot[k]);
       const FlockDev& fl = A.flocks[f];
-      const float4 p = __ldg(&A.pos[slot[k]]);
-      const int gx = gridCoord(p.x, fl.cell, fl.G), gy = gridCoord(p.y, fl.cell, fl.G), gz = gridCoord(p.z, fl.cell, fl.G);
+      const int gx = gridCoord(p[k].x, fl.cell, fl.G), gy = gridCoord(p[k].y, fl.cell, fl.G),
+                gz = gridCoord(p[k].z, fl.cell, fl.G);
       key[k] = fl.cellBase + ((uint32_t)gz * fl.G + (uint32_t)gy) * fl.G + (uint32_t)gx;
-      A.newKey[slot[k]] = key[k];
-      stay[k] = key[k] == A.prevPairs[slot[k]].x;
+      stay[k] = key[k] == prevKey[k];
       mover[k] = !stay[k];
     }
     bal[k] = __ballot_sync(0xffffffffu, stay[k]);
     moving += (uint32_t)__popc(__ballot_sync(0xffffffffu, mover[k]));
     if (lane == 0) sCount[k * kWarps + warp] = (uint32_t)__popc(bal[k]);
   }
+#pragma unroll
+  for (uint32_t k = 0; k < kMarkItems; ++k)
+    if (slot[k] < A.n) A.newKey[slot[k]] = key[k];
   // movers: both atomics of every item in flight together
   uint32_t prev[kMarkItems], count[kMarkItems];
 #pragma unroll
@@ -244,25 +262,26 @@ __device__ __forceinline__ uint32_t cellTotal(const ResortArgs& A, uint32_t c, u
   return t;
 }
 
-__global__ void __launch_bounds__(kCellScanThreads, 1) resortCellScanKernel(ResortArgs A) {
+template <uint32_t THREADS, uint32_t ITEMS>
+__global__ void __launch_bounds__(THREADS) resortCellScanKernel(ResortArgs A) {
   __shared__ uint32_t sTile, sPrefix;
-  __shared__ uint32_t sWarp[kCellScanThreads / 32 + 1];
+  __shared__ uint32_t sWarp[THREADS / 32 + 1];
   if (A.words[kResortWordMode] != kResortIncremental) return;
   if (threadIdx.x == 0) sTile = atomicAdd(A.tileCounter, 1u);
   __syncthreads();
   const uint32_t tile = sTile;
-  const uint32_t c0 = tile * kCellScanThreads * kCellScanItems + threadIdx.x * kCellScanItems;
-  uint32_t tot[kCellScanItems], ahead[kCellScanItems];
+  const uint32_t c0 = tile * THREADS * ITEMS + threadIdx.x * ITEMS;
+  uint32_t tot[ITEMS], ahead[ITEMS];
   uint32_t sum = 0;
 #pragma unroll
-  for (uint32_t k = 0; k < kCellScanItems; ++k) {
+  for (uint32_t k = 0; k < ITEMS; ++k) {
     const uint32_t c = c0 + k;
     ahead[k] = 0;
     tot[k] = c < A.numCells ? cellTotal(A, c, &ahead[k]) : 0u;
     sum += tot[k];
   }
   uint32_t tileTotal;
-  const uint32_t excl = ctaExclusiveScan<kCellScanThreads>(sum, sWarp, &tileTotal);
+  const uint32_t excl = ctaExclusiveScan<THREADS>(sum, sWarp, &tileTotal);
   if (threadIdx.x < 32) {
     // Warp-wide look-back: lane k reads predecessor p - k, so one round
     // covers 32 tiles (tiles that start together would otherwise walk back
@@ -306,7 +325,7 @@ __global__ void __launch_bounds__(kCellScanThreads, 1) resortCellScanKernel(Reso
   __syncthreads();
   uint32_t run = sPrefix + excl;
 #pragma unroll
-  for (uint32_t k = 0; k < kCellScanItems; ++k) {
+  for (uint32_t k = 0; k < ITEMS; ++k) {
     const uint32_t c = c0 + k;
     if (c < A.numCells) {
       A.newStart[c] = run;
@@ -364,8 +383,14 @@ __global__ void __launch_bounds__(256) resortPlaceKernel(ResortArgs A) {
 }  // namespace
 
 uint32_t resortBlocks(uint32_t n) { return (n + kResortChunk - 1) / kResortChunk; }
+// Cells per tile: 256 (1 a thread), 512, 1024 (256 threads) or 8192 (1024 threads of 8).
+static uint32_t cellScanTile(uint32_t numCells) {
+  for (uint32_t items = 1; items <= 4; items *= 2)
+    if ((numCells + 256u * items - 1) / (256u * items) <= kCellScanTilesTarget) return 256u * items;
+  return 8192u;
+}
 uint32_t resortCellTiles(uint32_t numCells) {
-  const uint32_t tile = kCellScanThreads * kCellScanItems;
+  const uint32_t tile = cellScanTile(numCells);
   return (numCells + tile - 1) / tile;
 }
 
@@ -377,7 +402,13 @@ cudaError_t launchResortMark(const ResortArgs& A, cudaStream_t st) {
 
 cudaError_t launchResortPlace(const ResortArgs& A, cudaStream_t st) {
   if (A.n == 0) return cudaSuccess;
-  resortCellScanKernel<<<resortCellTiles(A.numCells), kCellScanThreads, 0, st>>>(A);
+  const uint32_t tiles = resortCellTiles(A.numCells);
+  switch (cellScanTile(A.numCells)) {
+    case 256: resortCellScanKernel<256, 1><<<tiles, 256, 0, st>>>(A); break;
+    case 512: resortCellScanKernel<256, 2><<<tiles, 256, 0, st>>>(A); break;
+    case 1024: resortCellScanKernel<256, 4><<<tiles, 256, 0, st>>>(A); break;
+    default: resortCellScanKernel<1024, 8><<<tiles, 1024, 0, st>>>(A); break;
+  }
   resortPlaceKernel<<<(A.n + 255) / 256, 256, 0, st>>>(A);
   return cudaGetLastError();
 }
