@@ -889,7 +889,10 @@ int brt_engine_stage_times(brt_engine* e, double* ms4, uint64_t* steps, uint32_t
   }
   if (ms4) for (int k = 0; k < 4; ++k) ms4[k] = e->stageMs[k];
   if (steps) *steps = e->timedSteps;
-  if (launches_per_step) *launches_per_step = 3 + e->plan.passes;
+  // hash, radix passes, reorder, flock; with the incremental re-sort also its
+  // mark, cell-scan and place kernels (the hash and the passes still launch
+  // and return at once on the steps they are not needed)
+  if (launches_per_step) *launches_per_step = 3 + e->plan.passes + (e->resortOn ? 3 : 0);
   e->stageMs[0] = e->stageMs[1] = e->stageMs[2] = e->stageMs[3] = 0;
   e->timedSteps = 0;
   return BRT_OK;

@@ -259,7 +259,9 @@ int brt_step_prepare(brt_engine* e, float elapsedTime, uint32_t nsteps);
    sort, reorder and fused stages of every step.  brt_engine_stage_times
    synchronises and returns the accumulated milliseconds per stage
    (ms[0] hash, ms[1] all sort passes, ms[2] reorder + cell ranges, ms[3]
-   fused pass), the number of timed steps and the kernel launches per step. */
+   fused pass; with the incremental re-sort ms[0] also holds its mark kernel
+   and ms[1] its cell-scan and place kernels), the number of timed steps and
+   the kernel launches per step. */
 int brt_engine_stage_timing(brt_engine* e, int enable);
 int brt_engine_stage_times(brt_engine* e, double* ms4, uint64_t* steps, uint32_t* launches_per_step);
 
