@@ -113,6 +113,17 @@ __device__ __forceinline__ float imageShiftCells(int gi, int gj, uint32_t G, flo
   return d > 1 ? -L : (d < -1 ? L : 0.0f);
 }
 
+// Relaxed GPU-scope load and store: the look-back words of the radix passes
+// and of the re-sort's cell scan, polled and published across CTAs.
+__device__ __forceinline__ uint32_t ldRelaxed(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void stRelaxed(uint32_t* p, uint32_t v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 // Flock of a sorted slot (flocks own contiguous slot ranges).
 __device__ __forceinline__ uint32_t flockOfSlot(const uint32_t* __restrict__ agentBase, uint32_t nflocks, uint32_t slot) {
   uint32_t lo = 0, hi = nflocks;  // agentBase has nflocks+1 entries

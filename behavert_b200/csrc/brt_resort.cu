@@ -49,15 +49,6 @@ constexpr uint32_t kLookMask = 3u << 30;
 constexpr uint32_t kLookVal = (1u << 30) - 1u;
 constexpr uint32_t kLookSpinLimit = 1u << 21;
 
-__device__ __forceinline__ uint32_t ldRelaxed(const uint32_t* p) {
-  uint32_t v;
-  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void stRelaxed(uint32_t* p, uint32_t v) {
-  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
 // Stayers among slots [0, x) and [0, x].
 __device__ __forceinline__ uint32_t stayersBefore(const ResortArgs& A, uint32_t x) {
   return __ldg(&A.blockStay[x / kResortChunk]) + (__ldg(&A.prefix[x]) & ~kStayBit);

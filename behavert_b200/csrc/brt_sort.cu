@@ -31,15 +31,6 @@ constexpr uint32_t kFlagMask = 3u << 30;
 constexpr uint32_t kValMask = (1u << 30) - 1;
 constexpr uint32_t kLookbackSpinLimit = 1u << 21;
 
-__device__ __forceinline__ uint32_t ldRelaxed(const uint32_t* p) {
-  uint32_t v;
-  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void stRelaxed(uint32_t* p, uint32_t v) {
-  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
 // Exclusive scan of one value per thread across the CTA; returns the
 // exclusive prefix and writes the total to *total.
 template <int THREADS>
