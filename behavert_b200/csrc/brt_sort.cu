@@ -19,7 +19,6 @@
 #include "brt_internal.cuh"
 
 #include <algorithm>
-#include <mutex>
 #include <string>
 
 namespace brt {
@@ -369,30 +368,25 @@ constexpr size_t kNoAllocScratchBytes = a256(4 * 256 * 4) + a256(4 * 4) + a256(4
 
 static __device__ __align__(256) unsigned char g_noAllocSortScratch[kNoAllocScratchBytes];
 
-constexpr int kNoAllocMaxDevices = 64;
-std::mutex g_noAllocMutex;
-void* g_noAllocAddress[kNoAllocMaxDevices] = {};
-
 // The array's name is a host-side stand-in in host code, not a device
-// address: resolve the real address once per device, with that device current.
+// address.  The real address is looked up on every call, with the caller's
+// device current: the lookup allocates nothing and costs little, and a
+// cached address would go stale once the device's primary context is reset
+// or released and made again (the module then loads the array elsewhere).
 int noAllocScratchAddress(void** out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
+  if (e != cudaSuccess || dev < 0) {
     brt::setLastError("brt_radix_sort_pairs_noalloc: no usable current device");
     return BRT_ERR_NODEVICE;
   }
-  std::lock_guard<std::mutex> lock(g_noAllocMutex);
-  if (!g_noAllocAddress[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noAllocSortScratch);
-    if (e != cudaSuccess || !p) {
-      brt::setLastError(std::string("brt_radix_sort_pairs_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-      return BRT_ERR_CUDA;
-    }
-    g_noAllocAddress[dev] = p;
+  void* p = nullptr;
+  e = cudaGetSymbolAddress(&p, g_noAllocSortScratch);
+  if (e != cudaSuccess || !p) {
+    brt::setLastError(std::string("brt_radix_sort_pairs_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    return BRT_ERR_CUDA;
   }
-  *out = g_noAllocAddress[dev];
+  *out = p;
   return BRT_OK;
 }
 

@@ -3,7 +3,11 @@
 All randomness comes from ``numpy.random.default_rng(seed)`` (PCG64), drawn in
 the order written below, so a (config, seed, size) triple always yields the
 same arrays.  Positions are float32 in [0, worldSize); forward vectors are
-float32 unit directions with the speed in ``w``.
+float32 unit directions with the speed in ``w``.  ``defaults`` (plain, large)
+is the function that supplies the parameter defaults: the CUDA library's
+``brt_params_default`` unless a caller passes another source with the same
+values (the CPU reference arm of the benchmark passes the oracle's, so that it
+never loads the CUDA library).
 
   plain       config 0: 4,096 agents, cube 64, maxNeighbors 16, 200 steps
   large       config 1: 1,048,576 agents, cube 256, maxNeighbors 32, 70%
@@ -60,8 +64,8 @@ def _directions(rng, n):
     return d
 
 
-def _flock_params(n, L, M, weights=(1.5, 1.0, 1.0), F=0, relax=0.0) -> BrtParams:
-    p = params_default()
+def _flock_params(n, L, M, weights=(1.5, 1.0, 1.0), F=0, relax=0.0, defaults=None) -> BrtParams:
+    p = (defaults or params_default)()
     p.numBodies = int(n)
     p.worldSize = float(L)
     p.cellSize = 4.0
@@ -95,17 +99,17 @@ def cube_for(n: int, density: float = 1.0 / 16.0) -> float:
     return 4.0 * max(3, int(round((n / density) ** (1.0 / 3.0) / 4.0)))
 
 
-def plain(n: int = 4096, L: float = 64.0, M: int = 16, seed: int = 0, steps: int = 200) -> Workload:
+def plain(n: int = 4096, L: float = 64.0, M: int = 16, seed: int = 0, steps: int = 200, defaults=None) -> Workload:
     rng = np.random.default_rng(seed)
     pos, fwd = _agents(rng, n, L)
     acc = np.zeros((n, 4), np.float32)
-    return Workload("plain", [_flock_params(n, L, M)], pos, fwd, acc, None, steps, DT,
+    return Workload("plain", [_flock_params(n, L, M, defaults=defaults)], pos, fwd, acc, None, steps, DT,
                     {"config": 0, "seed": seed, "worldSize": L, "maxNeighbors": M})
 
 
 def large(n: int = 1 << 20, L: Optional[float] = None, M: int = 32, seed: int = 1, steps: int = 100,
           blob_fraction: float = 0.3, blobs: Optional[int] = None, sigma: float = 6.0, F: int = 8,
-          relax: float = 0.05) -> Workload:
+          relax: float = 0.05, defaults=None) -> Workload:
     if L is None:
         L = 256.0 if n == (1 << 20) else 4.0 * max(3, int(round(256.0 * (n / float(1 << 20)) ** (1.0 / 3.0) / 4.0)))
     if blobs is None:
@@ -120,7 +124,8 @@ def large(n: int = 1 << 20, L: Optional[float] = None, M: int = 32, seed: int = 
     pos[members, :3] = _below(pts, L)
     acc = np.zeros((n, 4), np.float32)
     feat = rng.random((n, F)).astype(np.float32) if F else None
-    return Workload("large", [_flock_params(n, L, M, F=F, relax=relax)], pos, fwd, acc, feat, steps, DT,
+    return Workload("large", [_flock_params(n, L, M, F=F, relax=relax, defaults=defaults)], pos, fwd, acc, feat,
+                    steps, DT,
                     {"config": 1, "seed": seed, "worldSize": L, "maxNeighbors": M, "blobs": blobs,
                      "blob_agents": nb, "sigma": sigma, "features": F, "relax": relax})
 

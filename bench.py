@@ -123,33 +123,62 @@ def dist_setup(args):
     return world, rank, local
 
 
+def _horizons(steps: int, horizon: int = E2E_HORIZON):
+    """Split `steps` into runs of at most `horizon` steps, each restarting from
+    the seeded state (config 1 is a 100-step run from its seeded state)."""
+    out = []
+    while steps > 0:
+        out.append(min(horizon, steps))
+        steps -= out[-1]
+    return out
+
+
+def bench_config(world: int) -> dict:
+    """The workload description; both arms print the same object."""
+    return {"workload": WORKLOAD, "horizon": E2E_HORIZON, "parallelism": "replicas" if world > 1 else "single"}
+
+
+def compact_tuned(t):
+    """The autotuner's choice without its trial list."""
+    if not t:
+        return t
+    return {k: v for k, v in t.items() if k != "trials"}
+
+
 def run_reference(args, world, rank):
-    """--impl reference: the CPU oracle (the reference's plugin logic restated
-    as multi-threaded C++; the reference itself cannot be built here) on a
-    bounded sample of the same workload, all host threads."""
+    """--impl reference: the reference's plugin logic on this path restated as
+    multi-threaded C++ (the CPU oracle; the reference's own CUDA cannot be
+    built here), on the box's host cores.  It times exactly --steps steps of
+    config 1, in runs of at most 100 steps that each restart from the seeded
+    state, like the GPU arm.  It loads only the oracle library: the workload's
+    parameter defaults come from the oracle, never from the CUDA library."""
     if rank != 0:
         return 0
     from behavert_b200 import workloads
     from oracle import oracle
-    w = workloads.large()
+    w = workloads.large(defaults=oracle.params_default)
     threads = oracle.hardware_threads()
-    pos, fwd, acc, feat = w.pos, w.fwd, w.acc, w.feat
-    for _ in range(max(0, min(args.warmup, 1))):
-        o = oracle.step(w.params, pos, fwd, acc, feat, dt=w.dt, threads=threads, want_intermediates=False)
-        pos, fwd, acc, feat = o["pos"], o["fwd"], o["acc"], o["feat"]
-    steps = max(1, min(args.steps, 3))
+
+    def run(nsteps):
+        pos, fwd, acc, feat = w.pos, w.fwd, w.acc, w.feat
+        for _ in range(nsteps):
+            o = oracle.step(w.params, pos, fwd, acc, feat, dt=w.dt, threads=threads, want_intermediates=False)
+            pos, fwd, acc, feat = o["pos"], o["fwd"], o["acc"], o["feat"]
+
+    run(args.warmup)
     t0 = time.perf_counter()
-    for _ in range(steps):
-        o = oracle.step(w.params, pos, fwd, acc, feat, dt=w.dt, threads=threads, want_intermediates=False)
-        pos, fwd, acc, feat = o["pos"], o["fwd"], o["acc"], o["feat"]
+    for h in _horizons(args.steps):
+        run(h)
     dt = time.perf_counter() - t0
+    steps = args.steps
     value = w.num_agents * steps / dt
-    sample = "%d full step(s) of the 1,048,576-agent config-1 state" % steps
+    sample = ("%d step(s) of the 1,048,576-agent config-1 workload from its seeded state (runs of at most %d "
+              "steps), the GPU arm's step count" % (steps, E2E_HORIZON))
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * dt / steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded config-1 generator)",
-        "config": {"workload": WORKLOAD, "parallelism": "cpu"},
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded config-1 generator, numpy PCG64 seed 1)",
+        "config": bench_config(world),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -206,10 +235,11 @@ def cpu_baseline_leg(w, eng_state_before, gpu_state_after, budget_s=12.0):
     return base, acc_err
 
 
-def batched_leg(device: int, steps: int = 100, loop_steps: int = 3):
+def batched_leg(device: int, steps: int = 100, loop_steps: int = 20, repeats: int = 3):
     """Config 2: 1,024 flocks of log-uniform sizes in one engine, the 100-step
     loop as one CUDA graph, against the same flocks stepped one engine per
-    flock (plain per-step launches, looped over the flocks)."""
+    flock (plain per-step launches, looped over the flocks).  Both sides are
+    the median of `repeats` timed runs from the seeded state."""
     import torch
     from behavert_b200 import Engine, workloads
     w = workloads.batched()
@@ -221,15 +251,14 @@ def batched_leg(device: int, steps: int = 100, loop_steps: int = 3):
     eng.step(dt, 3)
     tuned = eng.autotune(dt, steps=5)
     eng.step_prepare(dt, steps)
-    eng.sync()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    eng.step(dt, steps)
-    e1.record(stream)
-    e1.synchronize()
-    t_batched = e0.elapsed_time(e1) / 1e3
+    t_batched = []
+    for _ in range(repeats):
+        eng.set_state(w.pos, w.fwd, w.acc)
+        eng.sync()
+        t_batched.append(_events_ms(stream, lambda: eng.step(dt, steps)) / 1e3)
     eng.sync()
     eng.close()
+    t_batched = float(np.median(t_batched))
     # looped per-flock launches
     engines = []
     off = 0
@@ -237,32 +266,38 @@ def batched_leg(device: int, steps: int = 100, loop_steps: int = 3):
         e = Engine([p], device=device)
         # the full sort every step: fewer launches a step, the faster loop
         e.set_option("incremental_sort", 0)
-        k = int(p.numBodies)
-        e.set_state(np.ascontiguousarray(w.pos[off:off + k]), np.ascontiguousarray(w.fwd[off:off + k]),
-                    np.ascontiguousarray(w.acc[off:off + k]))
-        off += k
-        e.step(dt, 1)
         engines.append(e)
-    for e in engines:
-        e.sync()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(loop_steps):
-        for e in engines:
+    t_loops = []
+    for _ in range(repeats):
+        off = 0
+        for e, p in zip(engines, w.params):
+            k = int(p.numBodies)
+            e.set_state(np.ascontiguousarray(w.pos[off:off + k]), np.ascontiguousarray(w.fwd[off:off + k]),
+                        np.ascontiguousarray(w.acc[off:off + k]))
+            off += k
             e.step(dt, 1)
-    for e in engines:
-        e.sync()
-    t_loop = time.perf_counter() - t0
+        for e in engines:
+            e.sync()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(loop_steps):
+            for e in engines:
+                e.step(dt, 1)
+        for e in engines:
+            e.sync()
+        t_loops.append((time.perf_counter() - t0) / loop_steps)
     for e in engines:
         e.close()
+    t_loop = float(np.median(t_loops))
     batched = n * steps / t_batched
-    looped = n * loop_steps / t_loop
+    looped = n / t_loop
     return {"workload": "config 2: %d flocks, %d agents, sizes log-uniform [128, 65536], maxNeighbors 16" %
                         (len(w.params), n),
             "value": batched, "unit": UNIT, "ms_per_step": 1e3 * t_batched / steps, "steps": steps,
-            "looped_value": looped, "looped_ms_per_step": 1e3 * t_loop / loop_steps,
+            "looped_value": looped, "looped_ms_per_step": 1e3 * t_loop,
+            "looped_ms_per_step_runs": [1e3 * t for t in t_loops],
             "looped": "one engine per flock (full sort each step), %d steps of plain per-step launches looped "
-                      "over the flocks" % loop_steps,
+                      "over the flocks, median of %d runs" % (loop_steps, repeats),
             "speedup_vs_looped": batched / looped, "tuned": tuned}
 
 
@@ -457,8 +492,8 @@ def fitting_leg(device: int, iters: int = 200):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=4000)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
@@ -523,7 +558,16 @@ def main():
         return 0
 
     stream = torch.cuda.ExternalStream(eng.stream_handle())
-    # warm-up (single steps), then capture the K-step graph outside the timed region
+    from behavert_b200._abi import BRT_MEM_DEVICE, BRT_MEM_HOST, check, lib, ptr
+    h = eng.handle
+    dev = torch.device("cuda:%d" % local)
+    # the seeded state, resident in HBM: every run of the timed region starts from it
+    seeded = [torch.from_numpy(np.ascontiguousarray(x)).to(dev) for x in (w.pos, w.fwd, w.acc, w.feat)]
+
+    def reset_to_seeded():
+        check(lib().brt_set_state(h, *(ptr(x) for x in seeded), BRT_MEM_DEVICE), "set_state")
+
+    # warm-up (single steps), the autotuner, then the graphs of the timed runs
     for _ in range(args.warmup):
         eng.step(dt, 1)
     eng.sync()
@@ -531,9 +575,18 @@ def main():
     state_before = eng.get_state()
     eng.step(dt, 1)
     state_after = eng.get_state()
-    eng.step_prepare(dt, args.steps)
+    horizons = _horizons(args.steps)
+    for hs in sorted(set(horizons)):
+        eng.step_prepare(dt, hs)
     eng.sync()
 
+    def timed_runs():
+        for hs in horizons:
+            reset_to_seeded()
+            check(lib().brt_step(h, dt, hs), "step")
+
+    timed_runs()  # one untimed pass of the same sequence
+    eng.sync()
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)
@@ -544,7 +597,7 @@ def main():
     e1 = torch.cuda.Event(enable_timing=True)
     t_wall0 = time.time()
     e0.record(stream)
-    eng.step(dt, args.steps)
+    timed_runs()
     e1.record(stream)
     e1.synchronize()
     t_wall1 = time.time()
@@ -560,8 +613,9 @@ def main():
     ms_per_step = elapsed_ms / args.steps
     value = world * n * args.steps / (elapsed_ms / 1e3)
 
-    # second timed pass: per-stage CUDA events (single-step launches)
-    stage_steps = min(args.steps, 400)
+    # second timed pass: per-stage CUDA events (single-step launches from the seeded state)
+    stage_steps = min(args.steps, E2E_HORIZON)
+    reset_to_seeded()
     eng.stage_timing(True)
     for _ in range(stage_steps):
         eng.step(dt, 1)
@@ -569,16 +623,13 @@ def main():
     eng.stage_timing(False)
     stage_avg = [m / max(1, timed) for m in stage_ms]
 
-    # e2e through the C-ABI with pinned host buffers
+    # e2e through the C-ABI with pinned host buffers: upload the seeded state,
+    # run config 1's 100-step horizon, read the state back
     F = w.feat.shape[1]
-    hpos = torch.from_numpy(state_before[0]).pin_memory()
-    hfwd = torch.from_numpy(state_before[1]).pin_memory()
-    hacc = torch.from_numpy(state_before[2]).pin_memory()
-    hfeat = torch.from_numpy(state_before[3]).pin_memory()
+    hpos, hfwd, hacc, hfeat = (torch.from_numpy(np.ascontiguousarray(x)).pin_memory()
+                               for x in (w.pos, w.fwd, w.acc, w.feat))
     opos, ofwd, oacc, ofeat = (torch.empty_like(x).pin_memory() for x in (hpos, hfwd, hacc, hfeat))
     eng.step_prepare(dt, E2E_HORIZON)
-    from behavert_b200._abi import BRT_MEM_HOST, check, lib, ptr
-    h = eng.handle
     if pg:
         pg.barrier()
     torch.cuda.synchronize()
@@ -597,6 +648,16 @@ def main():
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         e2e_ms = float(t.item())
     e2e_value = world * n * E2E_HORIZON * args.e2e_iters / (e2e_ms / 1e3)
+
+    # the same timed runs with the full onesweep sort on every step (the
+    # incremental re-sort off), so the radix path stays measured
+    eng.set_option("incremental_sort", 0)
+    for hs in sorted(set(horizons)):
+        eng.step_prepare(dt, hs)
+    timed_runs()
+    eng.sync()
+    full_sort_ms = _events_ms(stream, timed_runs) / args.steps
+    eng.set_option("incremental_sort", 1)
     state_bytes = n * (16 * 3 + 4 * F)
 
     hbm, peak_kind = peaks()
@@ -618,11 +679,13 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded config-1 generator, numpy PCG64 seed 1)",
-        "config": {"workload": WORKLOAD, "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "no flush between steps: per-step working set ~%.0f MB > 126 MB L2" %
+        "config": bench_config(world),
+        "timing": {"l2": "no flush between steps: per-step working set ~%.0f MB > 126 MB L2" %
                          ((2 * state_bytes + 16 * n + 8 * eng.num_cells) / 1e6),
-                   "graph": "K steps as one CUDA graph",
-                   "tuned": tuned},
+                   "graph": "runs of at most %d steps (config 1's horizon), each restarting from the seeded state "
+                            "(a device-side state reset, inside the timed region) and launched as one CUDA graph"
+                            % E2E_HORIZON},
+        "tuned": compact_tuned(tuned),
         "roofline": {"bound": "hbm", "kernel": "flockKernel (fused neighbour search + steering + integration)",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
@@ -635,7 +698,8 @@ def main():
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes / E2E_HORIZON,
                 "d2h_bytes_per_step": state_bytes / E2E_HORIZON,
                 "note": "each call: upload state, %d-step horizon, read state back" % E2E_HORIZON},
-        "gpu_launches": args.steps * launches_per_step,
+        "gpu_launches": args.steps * launches_per_step + 4 * len(horizons),
+        "full_sort_ms_per_step": full_sort_ms,
         "clocks": clocks.summary(t_wall0, t_wall1),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -651,12 +715,49 @@ def main():
             line["adjoint"]["accuracy"] = adjoint_accuracy(local)
     if world == 1 and not args.no_fit:
         line["fitting"] = fitting_leg(local, args.fit_iters)
+    for leg in ("batched", "adjoint", "fitting"):
+        if leg in line and isinstance(line[leg].get("tuned"), dict):
+            line[leg]["tuned"] = compact_tuned(line[leg]["tuned"])
+    line.update(summary_keys(line))
     if pg:
         pg.barrier()
         pg.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+        short = {k: v for k, v in line.items() if not isinstance(v, (dict, list))}
+        sys.stderr.write("summary: %s\n" % json.dumps(short))
     return 0
+
+
+def summary_keys(line: dict) -> dict:
+    """Flat scalar copies of the legs' headline figures, so that a reader of
+    the top level sees them without the nested objects."""
+    out = {}
+    acc = line.get("accuracy")
+    if acc:
+        out["fp64_max_rel_err"] = max(acc[k]["max"] for k in ("pos_vs_fp64", "vel_vs_fp64", "feat_vs_fp64"))
+        out["fp64_p9999_rel_err"] = max(acc[k]["p9999"] for k in ("pos_vs_fp64", "vel_vs_fp64", "feat_vs_fp64"))
+        out["fp64_within_1e-5"] = acc["within_tolerance"]
+    b = line.get("batched")
+    if b:
+        out["batched_agent_steps_per_s"] = b["value"]
+        out["batched_ms_per_step"] = b["ms_per_step"]
+        out["batched_speedup_vs_looped"] = b["speedup_vs_looped"]
+    a = line.get("adjoint")
+    if a:
+        out["adjoint_cost_vs_forward"] = a["cost_vs_forward"]
+        ac = a.get("accuracy")
+        if ac:
+            out["adjoint_weights_rel_err_vs_fd_h1e-06"] = ac["weights_rel_err_gpu_vs_fd_h1e-06"]
+            out["adjoint_weights_rel_err_vs_fp64_reverse"] = ac["weights_rel_err_vs_fp64_reverse"]
+            out["adjoint_pos_grad_rel_err_normwise"] = ac["pos_grad_rel_err"]["normwise"]
+            out["adjoint_vel_grad_rel_err_normwise"] = ac["vel_grad_rel_err"]["normwise"]
+    f = line.get("fitting")
+    if f:
+        out["fit_iters_per_s"] = f["fit_iters_per_s"]
+        out["fit_speedup_vs_looped"] = f["speedup_vs_looped"]
+        out["fit_recovered_weight_median_abs_err"] = f["recovered_weight_abs_err"]["median"]
+    return out
 
 
 if __name__ == "__main__":

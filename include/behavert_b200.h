@@ -454,14 +454,16 @@ int brt_radix_sort_pairs(const uint32_t* pairs_in, uint32_t* pairs_out, uint32_t
    (about 10 MiB on every GPU that loads it, held until the process exits), so:
      - n is limited to brt_radix_sort_noalloc_max_pairs() (1,048,576) pairs;
        larger n returns BRT_ERR_CAPACITY;
-     - the first call on a device looks up the array's device address for the
-       current device; make that first call before any stream capture;
+     - every call looks up the array's device address on the current device
+       (cudaGetSymbolAddress, which allocates nothing), so a device reset or a
+       re-created primary context never leaves it a stale address;
      - every call clears the parts of the array that must start at zero, but
        all calls share the array: calls that overlap on the GPU (other
        streams, other host threads) race and must be serialised by the caller;
      - it allocates nothing: no cudaMalloc, cudaFree or allocating library call.
-   Results are identical to brt_radix_sort_pairs; the call synchronises
-   `stream` to read the device error word. */
+   Results are identical to brt_radix_sort_pairs.  Before it returns, the call
+   copies the device error word to the host and synchronises `stream`, so the
+   host waits for the sort to finish. */
 size_t brt_radix_sort_noalloc_max_pairs(void);
 int brt_radix_sort_pairs_noalloc(const uint32_t* pairs_in, uint32_t* pairs_out, uint32_t n,
                                  uint32_t bits, void* stream);

@@ -9,9 +9,7 @@
 // for this path, and its GPU code cannot be built here (cutil, texture
 // references, GL interop, MSVC-only constructs).  This restatement is therefore
 // "parity unpinned" against reference-produced outputs; each function cites
-// the reference lines it follows.  The integration maths is cross-checked
-// against the reference's CPU OpenSteer sources where they agree
-// (tests/test_oracle_opensteer.py).
+// the reference lines it follows.
 //
 // Two modes share one template:
 //   mode 0 (FP32): float arithmetic in the reference's operation order, built
@@ -843,5 +841,44 @@ int oracle_num_cells(uint32_t nflocks, const brt_params* params, uint32_t* cells
 }
 
 int oracle_hardware_threads(void) { return (int)std::max(1u, std::thread::hardware_concurrency()); }
+
+// The parameter defaults of the workloads, restated for the CPU side so that
+// a CPU-only run never loads the CUDA library: the flocking demo's values
+// (OpenSteerWrapperPlugIn install defaults, weights 1.5 / 1 / 1 of
+// BehaveRT_Flocking.cpp), the unspecified constants fixed for this path
+// (commonMass 1, sensing min radius 0, cosMaxAngle -2, maxBodiesPerCell
+// unbounded, clustering steering off) and the Schooling install constants
+// (SchoolingPlugIn.h:115-160).  A CPU test checks that the bytes equal the
+// library's brt_params_default.
+int oracle_params_default(brt_params* p) {
+  if (!p) return BRT_ERR_ARG;
+  std::memset(p, 0, sizeof(*p));
+  p->numBodies = 4096;
+  p->commonRadius = 1.0f;
+  p->worldSize = 64.0f;
+  p->cellSize = 4.0f;
+  p->maxNeighbors = 16;
+  p->commonSearchRadius = 4.0f;
+  p->commonMaxSpeed = 1.0f;
+  p->commonMaxForce = 0.1f;
+  p->commonMass = 1.0f;
+  const float w[3] = {1.5f, 1.0f, 1.0f};
+  float* tri[3] = {p->separationParams, p->alignmentParams, p->cohesionParams};
+  for (int k = 0; k < 3; ++k) { tri[k][0] = w[k]; tri[k][1] = 4.0f; tri[k][2] = -2.0f; }
+  p->similarityStatsParams[0] = 0.01f;
+  p->similarityStatsParams[1] = 0.1f;
+  p->similarityStatsParams[2] = 0.001f;
+  p->avgSimilarityController = 1.0f;
+  p->schooling.theta = (float)std::cos(0.1);
+  p->schooling.delta = 0.01f;
+  p->schooling.r_r = 1.0f;
+  p->schooling.r_p = 4.0f;
+  p->schooling.eta = (float)std::cos(3.05);
+  p->schooling.w_a = 1.0f;
+  p->schooling.w_o = 16.0f;
+  p->schooling.s = 3.0f;
+  p->schooling.randomDeviationWeight = 0.1f;
+  return BRT_OK;
+}
 
 }  // extern "C"

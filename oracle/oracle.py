@@ -46,6 +46,8 @@ def lib():
         L.oracle_num_cells.restype = C.c_int
         L.oracle_num_cells.argtypes = [C.c_uint32, _vp, _u32p]
         L.oracle_hardware_threads.restype = C.c_int
+        L.oracle_params_default.restype = C.c_int
+        L.oracle_params_default.argtypes = [_vp]
         L.oracle_frozen_forward.restype = C.c_int
         L.oracle_frozen_forward.argtypes = [C.c_uint32, _vp, _vp, C.c_uint32, C.c_double, _vp, _vp, _vp, _vp,
                                             _vp, _vp, _vp, _vp, _vp, C.c_int]
@@ -54,6 +56,18 @@ def lib():
                                             _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int]
         _LIB = L
     return _LIB
+
+
+def params_default():
+    """BrtParams filled with the workloads' defaults by the oracle library
+    (equal, byte for byte, to the CUDA library's brt_params_default), so a
+    CPU-only run builds its workload without loading the CUDA library."""
+    from behavert_b200._abi import BrtParams
+    p = BrtParams()
+    rc = lib().oracle_params_default(C.byref(p))
+    if rc:
+        raise RuntimeError("oracle_params_default failed: %d" % rc)
+    return p
 
 
 def hardware_threads() -> int:

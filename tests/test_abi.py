@@ -4,6 +4,7 @@ the C layout, and calls fail loudly (no CPU fallback) when no GPU is present."""
 import ctypes as C
 import re
 import subprocess
+import sys
 from pathlib import Path
 
 import pytest
@@ -89,3 +90,25 @@ def test_facade_header_compiles():
         subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", str(ROOT / "include"), str(probe)], check=True)
     finally:
         probe.unlink(missing_ok=True)
+
+
+def test_oracle_params_default_equals_the_library_defaults():
+    """The CPU reference arm builds its workload from the oracle's defaults so
+    that it never loads the CUDA library; both sources must agree byte for byte."""
+    from oracle import oracle
+    a = bytes(brt.params_default())
+    b = bytes(oracle.params_default())
+    assert a == b
+
+
+def test_reference_arm_workload_does_not_load_the_cuda_library():
+    """Building config 1 with the oracle's defaults and stepping the oracle
+    maps no library of the product into the process."""
+    code = ("import sys; sys.path.insert(0, %r)\n"
+            "from behavert_b200 import workloads\nfrom oracle import oracle\n"
+            "w = workloads.large(n=4096, defaults=oracle.params_default)\n"
+            "oracle.step(w.params, w.pos, w.fwd, w.acc, w.feat, dt=w.dt, want_intermediates=False)\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "assert 'libbehavert_b200' not in maps and '_brt_torch' not in maps, 'product library loaded'\n"
+            "assert 'liboracle_brt' in maps\n" % str(ROOT))
+    subprocess.run([sys.executable, "-c", code], check=True, timeout=300)

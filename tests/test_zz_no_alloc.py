@@ -51,6 +51,24 @@ def test_noalloc_matches_allocating_sort_twice_in_a_row():
         assert np.array_equal(got, pairs[order])
 
 
+def test_noalloc_leaves_free_device_memory_unchanged():
+    """The property the entry point exists for: after one warm-up call (which
+    may make the module commit the static array), further calls take no
+    device memory."""
+    import torch
+    n, bits = 300000, 16
+    din = torch.from_numpy(_pairs(n, bits, 7).view(np.int32)).cuda()
+    out = torch.empty_like(din)
+    _noalloc(din, out, n, bits)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(5):
+        _noalloc(din, out, n, bits)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+
+
 def test_noalloc_rejects_sizes_beyond_the_static_scratch():
     import torch
     n = (1 << 20) + 1
