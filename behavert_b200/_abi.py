@@ -176,6 +176,7 @@ _SIGS = {
     "brt_adjoint_forward": (C.c_int, [_vp, C.c_float, C.c_uint32, C.c_uint32, _vp, C.c_int, _vp]),
     "brt_adjoint_backward": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_int]),
     "brt_adjoint_get_tape": (C.c_int, [_vp, _vp, _vp, C.c_int]),
+    "brt_adjoint_get_tape_states": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int]),
     "brt_set_steering_weights": (C.c_int, [_vp, _vp, C.c_int]),
     "brt_get_steering_weights": (C.c_int, [_vp, _vp, C.c_int]),
     "brt_radix_sort_scratch_bytes": (C.c_size_t, [C.c_uint32, C.c_uint32]),

@@ -41,18 +41,36 @@ def _stale(target: Path, deps) -> bool:
 
 
 def build_library(force: bool = False, verbose: bool = False) -> Path:
+    """Compiles every source to an object in parallel (each translation unit
+    is self-contained: no device code crosses files), then links."""
     deps = [CSRC / s for s in SOURCES] + [CSRC / h for h in HEADERS] + [ROOT / "include" / "behavert_b200.h", Path(__file__)]
     if not force and not _stale(LIB, deps):
         return LIB
-    cmd = [_nvcc(), *NVCC_FLAGS, "-I", str(ROOT / "include"), "-o", str(LIB), *[str(CSRC / s) for s in SOURCES]]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    res = subprocess.run(cmd, capture_output=True, text=True)
-    if res.returncode != 0:
-        sys.stderr.write(res.stdout + res.stderr)
-        raise RuntimeError("nvcc failed building libbehavert_b200.so")
-    if verbose:
-        sys.stderr.write(res.stderr)
+    import concurrent.futures as cf
+    import tempfile
+    compile_flags = [f for f in NVCC_FLAGS if f not in ("-shared",)]
+    with tempfile.TemporaryDirectory(prefix="brt_build_") as tmp:
+        def compile_one(src):
+            obj = Path(tmp) / (src + ".o")
+            cmd = [_nvcc(), *compile_flags, "-I", str(ROOT / "include"), "-c", "-o", str(obj), str(CSRC / src)]
+            if verbose:
+                cmd.insert(1, "-Xptxas=-v")
+            return obj, subprocess.run(cmd, capture_output=True, text=True)
+        workers = max(1, min(len(SOURCES), os.cpu_count() or 1))
+        with cf.ThreadPoolExecutor(workers) as ex:
+            results = list(ex.map(compile_one, SOURCES))
+        for _, res in results:
+            if res.returncode != 0:
+                sys.stderr.write(res.stdout + res.stderr)
+                raise RuntimeError("nvcc failed building libbehavert_b200.so")
+            if verbose:
+                sys.stderr.write(res.stderr)
+        link = [_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-cudart", "static",
+                "-Xcompiler", "-fPIC", "-o", str(LIB), *[str(o) for o, _ in results]]
+        res = subprocess.run(link, capture_output=True, text=True)
+        if res.returncode != 0:
+            sys.stderr.write(res.stdout + res.stderr)
+            raise RuntimeError("linking libbehavert_b200.so failed")
     return LIB
 
 

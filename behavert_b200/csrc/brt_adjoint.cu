@@ -13,11 +13,22 @@
 // Indexing.  A step reads its input in the canonical order left by the
 // previous step, sorts it, and writes its output in its own sorted order.
 // The adjoint of a step's output is therefore indexed by the step's sorted
-// slot (read coalesced, then zeroed so the buffer can take the next-earlier
-// step's accumulation), and the adjoint of its input by canonical slot =
-// the reorder's source slot `prev` of each sorted slot.  Neighbour
-// contributions go into the input adjoint with float4 atomics; neighbours are
-// near each other in both orders, so the atomics stay local in L2.
+// slot, and the adjoint of its input by canonical slot = the reorder's
+// source slot `prev` of each sorted slot.
+//
+// Determinism.  The reverse of a step runs in two kernels, and no float is
+// ever accumulated with an atomic:
+//   emit    one thread per agent i: recomputes the forward, forms its own
+//           adjoint terms and, for each list entry (i, k), the adjoint it
+//           sends to the listed agent j, stored at the entry; the entry code
+//           goes into j's in-list (an inbox whose positions come from an
+//           atomic counter: the transposed neighbour list of the frozen step);
+//   gather  one thread per agent j: sorts its in-list by entry code (i, k),
+//           adds the stored contributions in that order to its own terms and
+//           stores its input adjoint (every canonical slot is written once).
+// The weight adjoint is summed per agent over the steps in FP64 (each agent
+// by its own thread, in step order) and reduced per flock in a fixed tree at
+// the end.  Two runs from the same state give the same bits.
 #include "brt_agent.cuh"
 #include "brt_kernels.cuh"
 
@@ -38,32 +49,43 @@ __device__ __forceinline__ f3 clipBar(f3 x, float m, f3 ybar) {
   return mul3(sub3(ybar, mul3(h, dot3(h, ybar))), m / l);
 }
 
-__device__ __forceinline__ void atomicAdd3(float4* dst, f3 v, float w) {
-  atomicAdd(dst, make_float4(v.x, v.y, v.z, w));
+// Adjoint, with respect to the neighbour's offset o (|o|^2 = d2), of the
+// separation term -o / |o|^2 given the adjoint g of the agent's separation
+// sum divided by its count: -(g / d2 - 2 o (o . g) / d2^2).  Emit and gather
+// evaluate it with this one sequence, so both sides hold the same bits.
+__device__ __forceinline__ f3 separationBar(f3 o, float d2, f3 g) {
+  return mul3(sub3(div3(g, d2), mul3(o, 2.0f * dot3(o, g) / (d2 * d2))), -1.0f);
 }
 
-// Per-flock FP64 sum of three values over a warp, then into `out`.
-__device__ __forceinline__ void warpFlockSum3(double* out, uint32_t f, bool valid, double v0, double v1, double v2) {
-  const uint32_t full = 0xFFFFFFFFu;
-  const uint32_t f0 = __shfl_sync(full, f, 0);
-  if (__all_sync(full, !valid || f == f0)) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      v0 += __shfl_down_sync(full, v0, o);
-      v1 += __shfl_down_sync(full, v1, o);
-      v2 += __shfl_down_sync(full, v2, o);
-    }
-    if ((threadIdx.x & 31u) == 0u) {
-      atomicAdd(&out[3 * f0 + 0], v0);
-      atomicAdd(&out[3 * f0 + 1], v1);
-      atomicAdd(&out[3 * f0 + 2], v2);
-    }
-  } else if (valid) {
-    atomicAdd(&out[3 * f + 0], v0);
-    atomicAdd(&out[3 * f + 1], v1);
-    atomicAdd(&out[3 * f + 2], v2);
+// Compensated sum of float3 terms (Knuth's TwoSum per component; exact
+// error terms, since the library is built without contraction).
+struct Comp3 {
+  f3 s = {0.f, 0.f, 0.f}, e = {0.f, 0.f, 0.f};
+  __device__ __forceinline__ static void twoSum(float& sum, float& err, float t) {
+    const float n = sum + t;
+    const float bb = n - sum;
+    err += (sum - (n - bb)) + (t - bb);
+    sum = n;
   }
+  __device__ __forceinline__ void add(f3 t) { twoSum(s.x, e.x, t.x); twoSum(s.y, e.y, t.y); twoSum(s.z, e.z, t.z); }
+  __device__ __forceinline__ f3 value() const { return add3(s, e); }
+};
+
+// vecLimitDeviationAngle's result once the source is outside the cone
+// (Core/common_resources.cu:214-227): the vector of the source's length on
+// the cone's surface, in the plane of the source and the basis.
+__device__ __forceinline__ f3 limitedDeviation(f3 source, float cosineOfConeAngle, f3 basis) {
+  const float sourceLength = len3(source);
+  const f3 perp = sub3(source, mul3(basis, dot3(source, basis)));
+  const f3 unitPerp = normalize3(perp);
+  const float perpDist = sqrtf(1.0f - (cosineOfConeAngle * cosineOfConeAngle));
+  return mul3(add3(mul3(basis, cosineOfConeAngle), mul3(unitPerp, perpDist)), sourceLength);
 }
+
+// In-list entries a gather thread sorts in local memory; longer in-lists
+// (rare: that many agents listing one neighbour) are processed in ascending
+// order by repeated selection instead.
+constexpr uint32_t kGatherCap = 64;
 
 }  // namespace
 
@@ -86,14 +108,19 @@ __global__ void __launch_bounds__(kAdjointThreads) adjointStepKernel(AdjointStep
     const uint32_t n = lst[0];
     const uint32_t self = __ldg(&A.prev[i]);
 
-    // The adjoint of this step's output; the buffers are zeroed for the
-    // accumulation of the next-earlier step.
+    // The adjoint of this step's output.
     const float4 gOp = A.gOutP[i], gOf = A.gOutF[i], gOa = A.gOutA[i];
-    A.gOutP[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-    A.gOutF[i] = make_float4(0.f, 0.f, 0.f, 0.f);
 
     // --- forward recomputation (flockingSteer's sequence) -----------------
+    // Two evaluations of the three neighbour sums.  The forward's own order
+    // (x, steer) decides every branch exactly as the forward did.  The
+    // adjoint is linearised at the sums taken in offset form with
+    // compensated (TwoSum) accumulation (xL, steerL): the cohesion sum in
+    // the forward's form, (sum of positions) / n - own position, cancels
+    // coordinates of the world's size down to about one and keeps only
+    // ~1e-4 of its value, which the 50-step reverse would amplify.
     f3 sSep = mk3(0.f, 0.f, 0.f), sAli = mk3(0.f, 0.f, 0.f), sCoh = mk3(0.f, 0.f, 0.f);
+    Comp3 cpSep, cpAli, cpCoh;
     uint32_t cSep = 0, cAli = 0, cCoh = 0, mS = 0, mA = 0, mC = 0;
     for (uint32_t k = 0; k < n; ++k) {
       const uint32_t j = lst[1 + k];
@@ -104,34 +131,49 @@ __global__ void __launch_bounds__(kAdjointThreads) adjointStepKernel(AdjointStep
       const f3 nrm = mul3(offset, 1.0f / dist);
       const float cosAngle = dot3(a.fwd, nrm);
       if (inBoid(dist, cosAngle, fl.minR, fl.sep[1], fl.sep[2])) {
-        sSep = add3(sSep, div3(offset, -d2));
+        const f3 t = div3(offset, -d2);
+        sSep = add3(sSep, t);
+        cpSep.add(t);
         ++cSep;
         mS |= 1u << k;
       }
       if (inBoid(dist, cosAngle, fl.minR, fl.ali[1], fl.ali[2])) {
-        sAli = add3(sAli, xyz(__ldg(&A.fwdS[j])));
+        const f3 fj = xyz(__ldg(&A.fwdS[j]));
+        sAli = add3(sAli, fj);
+        cpAli.add(sub3(fj, a.fwd));
         ++cAli;
         mA |= 1u << k;
       }
       if (inBoid(dist, cosAngle, fl.minR, fl.coh[1], fl.coh[2])) {
         sCoh = add3(sCoh, other);
+        cpCoh.add(offset);
         ++cCoh;
         mC |= 1u << k;
       }
     }
     const float w[3] = {fl.sep[0], fl.ali[0], fl.coh[0]};
-    f3 x[3], u[3];
+    f3 x[3], xL[3], u[3], uL[3];
     const uint32_t cnt[3] = {cSep, cAli, cCoh};
     x[0] = cSep ? div3(sSep, (float)cSep) : sSep;
     x[1] = cAli ? sub3(div3(sAli, (float)cAli), a.fwd) : sAli;
     x[2] = cCoh ? sub3(div3(sCoh, (float)cCoh), a.pos) : sCoh;
-    f3 steer = mk3(0.f, 0.f, 0.f);
+    xL[0] = cSep ? div3(cpSep.value(), (float)cSep) : sSep;
+    xL[1] = cAli ? div3(cpAli.value(), (float)cAli) : sAli;
+    xL[2] = cCoh ? div3(cpCoh.value(), (float)cCoh) : sCoh;
+    f3 steer = mk3(0.f, 0.f, 0.f), steerL = mk3(0.f, 0.f, 0.f);
 #pragma unroll
     for (int b = 0; b < 3; ++b) {
       u[b] = cnt[b] ? normalize3(x[b]) : x[b];
-      if (w[b] != 0.0f) steer = add3(mul3(u[b], w[b]), steer);
+      uL[b] = cnt[b] ? normalize3(xL[b]) : xL[b];
+      if (w[b] != 0.0f) {
+        steer = add3(mul3(u[b], w[b]), steer);
+        steerL = add3(mul3(uL[b], w[b]), steerL);
+      }
     }
-    if (fl.numObstacles && fl.obsW != 0.0f) steer = obstacleSteer(a, fl, A.obstacles, A.obsMask, steer);
+    if (fl.numObstacles && fl.obsW != 0.0f) {
+      steer = obstacleSteer(a, fl, A.obstacles, A.obsMask, steer);
+      steerL = obstacleSteer(a, fl, A.obstacles, A.obsMask, steerL);
+    }
 
     f3 gSteer = mk3(0.f, 0.f, 0.f);
     f3 selfP = xyz(gOp), selfF = mk3(0.f, 0.f, 0.f), selfA = xyz(gOa);
@@ -152,7 +194,7 @@ __global__ void __launch_bounds__(kAdjointThreads) adjointStepKernel(AdjointStep
       if (!(speed > s0) && !(steer.x == 0.0f && steer.y == 0.0f && steer.z == 0.0f)) {
         br |= kBrLow;
         const float range = speed / s0;
-        cosine = 1.0f + ((-1.0f - 1.0f) * powf(range, 20.0f));
+        cosine = 1.0f + ((-1.0f - 1.0f) * pow20f(range));
         const float srcLen = len3(steer);
         if (srcLen != 0.0f && !(dot3(div3(steer, srcLen), fwd) >= cosine)) br |= kBrLimited;
         adjusted = vecLimitDeviationAngle(steer, cosine, fwd);
@@ -166,9 +208,19 @@ __global__ void __launch_bounds__(kAdjointThreads) adjointStepKernel(AdjointStep
         alpha = clampf(clampf(9.0f * dt, 0.15f, 0.4f), 0.0f, 1.0f);
         smoothed = add3(smoothed, mul3(sub3(newAccel, smoothed), alpha));
       }
-      const f3 v = add3(mul3(fwd, speed), mul3(smoothed, dt));
-      if (!(len3(v) <= maxS)) br |= kBrClipV;
-      const f3 vT = truncateLength(v, maxS);
+      const f3 vF = add3(mul3(fwd, speed), mul3(smoothed, dt));
+      if (!(len3(vF) <= maxS)) br |= kBrClipV;
+
+      // The same integration from steerL, through the branches taken above:
+      // the point the adjoint is linearised at.
+      if ((br & kBrLow) && (br & kBrLimited)) adjusted = limitedDeviation(steerL, cosine, fwd);
+      else adjusted = steerL;
+      const f3 clippedL = (br & kBrClipF) ? mul3(adjusted, maxF / len3(adjusted)) : adjusted;
+      f3 smoothedL = xyz(a4);
+      if (dt > 0.0f) smoothedL = add3(smoothedL, mul3(sub3(div3(clippedL, mass), smoothedL), alpha));
+      const f3 v = add3(mul3(fwd, speed), mul3(smoothedL, dt));
+      const f3 vT = (br & kBrClipV) ? mul3(v, maxS / len3(v)) : v;
+      steer = steerL;
 
       // --- adjoint of the integration --------------------------------------
       const float lvT = len3(vT);
@@ -207,7 +259,7 @@ __global__ void __launch_bounds__(kAdjointThreads) adjointStepKernel(AdjointStep
         gSrc = add3(gSrc, mul3(fwd, gk));
         gF = add3(gF, mul3(steer, gk));
         if (pd > 0.0f) gC += gPd * (-cosine / pd);
-        selfS += gC * (-40.0f * powf(range, 19.0f) / s0);
+        selfS += gC * (-40.0f * pow19f(range) / s0);
         selfF = add3(selfF, gF);
         gSteer = gSrc;
       }
@@ -219,8 +271,8 @@ __global__ void __launch_bounds__(kAdjointThreads) adjointStepKernel(AdjointStep
     for (int b = 0; b < 3; ++b) {
       gx[b] = mk3(0.f, 0.f, 0.f);
       if (!cnt[b]) continue;
-      gw[b] = dot3(gSteer, u[b]);
-      gx[b] = normalizeBar(x[b], mul3(gSteer, w[b]));
+      gw[b] = dot3(gSteer, uL[b]);
+      gx[b] = normalizeBar(xL[b], mul3(gSteer, w[b]));
     }
     if (fl.numObstacles && fl.obsW != 0.0f) {
       const f3 g = mul3(gSteer, fl.obsW);
@@ -245,72 +297,171 @@ __global__ void __launch_bounds__(kAdjointThreads) adjointStepKernel(AdjointStep
     const f3 gSc = cCoh ? div3(gx[2], (float)cCoh) : gx[2];
     selfF = sub3(selfF, gx[1]);
     selfP = sub3(selfP, gx[2]);
-    const uint32_t any = mS | mA | mC;
-    for (uint32_t k = 0; k < n; ++k) {
-      if (!((any >> k) & 1u)) continue;
+    // Every list entry (i, k) with a contribution: the adjoint it sends to
+    // the agent j it lists, stored at the entry, and the entry into j's
+    // in-list.  The separation term's own share goes to selfP (in list order).
+    for (uint32_t m = mS | mA | mC; m; m &= m - 1u) {
+      const uint32_t k = (uint32_t)__ffs(m) - 1u;
       const uint32_t j = lst[1 + k];
-      const uint32_t tj = __ldg(&A.prev[j]);
       f3 gp = mk3(0.f, 0.f, 0.f);
       if ((mS >> k) & 1u) {
-        // -o / |o|^2 with Jacobian -(I / d2 - 2 o o^T / d2^2)
         const f3 other = neighborImage(a, __ldg(&A.posS[j]), fl);
         const f3 o = sub3(other, a.pos);
-        const float d2 = dot3(o, o);
-        const f3 go = mul3(sub3(div3(gSs, d2), mul3(o, 2.0f * dot3(o, gSs) / (d2 * d2))), -1.0f);
+        const f3 go = separationBar(o, dot3(o, o), gSs);
         gp = add3(gp, go);
         selfP = sub3(selfP, go);
       }
       if ((mC >> k) & 1u) gp = add3(gp, gSc);
-      if (((mS | mC) >> k) & 1u) atomicAdd3(&A.gInP[tj], gp, 0.0f);
-      if ((mA >> k) & 1u) atomicAdd3(&A.gInF[tj], gSa, 0.0f);
+      const f3 gf = ((mA >> k) & 1u) ? gSa : mk3(0.f, 0.f, 0.f);
+      const uint32_t e = i * A.entryStride + k;
+      A.contrib[2 * (size_t)e + 0] = make_float4(gp.x, gp.y, gp.z, gf.x);
+      A.contrib[2 * (size_t)e + 1] = make_float4(gf.y, gf.z, 0.0f, 0.0f);
+      const uint32_t q = atomicAdd(&A.inCount[j], 1u);
+      if (q < A.inCap) A.inbox[(size_t)j * A.inCap + q] = e;
+      else A.ovNext[e] = atomicExch(&A.ovHead[j], e);
     }
-    atomicAdd3(&A.gInP[self], selfP, 0.0f);
-    atomicAdd3(&A.gInF[self], selfF, selfS);
-    A.gInA[self] = make_float4(selfA.x, selfA.y, selfA.z, 0.0f);
+    A.selfP[i] = make_float4(selfP.x, selfP.y, selfP.z, 0.0f);
+    A.selfF[i] = make_float4(selfF.x, selfF.y, selfF.z, selfS);
+    if (self < A.n) A.gInA[self] = make_float4(selfA.x, selfA.y, selfA.z, 0.0f);
+
+    const uint32_t id = __ldg(&A.idS[i]);
+    double* acc = A.accW + 3 * (size_t)id;
+    acc[0] += (double)gw[0];
+    acc[1] += (double)gw[1];
+    acc[2] += (double)gw[2];
 
     if (A.exportFlags) {
-      const uint32_t id = __ldg(&A.idS[i]);
       reinterpret_cast<uint4*>(A.exportFlags)[id] = make_uint4(br, mS, mA, mC);
       uint32_t* row = A.exportLists + (size_t)id * A.listStride;
       row[0] = n;
       for (uint32_t k = 0; k < n; ++k) row[1 + k] = __ldg(&A.idS[lst[1 + k]]);
     }
+    if (A.exportState) {
+      A.exportState[3 * (size_t)id + 0] = p4;
+      A.exportState[3 * (size_t)id + 1] = w4;
+      A.exportState[3 * (size_t)id + 2] = a4;
+    }
   }
-  warpFlockSum3(A.gW, f, valid, (double)gw[0], (double)gw[1], (double)gw[2]);
+}
+
+// Adds in-list entry e's contribution (stored by its emitter) to this
+// agent's position and forward adjoints.
+__device__ __forceinline__ void addContribution(const float4 c0, const float4 c1, f3& tP, f3& tF) {
+  tP = add3(tP, xyz(c0));
+  tF = add3(tF, mk3(c0.w, c1.x, c1.y));
+}
+
+__global__ void __launch_bounds__(kAdjointThreads) adjointGatherKernel(AdjointStepArgs A) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= A.n) return;
+  const uint32_t cnt = A.inCount[j];
+  A.inCount[j] = 0u;  // clean for the next-earlier step
+  const float4 sp = A.selfP[j], sf = A.selfF[j];
+  f3 tP = xyz(sp), tF = xyz(sf);
+  if (cnt <= A.inCap && cnt <= kGatherCap) {
+    uint32_t buf[kGatherCap];
+    const uint32_t* box = A.inbox + (size_t)j * A.inCap;
+    for (uint32_t q = 0; q < cnt; ++q) buf[q] = box[q];
+    for (uint32_t q = 1; q < cnt; ++q) {  // insertion sort by entry code
+      const uint32_t v = buf[q];
+      uint32_t r = q;
+      while (r > 0 && buf[r - 1] > v) { buf[r] = buf[r - 1]; --r; }
+      buf[r] = v;
+    }
+    // four entries' loads in flight, their sums in entry order
+    for (uint32_t q = 0; q < cnt; q += 4) {
+      float4 c[4][2];
+#pragma unroll
+      for (uint32_t u = 0; u < 4; ++u)
+        if (q + u < cnt) {
+          c[u][0] = A.contrib[2 * (size_t)buf[q + u] + 0];
+          c[u][1] = A.contrib[2 * (size_t)buf[q + u] + 1];
+        }
+#pragma unroll
+      for (uint32_t u = 0; u < 4; ++u)
+        if (q + u < cnt) addContribution(c[u][0], c[u][1], tP, tF);
+    }
+  } else {
+    // ascending order by repeated selection over the inbox and the overflow list
+    const uint32_t head = A.ovHead[j];
+    A.ovHead[j] = kNoEntry;
+    const uint32_t* box = A.inbox + (size_t)j * A.inCap;
+    const uint32_t inBox = min(cnt, A.inCap);
+    uint32_t last = 0;
+    for (uint32_t q = 0; q < cnt; ++q) {
+      uint32_t best = kNoEntry;
+      for (uint32_t r = 0; r < inBox; ++r) {
+        const uint32_t e = box[r];
+        if ((q == 0 || e > last) && e < best) best = e;
+      }
+      for (uint32_t e = head; e != kNoEntry; e = A.ovNext[e])
+        if ((q == 0 || e > last) && e < best) best = e;
+      addContribution(A.contrib[2 * (size_t)best], A.contrib[2 * (size_t)best + 1], tP, tF);
+      last = best;
+    }
+  }
+  const uint32_t t = __ldg(&A.prev[j]);
+  if (t >= A.n) return;  // only a corrupted step leaves such a source slot
+  A.gInP[t] = make_float4(tP.x, tP.y, tP.z, 0.0f);
+  A.gInF[t] = make_float4(tF.x, tF.y, tF.z, sf.w);
+}
+
+// Per-flock sums of `width` doubles per item over flock f's items
+// [agentBase[f], agentBase[f+1]), in an order fixed by the sizes alone:
+// block (f, b) sums part b of the flock (kReduceParts equal parts; each
+// thread a fixed stride of items, then a fixed tree in shared memory), and
+// flockReducePartsKernel adds the parts in order.
+__global__ void __launch_bounds__(256) flockReduceKernel(FlockReduceArgs A) {
+  __shared__ double sh[3][256];
+  const uint32_t f = blockIdx.x, b = blockIdx.y;
+  const uint32_t a0 = __ldg(&A.agentBase[f]), a1 = __ldg(&A.agentBase[f + 1]);
+  const uint32_t part = (a1 - a0 + kReduceParts - 1) / kReduceParts;
+  const uint32_t p0 = a0 + b * part, p1 = min(a1, p0 + part);
+  const uint32_t w = A.width;
+  double s[3] = {0.0, 0.0, 0.0};
+  for (uint32_t id = p0 + threadIdx.x; id < p1; id += 256u)
+    for (uint32_t c = 0; c < w; ++c) s[c] += A.vals[(size_t)w * id + c];
+  for (int c = 0; c < 3; ++c) sh[c][threadIdx.x] = s[c];
+  __syncthreads();
+  for (uint32_t h = 128; h > 0; h >>= 1) {
+    if (threadIdx.x < h)
+      for (int c = 0; c < 3; ++c) sh[c][threadIdx.x] += sh[c][threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (uint32_t c = 0; c < w; ++c) A.partial[((size_t)f * kReduceParts + b) * w + c] = sh[c][0];
+}
+
+__global__ void __launch_bounds__(256) flockReducePartsKernel(FlockReduceArgs A) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= A.nflocks * A.width) return;
+  const uint32_t f = t / A.width, c = t - f * A.width;
+  double s = 0.0;
+  for (uint32_t b = 0; b < kReduceParts; ++b) s += A.partial[((size_t)f * kReduceParts + b) * A.width + c];
+  A.out[t] = s;
 }
 
 // Loss = sum over flocks of the mean squared minimum-image distance between
-// final and target positions (FP64), per flock into lossPerFlock, and the
-// unscaled terminal position adjoint 2 d / n_f (canonical order).
+// final and target positions (FP64): each agent's term into lossTerm (by
+// canonical slot; flocks own fixed slot ranges), reduced per flock in a fixed
+// order by flockReduceKernel; and the unscaled terminal position adjoint
+// 2 d / n_f (canonical order).
 __global__ void __launch_bounds__(256) lossKernel(LossArgs A) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool valid = i < A.n;
-  uint32_t f = 0;
-  double l = 0.0;
-  if (valid) {
-    f = A.nflocks == 1 ? 0u : flockOfSlot(A.agentBase, A.nflocks, i);
-    const FlockDev& fl = A.flocks[f];
-    const float4 p = __ldg(&A.posA[i]);
-    const float4 t = __ldg(&A.target[__ldg(&A.idA[i])]);
-    const double L = fl.L, hL = 0.5 * (double)fl.L;
-    double d[3] = {(double)p.x - (double)t.x, (double)p.y - (double)t.y, (double)p.z - (double)t.z};
+  if (i >= A.n) return;
+  const uint32_t f = A.nflocks == 1 ? 0u : flockOfSlot(A.agentBase, A.nflocks, i);
+  const FlockDev& fl = A.flocks[f];
+  const float4 p = __ldg(&A.posA[i]);
+  const float4 t = __ldg(&A.target[__ldg(&A.idA[i])]);
+  const double L = fl.L, hL = 0.5 * (double)fl.L;
+  double d[3] = {(double)p.x - (double)t.x, (double)p.y - (double)t.y, (double)p.z - (double)t.z};
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      if (d[c] > hL) d[c] -= L; else if (d[c] < -hL) d[c] += L;
-    }
-    const double inv = 1.0 / (double)fl.n;
-    l = (d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) * inv;
-    A.gT[i] = make_float4((float)(2.0 * d[0] * inv), (float)(2.0 * d[1] * inv), (float)(2.0 * d[2] * inv), 0.0f);
+  for (int c = 0; c < 3; ++c) {
+    if (d[c] > hL) d[c] -= L; else if (d[c] < -hL) d[c] += L;
   }
-  const uint32_t full = 0xFFFFFFFFu;
-  const uint32_t f0 = __shfl_sync(full, f, 0);
-  if (__all_sync(full, !valid || f == f0)) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) l += __shfl_down_sync(full, l, o);
-    if ((threadIdx.x & 31u) == 0u) atomicAdd(&A.lossPerFlock[f0], l);
-  } else if (valid) {
-    atomicAdd(&A.lossPerFlock[f], l);
-  }
+  const double inv = 1.0 / (double)fl.n;
+  A.lossTerm[i] = (d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) * inv;
+  A.gT[i] = make_float4((float)(2.0 * d[0] * inv), (float)(2.0 * d[1] * inv), (float)(2.0 * d[2] * inv), 0.0f);
 }
 
 // Terminal adjoint of the last step's output (its sorted order = the final
@@ -353,9 +504,24 @@ __global__ void __launch_bounds__(256) adjointOutKernel(OutArgs A) {
   }
 }
 
+
 cudaError_t launchAdjointStep(const AdjointStepArgs& A, cudaStream_t st) {
   if (A.n == 0) return cudaSuccess;
-  adjointStepKernel<<<(A.n + kAdjointThreads - 1) / kAdjointThreads, kAdjointThreads, 0, st>>>(A);
+  if (A.entryStride == 0 || A.entryStride > 32) return cudaErrorInvalidValue;
+  const uint32_t blocks = (A.n + kAdjointThreads - 1) / kAdjointThreads;
+  adjointStepKernel<<<blocks, kAdjointThreads, 0, st>>>(A);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return err;
+  adjointGatherKernel<<<blocks, kAdjointThreads, 0, st>>>(A);
+  return cudaGetLastError();
+}
+cudaError_t launchFlockReduce(const FlockReduceArgs& A, cudaStream_t st) {
+  if (A.nflocks == 0) return cudaSuccess;
+  if (A.width < 1 || A.width > 3) return cudaErrorInvalidValue;
+  flockReduceKernel<<<dim3(A.nflocks, kReduceParts), 256, 0, st>>>(A);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return err;
+  flockReducePartsKernel<<<(A.nflocks * A.width + 255) / 256, 256, 0, st>>>(A);
   return cudaGetLastError();
 }
 cudaError_t launchLoss(const LossArgs& A, cudaStream_t st) {

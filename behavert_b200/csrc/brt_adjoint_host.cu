@@ -47,6 +47,13 @@ struct AdjointState {
   double* loss = nullptr;
   float* scale = nullptr;
   uint32_t *expLists = nullptr, *expFlags = nullptr;
+  float4* expState = nullptr;  // per step: input pos, fwd, acc by agent id
+  // emit -> gather hand-over of one reverse step, and the weight sums
+  float4 *contrib = nullptr, *selfP = nullptr, *selfF = nullptr;
+  double* partial = nullptr;  // per-flock reduction parts
+  uint32_t *inCount = nullptr, *inbox = nullptr, *ovHead = nullptr, *ovNext = nullptr;
+  uint32_t inCap = 0;
+  double* accW = nullptr;
   // graphs: (kind, T, k, dt bits, params version, variant bits)
   std::map<std::tuple<int, uint32_t, uint32_t, uint32_t, uint32_t, uint32_t>, cudaGraphExec_t> graphs;
 };
@@ -110,6 +117,18 @@ int ensureCapacity(brt_engine* e, uint32_t nck, uint32_t k, uint32_t T) {
     if ((rc = adjAlloc(a, &a->finAcc, n))) return rc;
     if ((rc = adjAlloc(a, &a->finId, n))) return rc;
     if ((rc = adjAlloc(a, &a->finFeat, n * e->Fs))) return rc;
+    if ((rc = adjAlloc(a, &a->contrib, 2 * n * (size_t)e->Mmax))) return rc;
+    if ((rc = adjAlloc(a, &a->selfP, n))) return rc;
+    if ((rc = adjAlloc(a, &a->selfF, n))) return rc;
+    if ((rc = adjAlloc(a, &a->partial, 3 * (size_t)kReduceParts * e->nflocks))) return rc;
+    // in-degree is about the list length: room for twice maxNeighbors, the
+    // rest overflows into a linked list
+    a->inCap = std::min(64u, 2u * e->Mmax);
+    if ((rc = adjAlloc(a, &a->inCount, n))) return rc;
+    if ((rc = adjAlloc(a, &a->inbox, n * (size_t)a->inCap))) return rc;
+    if ((rc = adjAlloc(a, &a->ovHead, n))) return rc;
+    if ((rc = adjAlloc(a, &a->ovNext, n * (size_t)e->Mmax))) return rc;
+    if ((rc = adjAlloc(a, &a->accW, 3 * n))) return rc;
     BRT_CUDA_TRY(cudaMemsetAsync(a->target, 0, n * 16, e->stream));
   }
   auto regrow = [&](auto** p, size_t count) -> int {
@@ -136,7 +155,9 @@ int ensureCapacity(brt_engine* e, uint32_t nck, uint32_t k, uint32_t T) {
   }
   if (e->adjointExport && T > a->capExport) {
     BRT_CUDA_TRY(cudaStreamSynchronize(e->stream));
-    if ((rc = regrow(&a->expLists, n * T * e->listStride)) || (rc = regrow(&a->expFlags, n * T * 4))) return rc;
+    if ((rc = regrow(&a->expLists, n * T * e->listStride)) || (rc = regrow(&a->expFlags, n * T * 4)) ||
+        (rc = regrow(&a->expState, n * T * 3)))
+      return rc;
     a->capExport = T;
     changed = true;
   }
@@ -171,13 +192,16 @@ int enqueueForward(brt_engine* e) {
   }
   if ((rc = copyState(e, a->finPos, a->finFwd, a->finAcc, a->finId, e->posA, e->fwdA, e->accA, e->idA))) return rc;
   if (e->Fs) BRT_CUDA_TRY(cudaMemcpyAsync(a->finFeat, e->featA, n * e->Fs * 4, cudaMemcpyDeviceToDevice, e->stream));
-  BRT_CUDA_TRY(cudaMemsetAsync(a->loss, 0, 8 * (size_t)e->nflocks, e->stream));
   LossArgs L;
   std::memset(&L, 0, sizeof(L));
   L.posA = e->posA; L.idA = e->idA; L.target = a->target;
   L.flocks = e->flocks; L.agentBase = e->agentBase; L.nflocks = e->nflocks; L.n = e->N;
-  L.lossPerFlock = a->loss; L.gT = a->gT;
+  L.lossTerm = a->accW; L.gT = a->gT;  // accW is free until the backward
   BRT_CUDA_TRY(launchLoss(L, e->stream));
+  FlockReduceArgs R;
+  R.vals = a->accW; R.width = 1; R.agentBase = e->agentBase; R.nflocks = e->nflocks; R.out = a->loss;
+  R.partial = a->partial;
+  BRT_CUDA_TRY(launchFlockReduce(R, e->stream));
   return BRT_OK;
 }
 
@@ -223,8 +247,9 @@ int enqueueBackward(brt_engine* e, uint32_t variant) {
   int cur = 0;
   S.gP = a->g[cur][0]; S.gF = a->g[cur][1]; S.gA = a->g[cur][2];
   BRT_CUDA_TRY(launchAdjointSeed(S, e->stream));
-  for (int c = 0; c < 3; ++c) BRT_CUDA_TRY(cudaMemsetAsync(a->g[1][c], 0, n * 16, e->stream));
-  BRT_CUDA_TRY(cudaMemsetAsync(a->gW, 0, 24 * (size_t)e->nflocks, e->stream));
+  BRT_CUDA_TRY(cudaMemsetAsync(a->accW, 0, 24 * n, e->stream));
+  BRT_CUDA_TRY(cudaMemsetAsync(a->inCount, 0, 4 * n, e->stream));     // empty in-lists
+  BRT_CUDA_TRY(cudaMemsetAsync(a->ovHead, 0xFF, 4 * n, e->stream));    // kNoEntry
   for (int c = (int)a->nck - 1; c >= 0; --c) {
     if ((rc = copyState(e, e->posA, e->fwdA, e->accA, e->idA, a->ckPos + c * n, a->ckFwd + c * n, a->ckAcc + c * n,
                         a->ckId + c * n)))
@@ -241,16 +266,24 @@ int enqueueBackward(brt_engine* e, uint32_t variant) {
       R.nflocks = e->nflocks; R.n = e->N; R.dt = a->dt;
       R.gOutP = a->g[cur][0]; R.gOutF = a->g[cur][1]; R.gOutA = a->g[cur][2];
       R.gInP = a->g[cur ^ 1][0]; R.gInF = a->g[cur ^ 1][1]; R.gInA = a->g[cur ^ 1][2];
-      R.gW = a->gW;
+      R.contrib = a->contrib; R.selfP = a->selfP; R.selfF = a->selfF;
+      R.inCount = a->inCount; R.inbox = a->inbox; R.inCap = a->inCap;
+      R.ovHead = a->ovHead; R.ovNext = a->ovNext; R.entryStride = e->Mmax;
+      R.accW = a->accW;
       if (e->adjointExport && a->expLists) {
         const size_t t = (size_t)c * a->k + s;
         R.exportLists = a->expLists + t * n * e->listStride;
         R.exportFlags = a->expFlags + t * n * 4;
+        R.exportState = a->expState + t * n * 3;
       }
       BRT_CUDA_TRY(launchAdjointStep(R, e->stream));
       cur ^= 1;
     }
   }
+  FlockReduceArgs W;
+  W.vals = a->accW; W.width = 3; W.agentBase = e->agentBase; W.nflocks = e->nflocks; W.out = a->gW;
+  W.partial = a->partial;
+  BRT_CUDA_TRY(launchFlockReduce(W, e->stream));
   OutArgs O;
   std::memset(&O, 0, sizeof(O));
   O.gP = a->g[cur][0]; O.gF = a->g[cur][1]; O.gA = a->g[cur][2];
@@ -402,6 +435,27 @@ int brt_adjoint_get_tape(brt_engine* e, uint32_t* lists_by_id, uint32_t* flags_b
   if (lists_by_id)
     BRT_CUDA_TRY(cudaMemcpyAsync(lists_by_id, a->expLists, n * a->T * e->listStride * 4, kindOut(where), e->stream));
   if (flags_by_id) BRT_CUDA_TRY(cudaMemcpyAsync(flags_by_id, a->expFlags, n * a->T * 16, kindOut(where), e->stream));
+  if (where == BRT_MEM_HOST) return engineSyncAndCheck(e);
+  return BRT_OK;
+}
+
+int brt_adjoint_get_tape_states(brt_engine* e, float* pos4, float* fwd4, float* acc4, int where) {
+  if (!e) return BRT_ERR_ARG;
+  AdjointState* a = e->adj;
+  if (!e->adjointExport || !a || !a->expState || a->capExport < a->T) {
+    setLastError("brt_adjoint_get_tape_states: enable option adjoint_export before brt_adjoint_forward");
+    return BRT_ERR_STATE;
+  }
+  if (where != BRT_MEM_HOST && where != BRT_MEM_DEVICE) return BRT_ERR_ARG;
+  DeviceGuard guard(e->device);
+  const size_t n = e->N;
+  float* dst[3] = {pos4, fwd4, acc4};
+  for (int c = 0; c < 3; ++c) {
+    if (!dst[c]) continue;
+    // the tape holds (pos, fwd, acc) interleaved per agent; copy one of three
+    BRT_CUDA_TRY(cudaMemcpy2DAsync(dst[c], 16, (const char*)a->expState + 16 * c, 48, 16, n * a->T, kindOut(where),
+                                   e->stream));
+  }
   if (where == BRT_MEM_HOST) return engineSyncAndCheck(e);
   return BRT_OK;
 }

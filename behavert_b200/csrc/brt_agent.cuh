@@ -38,9 +38,8 @@ __device__ __forceinline__ uint32_t buildNeighborList(uint32_t self, f3 p, const
         const float sz = imageShift(gz, oz, fl.G, fl.L);
         const uint32_t h = fl.cellBase + ((uint32_t)cz * fl.G + (uint32_t)cy) * fl.G + (uint32_t)cx;
         const uint32_t start = __ldg(&cellStart[h]);
-        if (start == kEmpty) continue;
         uint32_t stop = __ldg(&cellEnd[h]);
-        if (stop <= start) continue;
+        if (!usableRange(fl, start, stop)) continue;
         if (fl.maxPerCell && stop - start > fl.maxPerCell) stop = start + fl.maxPerCell;
         for (uint32_t j = start; j < stop; ++j) {
           if (j == self) continue;
@@ -99,9 +98,8 @@ __device__ __forceinline__ uint32_t scanNeighborsFlat(uint32_t self, f3 p, const
         const int cx = wrapCoord(gx + ox, fl.G), cy = wrapCoord(gy + oy, fl.G), cz = wrapCoord(gz + oz, fl.G);
         const uint32_t h = fl.cellBase + ((uint32_t)cz * fl.G + (uint32_t)cy) * fl.G + (uint32_t)cx;
         const uint32_t start = __ldg(&cellStart[h]);
-        if (start == kEmpty) continue;
         uint32_t end = __ldg(&cellEnd[h]);
-        if (end <= start) continue;
+        if (!usableRange(fl, start, end)) continue;
         if (fl.maxPerCell && end - start > fl.maxPerCell) end = start + fl.maxPerCell;
         j = start;
         stop = end;
@@ -181,7 +179,7 @@ __device__ __forceinline__ uint32_t scanNeighborsPipelined(uint32_t self, f3 p, 
       for (int k = 0; k < 3; ++k) {
         const uint32_t start = st[k];
         uint32_t stop = en[k];
-        if (start == kEmpty || stop <= start) continue;
+        if (!usableRange(fl, start, stop)) continue;
         if (CULL && bxy + (k == 0 ? lo2[2] : (k == 2 ? hi2[2] : 0.0f)) > cullThr) continue;
         if (fl.maxPerCell && stop - start > fl.maxPerCell) stop = start + fl.maxPerCell;
         const float sz = imageShift(gz, k - 1, fl.G, fl.L);
@@ -297,7 +295,7 @@ __device__ __forceinline__ uint32_t scanNeighborsCooperative(bool active, uint32
       const int cx = wrapCoord(gx + ox, G), cy = wrapCoord(gy + oy, G), cz = wrapCoord(gz + oz, G);
       const uint32_t h = fl.cellBase + ((uint32_t)cz * G + (uint32_t)cy) * G + (uint32_t)cx;
       const uint32_t st = __ldg(&cellStart[h]), en = __ldg(&cellEnd[h]);
-      if (st != kEmpty && en > st) {
+      if (usableRange(fl, st, en)) {
         segStart = st;
         segLen = en - st;
         if (fl.maxPerCell && segLen > fl.maxPerCell) segLen = fl.maxPerCell;
@@ -717,11 +715,26 @@ __device__ __forceinline__ f3 vecLimitDeviationAngle(f3 source, float cosineOfCo
   const f3 c1 = mul3(unitPerp, perpDist);
   return mul3(add3(c0, c1), sourceLength);
 }
+// range^20 of adjustRawSteeringForce's low-speed branch, where the reference
+// calls powf(range, 20) (Core/common_resources.cu:251).  Evaluated in double
+// by repeated squaring (x^16 * x^4) and rounded to float once.  The CPU
+// oracle runs the same operation sequence, so host and device agree bit for
+// bit, and the result is the correctly rounded x^20 unless the exact value
+// lies within about 6e-16 (relative) of a float rounding boundary.
+__host__ __device__ __forceinline__ float pow20f(float x) {
+  const double d = (double)x, d2 = d * d, d4 = d2 * d2, d8 = d4 * d4, d16 = d8 * d8;
+  return (float)(d16 * d4);
+}
+// x^19 in the same way (the derivative of pow20f in the adjoint).
+__host__ __device__ __forceinline__ float pow19f(float x) {
+  const double d = (double)x, d2 = d * d, d4 = d2 * d2, d8 = d4 * d4, d16 = d8 * d8;
+  return (float)((d16 * d2) * d);
+}
 __device__ __forceinline__ f3 adjustRawSteeringForce(f3 force, float speed, f3 forward, float maxSpeed) {
   const float maxAdjustedSpeed = 0.2f * maxSpeed;
   if ((speed > maxAdjustedSpeed) || (force.x == 0.0f && force.y == 0.0f && force.z == 0.0f)) return force;
   const float range = speed / maxAdjustedSpeed;
-  const float p = powf(range, 20.0f);
+  const float p = pow20f(range);
   const float cosine = 1.0f + ((-1.0f - 1.0f) * p);
   return vecLimitDeviationAngle(force, cosine, forward);
 }

@@ -159,6 +159,23 @@ using namespace brt;
 
 namespace {
 
+__global__ void iotaKernel(uint32_t* a, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = i;
+}
+cudaError_t launchIota(uint32_t* a, uint32_t n, cudaStream_t st) {
+  iotaKernel<<<(n + 255) / 256, 256, 0, st>>>(a, n);
+  return cudaGetLastError();
+}
+
+// The re-sort's state as after creation: no previous order, empty mover
+// lists (kNoMover heads), zero counters and look-back words.
+cudaError_t resetResort(brt_engine* e) {
+  cudaError_t err = cudaMemsetAsync(e->resortMem, 0, e->resortWords * 4, e->stream);
+  if (err == cudaSuccess && e->C) err = cudaMemsetAsync(e->rsHead, 0xFF, (size_t)e->C * 4, e->stream);
+  return err;
+}
+
 void freeAll(brt_engine* e) {
   freeAdjoint(e->adj);
   e->adj = nullptr;
@@ -249,6 +266,7 @@ ResortArgs resortArgs(brt_engine* e) {
   A.stepCounter = e->stepCounter;
   A.out = e->pairs[e->plan.passes & 1];
   A.errWord = e->errWord;
+  A.wait = e->wait;
   return A;
 }
 
@@ -383,6 +401,7 @@ int checkDeviceError(brt_engine* e, bool clear) {
   uint32_t w = 0;
   BRT_CUDA_TRY(cudaMemcpyAsync(&w, e->errWord, 4, cudaMemcpyDeviceToHost, e->stream));
   BRT_CUDA_TRY(cudaStreamSynchronize(e->stream));
+  if (w) e->stateLost = true;
   if (w && clear) BRT_CUDA_TRY(cudaMemsetAsync(e->errWord, 0, 4, e->stream));
   if (w & kDevErrLookback) { setLastError("onesweep look-back spin limit reached"); return BRT_ERR_TIMEOUT; }
   if (w) { setLastError("device-side pipeline check failed"); return BRT_ERR_STATE; }
@@ -552,6 +571,7 @@ int brt_engine_create(const brt_params* flocks, uint32_t num_flocks, int device,
   size_t rsWordsTotal = 0;
   for (size_t w : rsSizes) rsWordsTotal += words4(w);
   if (!rc && cudaMalloc(&e->resortMem, rsWordsTotal * 4) != cudaSuccess) { setLastError("re-sort allocation failed"); rc = BRT_ERR_CUDA; }
+  e->resortWords = rsWordsTotal;
   if (rc) { freeAll(e); delete e; return rc; }
   {
     uint32_t** rsPtrs[11] = {&e->rsNewKey, &e->rsPrefix, &e->rsNext, &e->rsBlockStay, &e->rsCount, &e->rsHead,
@@ -571,8 +591,11 @@ int brt_engine_create(const brt_params* flocks, uint32_t num_flocks, int device,
     BRT_CUDA_TRY(cudaStreamSynchronize(st));
   }
   BRT_CUDA_TRY(cudaMemsetAsync(e->sortMem, 0, sortBytes, st));
-  BRT_CUDA_TRY(cudaMemsetAsync(e->resortMem, 0, rsWordsTotal * 4, st));
-  if (e->C) BRT_CUDA_TRY(cudaMemsetAsync(e->rsHead, 0xFF, (size_t)e->C * 4, st));  // kNoMover
+  BRT_CUDA_TRY(resetResort(e));
+  if (n) {
+    BRT_CUDA_TRY(cudaMemsetAsync(e->pairs[0], 0, n * 8, st));
+    BRT_CUDA_TRY(cudaMemsetAsync(e->pairs[1], 0, n * 8, st));
+  }
   BRT_CUDA_TRY(cudaMemsetAsync(e->errWord, 0, 4, st));
   BRT_CUDA_TRY(cudaMemsetAsync(e->stepCounter, 0, 4, st));
   if (n) {
@@ -700,10 +723,19 @@ int brt_engine_set_option(brt_engine* e, const char* key, int64_t value) {
     e->adjointGraphs = value != 0;
   } else if (k == "adjoint_export") {
     e->adjointExport = value != 0;
+  } else if (k == "lookback_spin_limit") {
+    if (value < 0 || value > 0x7FFFFFFFll) { setLastError("lookback_spin_limit must be in [0, 2^31)"); return BRT_ERR_ARG; }
+    e->wait.spinLimit = (uint32_t)value;
+    e->plan.wait = e->wait;
+  } else if (k == "lookback_stall_tile") {
+    if (value < -1 || value > 0x7FFFFFFFll) { setLastError("lookback_stall_tile must be -1 or a tile index"); return BRT_ERR_ARG; }
+    e->wait.stallTile = value < 0 ? kNoStallTile : (uint32_t)value;
+    e->plan.wait = e->wait;
   } else if (k == "sort_digit_bits") {
     if (value < 4 || value > 9) { setLastError("sort_digit_bits must be in [4, 9]"); return BRT_ERR_ARG; }
     BRT_CUDA_TRY(cudaStreamSynchronize(e->stream));
     SortPlan plan = makeSortPlan(e->N, e->plan.bits, (uint32_t)value);
+    plan.wait = e->wait;
     const size_t bytes = sortScratchBytes(plan, false);
     void* mem = nullptr;
     BRT_CUDA_TRY(cudaMalloc(&mem, bytes));
@@ -748,6 +780,7 @@ int brt_engine_check_device_error(brt_engine* e, uint32_t* word) {
   DeviceGuard guard(e->device);
   BRT_CUDA_TRY(cudaMemcpyAsync(word, e->errWord, 4, cudaMemcpyDeviceToHost, e->stream));
   BRT_CUDA_TRY(cudaStreamSynchronize(e->stream));
+  if (*word) e->stateLost = true;
   BRT_CUDA_TRY(cudaMemsetAsync(e->errWord, 0, 4, e->stream));
   BRT_CUDA_TRY(cudaStreamSynchronize(e->stream));
   return BRT_OK;
@@ -761,6 +794,16 @@ int brt_set_state(brt_engine* e, const float* pos4, const float* fwd4, const flo
   DeviceGuard guard(e->device);
   cudaStream_t st = e->stream;
   const size_t n = e->N;
+  if (e->stateLost && n) {
+    // After a failed device check the slot order may hold an agent twice:
+    // start again from the identity order (registered arrays included,
+    // whose contents the caller sets again) and a clean re-sort state.
+    BRT_CUDA_TRY(launchIota(e->idA, e->N, st));
+    if (e->userIds.a) BRT_CUDA_TRY(launchIota(e->userIds.a, e->N, st));
+    // a garbled order can leave mover lists of cells that end up empty
+    BRT_CUDA_TRY(resetResort(e));
+    e->stateLost = false;
+  }
   auto stage4 = [&](const float* src) -> const float4* {
     if (where == BRT_MEM_DEVICE) return (const float4*)src;
     cudaMemcpyAsync(e->stage4, src, n * 16, cudaMemcpyHostToDevice, st);

@@ -53,7 +53,12 @@ struct brt_engine {
   uint32_t* errWord = nullptr;
   // incremental re-sort (brt_resort.cu); option "incremental_sort"
   bool resortOn = true;
+  brt::LookbackWait wait;  // bound of the look-back waits (copied into plan.wait)
+  // A device check failed (a wait ran out, a pipeline invariant broke): the
+  // slot order may no longer be a permutation.  brt_set_state rebuilds it.
+  bool stateLost = false;
   uint32_t* resortMem = nullptr;   // one allocation carved into the arrays below
+  size_t resortWords = 0;          // its size in words
   uint32_t *rsNewKey = nullptr, *rsPrefix = nullptr, *rsNext = nullptr, *rsBlockStay = nullptr;
   uint32_t *rsCount = nullptr, *rsHead = nullptr, *rsNewStart = nullptr, *rsTiles = nullptr;
   uint32_t *rsCounter = nullptr, *rsWords = nullptr, *rsStayBase = nullptr;

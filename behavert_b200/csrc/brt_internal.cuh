@@ -125,6 +125,15 @@ __device__ __forceinline__ void stRelaxed(uint32_t* p, uint32_t v) {
 }
 
 // Flock of a sorted slot (flocks own contiguous slot ranges).
+// A cell's sorted-slot range [start, end) as the neighbour scans use it:
+// empty unless it lies inside the flock's slots.  A well-formed step always
+// passes; after a corrupted one (a look-back wait that ran out, reported
+// through the device error word) the words can be stale or torn, and a scan
+// must never follow them out of the arrays.
+__device__ __forceinline__ bool usableRange(const FlockDev& fl, uint32_t start, uint32_t end) {
+  return start != kEmpty && end > start && start >= fl.agentBase && end <= fl.agentBase + fl.n;
+}
+
 __device__ __forceinline__ uint32_t flockOfSlot(const uint32_t* __restrict__ agentBase, uint32_t nflocks, uint32_t slot) {
   uint32_t lo = 0, hi = nflocks;  // agentBase has nflocks+1 entries
   while (hi - lo > 1) {
@@ -136,9 +145,24 @@ __device__ __forceinline__ uint32_t flockOfSlot(const uint32_t* __restrict__ age
 
 // ---------------------------------------------------------------------------
 // Sort plan shared by the engine and the standalone entry point.
+// Bound of every decoupled look-back wait (onesweep passes, the incremental
+// re-sort's cell scan): polls of a predecessor's unpublished status word
+// before the tile gives up, records kDevErrLookback and goes on (the host
+// then reports BRT_ERR_TIMEOUT).  About a second at the default.
+// stallTile names one tile whose look-back polls as if its predecessor never
+// published (a status word that nothing sets), so that tests can make a wait
+// run out on purpose; kNoStallTile in normal use.
+constexpr uint32_t kDefaultSpinLimit = 1u << 21;
+constexpr uint32_t kNoStallTile = 0xFFFFFFFFu;
+struct LookbackWait {
+  uint32_t spinLimit = kDefaultSpinLimit;
+  uint32_t stallTile = kNoStallTile;
+};
+
 struct SortPlan {
   uint32_t n = 0, bits = 0, passes = 0, digitBits = 0, bins = 0, tiles = 0;
   uint32_t shift[4] = {0, 0, 0, 0};
+  LookbackWait wait;
 };
 constexpr uint32_t kSortThreads = 256;
 // Items a thread ranks per tile: 16, or 8 for 9-bit digits, whose per-warp

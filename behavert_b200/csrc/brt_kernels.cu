@@ -349,7 +349,8 @@ __global__ void gatherWordsKernel(const uint32_t* __restrict__ src, const uint32
   const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (size_t)n * words) return;
   const size_t i = t / words, k = t - i * words;
-  dst[t] = src[(size_t)__ldg(&index[i * stride]) * words + k];
+  const uint32_t from = __ldg(&index[i * stride]);
+  dst[t] = from < n ? src[(size_t)from * words + k] : 0u;  // a corrupted step's stale index reads nothing
 }
 __global__ void scatterWordsKernel(const uint32_t* __restrict__ src, const uint32_t* __restrict__ index,
                                    uint32_t* __restrict__ dst, uint32_t words, uint32_t n) {

@@ -116,6 +116,7 @@ struct ResortArgs {
   uint32_t* stepCounter;         // random-stream step (advanced here when the hash does not run)
   uint2* out;                    // sorted pairs: the sort's final buffer
   uint32_t* errWord;
+  LookbackWait wait;             // bound of the cell scan's look-back
 };
 uint32_t resortBlocks(uint32_t n);
 uint32_t resortCellTiles(uint32_t numCells);
@@ -133,18 +134,44 @@ struct AdjointStepArgs {
   const uint2* obsMask;
   uint32_t nflocks, n;
   float dt;
-  float4* gOutP; float4* gOutF; float4* gOutA;                   // output adjoint by sorted slot (zeroed)
+  const float4* gOutP; const float4* gOutF; const float4* gOutA; // output adjoint by sorted slot
   float4* gInP; float4* gInF; float4* gInA;                      // input adjoint by canonical slot
-  double* gW;                                                    // nflocks * 3, accumulated
+  // Emit -> gather hand-over of one step (sorted slots of this step):
+  float4* contrib;      // 2 per list entry e = i * entryStride + k: the position adjoint (xyz)
+                        // and forward adjoint (w, then xy) that agent i sends the agent it lists at k
+  float4* selfP;        // per slot: the agent's own position adjoint terms
+  float4* selfF;        // per slot: the agent's own forward adjoint terms (w: speed)
+  // In-lists (the transposed neighbour list of the step): agent j's entries
+  // e = i * entryStride + k (agent i lists j at position k) go to
+  // inbox[j * inCap + q] at q = atomicAdd(&inCount[j], 1); entries beyond
+  // inCap go to a linked overflow list (ovHead[j], ovNext[e]).  The gather
+  // resets inCount and ovHead for the next-earlier step.
+  uint32_t* inCount; uint32_t* inbox; uint32_t inCap;
+  uint32_t* ovHead; uint32_t* ovNext;
+  uint32_t entryStride; // list positions per slot in the entry code (maxNeighbors, <= 32)
+  double* accW;         // per agent id: the weight adjoint summed over the steps (3 doubles)
   uint32_t* exportLists;                                         // optional, by agent id
   uint32_t* exportFlags;                                         // optional, 4 words by agent id
+  float4* exportState;                                           // optional: pos, fwd, acc by agent id
+};
+constexpr uint32_t kNoEntry = 0xFFFFFFFFu;
+// Per-flock FP64 sums of per-item values (the weight adjoint, the loss), in
+// a fixed order: kReduceParts blocks per flock, each over a fixed part of the
+// flock's items, then the parts in order.
+constexpr uint32_t kReduceParts = 32;
+struct FlockReduceArgs {
+  const double* vals; uint32_t width;   // width (1..3) doubles per item
+  const uint32_t* agentBase;            // items of flock f: [agentBase[f], agentBase[f+1])
+  uint32_t nflocks;
+  double* partial;                      // nflocks * kReduceParts * width scratch
+  double* out;                          // nflocks * width, written
 };
 struct LossArgs {
   const float4* posA; const uint32_t* idA;    // final state, canonical order
   const float4* target;                       // by agent id
   const FlockDev* flocks; const uint32_t* agentBase;
   uint32_t nflocks, n;
-  double* lossPerFlock;                       // accumulated
+  double* lossTerm;                           // per canonical slot (reduced per flock afterwards)
   float4* gT;                                 // unscaled terminal position adjoint, canonical order
 };
 struct SeedArgs {
@@ -162,6 +189,7 @@ struct OutArgs {
   float4* outP; float4* outF; float4* outA; float4* outV;  // by agent id, each optional
 };
 cudaError_t launchAdjointStep(const AdjointStepArgs& A, cudaStream_t st);
+cudaError_t launchFlockReduce(const FlockReduceArgs& A, cudaStream_t st);
 cudaError_t launchLoss(const LossArgs& A, cudaStream_t st);
 cudaError_t launchAdjointSeed(const SeedArgs& A, cudaStream_t st);
 cudaError_t launchAdjointOut(const OutArgs& A, cudaStream_t st);

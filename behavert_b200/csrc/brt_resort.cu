@@ -47,7 +47,6 @@ constexpr uint32_t kLookAgg = 1u << 30;
 constexpr uint32_t kLookInc = 2u << 30;
 constexpr uint32_t kLookMask = 3u << 30;
 constexpr uint32_t kLookVal = (1u << 30) - 1u;
-constexpr uint32_t kLookSpinLimit = 1u << 21;
 
 // Stayers among slots [0, x) and [0, x].
 __device__ __forceinline__ uint32_t stayersBefore(const ResortArgs& A, uint32_t x) {
@@ -285,10 +284,11 @@ __global__ void __launch_bounds__(THREADS) resortCellScanKernel(ResortArgs A) {
       if (lane == 0) stRelaxed(&A.tileStatus[tile], kLookAgg | (tileTotal & kLookVal));
       int p = (int)tile - 1;
       uint32_t spins = 0;
+      const bool stalled = tile == A.wait.stallTile;
       while (p >= 0) {
         const int q = p - (int)lane;
         // before tile 0 there is nothing: read as an inclusive zero
-        const uint32_t v = q >= 0 ? ldRelaxed(&A.tileStatus[q]) : kLookInc;
+        const uint32_t v = q >= 0 ? (stalled ? 0u : ldRelaxed(&A.tileStatus[q])) : kLookInc;
         const uint32_t f = v & kLookMask;
         const uint32_t inc = __ballot_sync(0xffffffffu, f == kLookInc);
         const uint32_t unpublished = __ballot_sync(0xffffffffu, f == 0u);
@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(THREADS) resortCellScanKernel(ResortArgs A) {
         const uint32_t need = first == 31u ? 0xffffffffu : ((2u << first) - 1u);
         if (unpublished & need) {
           // a predecessor that claimed its tile is resident and publishes soon
-          if (++spins > kLookSpinLimit) {
+          if (++spins > A.wait.spinLimit) {
             if (lane == 0) atomicOr(A.errWord, kDevErrLookback);
             break;
           }

@@ -13,9 +13,12 @@
 //     decoupled look-back over its predecessors' published counts;
 //   * the tile is reordered by digit in shared memory and written out, so
 //     equal-digit runs leave as contiguous, coalesced stores.
-// Every look-back wait is bounded: after kLookbackSpinLimit polls the tile
-// records kDevErrLookback in the error word and continues, so a kernel never
-// hangs the GPU (the host then reports BRT_ERR_TIMEOUT).
+// Every look-back wait is bounded: after the plan's spin limit of polls the
+// tile records kDevErrLookback in the error word and continues, so a kernel
+// never hangs the GPU (the host then reports BRT_ERR_TIMEOUT).  A tile that
+// gives up takes a partial prefix: its outputs land at positions below the
+// right ones, still inside [0, n), so a failed sort is wrong but never writes
+// out of bounds.
 #include "brt_internal.cuh"
 
 #include <algorithm>
@@ -28,7 +31,6 @@ constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagInc = 2u << 30;
 constexpr uint32_t kFlagMask = 3u << 30;
 constexpr uint32_t kValMask = (1u << 30) - 1;
-constexpr uint32_t kLookbackSpinLimit = 1u << 21;
 
 // Exclusive scan of one value per thread across the CTA; returns the
 // exclusive prefix and writes the total to *total.
@@ -66,7 +68,8 @@ template <int BITS>
 __global__ void __launch_bounds__(kSortThreads)
 onesweepKernel(const uint2* __restrict__ in, uint2* __restrict__ out, uint32_t n, uint32_t shift,
                uint32_t mask, const uint32_t* __restrict__ hist, uint32_t* __restrict__ status,
-               uint32_t* __restrict__ counter, uint32_t* __restrict__ errWord, const uint32_t* gate) {
+               uint32_t* __restrict__ counter, uint32_t* __restrict__ errWord, const uint32_t* gate,
+               LookbackWait wait) {
   constexpr int BINS = 1 << BITS;
   constexpr int T = kSortThreads;
   constexpr int WARPS = T / 32;
@@ -165,13 +168,14 @@ onesweepKernel(const uint2* __restrict__ in, uint2* __restrict__ out, uint32_t n
       if (tile > 0) {
         int p = (int)tile - 1;
         uint32_t spins = 0;
+        const bool stalled = tile == wait.stallTile;
         while (p >= 0) {
-          const uint32_t v = ldRelaxed(&status[(size_t)p * BINS + d]);
+          const uint32_t v = stalled ? 0u : ldRelaxed(&status[(size_t)p * BINS + d]);
           const uint32_t f = v & kFlagMask;
           if (f == 0u) {
             // Plain bounded polling: a predecessor that has claimed its tile
             // is resident and publishes within microseconds.
-            if (++spins > kLookbackSpinLimit) {
+            if (++spins > wait.spinLimit) {
               atomicOr(errWord, kDevErrLookback);
               break;
             }
@@ -202,7 +206,11 @@ onesweepKernel(const uint2* __restrict__ in, uint2* __restrict__ out, uint32_t n
   for (uint32_t p = tid; p < valid; p += T) {
     const uint2 it = sItems[p];
     const uint32_t d = (it.x >> shift) & mask;
-    out[sGlobal[d] + p] = it;
+    // Inside [0, n) whenever the digit histogram counts this input (always,
+    // unless a corrupted step left the engine's pairs and histogram apart).
+    const uint32_t dst = sGlobal[d] + p;
+    if (dst < n) out[dst] = it;
+    else if (errWord) atomicOr(errWord, kDevErrOrder);
   }
 }
 
@@ -279,12 +287,12 @@ cudaError_t launchOnesweepPass(const SortPlan& p, uint32_t pass, const uint2* in
   uint32_t* counter = s.counters + pass;
   dim3 grid(p.tiles), block(kSortThreads);
   switch (p.digitBits) {
-    case 4: onesweepKernel<4><<<grid, block, 0, st>>>(in, out, p.n, shift, mask, hist, status, counter, errWord, gate); break;
-    case 5: onesweepKernel<5><<<grid, block, 0, st>>>(in, out, p.n, shift, mask, hist, status, counter, errWord, gate); break;
-    case 6: onesweepKernel<6><<<grid, block, 0, st>>>(in, out, p.n, shift, mask, hist, status, counter, errWord, gate); break;
-    case 7: onesweepKernel<7><<<grid, block, 0, st>>>(in, out, p.n, shift, mask, hist, status, counter, errWord, gate); break;
-    case 8: onesweepKernel<8><<<grid, block, 0, st>>>(in, out, p.n, shift, mask, hist, status, counter, errWord, gate); break;
-    case 9: onesweepKernel<9><<<grid, block, 0, st>>>(in, out, p.n, shift, mask, hist, status, counter, errWord, gate); break;
+    case 4: onesweepKernel<4><<<grid, block, 0, st>>>(in, out, p.n, shift, mask, hist, status, counter, errWord, gate, p.wait); break;
+    case 5: onesweepKernel<5><<<grid, block, 0, st>>>(in, out, p.n, shift, mask, hist, status, counter, errWord, gate, p.wait); break;
+    case 6: onesweepKernel<6><<<grid, block, 0, st>>>(in, out, p.n, shift, mask, hist, status, counter, errWord, gate, p.wait); break;
+    case 7: onesweepKernel<7><<<grid, block, 0, st>>>(in, out, p.n, shift, mask, hist, status, counter, errWord, gate, p.wait); break;
+    case 8: onesweepKernel<8><<<grid, block, 0, st>>>(in, out, p.n, shift, mask, hist, status, counter, errWord, gate, p.wait); break;
+    case 9: onesweepKernel<9><<<grid, block, 0, st>>>(in, out, p.n, shift, mask, hist, status, counter, errWord, gate, p.wait); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

@@ -351,6 +351,15 @@ class Engine:
         check(lib().brt_adjoint_get_tape(self._h, ptr(lists), ptr(flags), BRT_MEM_HOST), "brt_adjoint_get_tape")
         return lists, flags
 
+    def adjoint_tape_states(self, nsteps: int):
+        """Input state of every step of the last backward (T x N x 4 each:
+        position, forward with speed in w, smoothed acceleration; by agent id;
+        needs option adjoint_export)."""
+        out = [np.empty((nsteps, self.num_agents, 4), np.float32) for _ in range(3)]
+        check(lib().brt_adjoint_get_tape_states(self._h, *(ptr(x) for x in out), BRT_MEM_HOST),
+              "brt_adjoint_get_tape_states")
+        return tuple(out)
+
 
 def radix_sort_pairs(pairs_in, pairs_out, n: int, bits: int, scratch, stream: Optional[int] = None) -> None:
     """Standalone onesweep sort of uint2 (key, value) pairs on device memory."""

@@ -210,7 +210,17 @@ int brt_engine_set_params(brt_engine* e, uint32_t flock, const brt_params* p);
      "adjoint_export"   0/1   keep the frozen lists and branch flags (brt_adjoint_get_tape)
      "random_step"      uint32 the step counter of the Schooling random stream
                               (every hash pass adds 1 before the move reads it)
-   None of these changes results; unknown keys return BRT_ERR_ARG. */
+     "lookback_spin_limit" 0..2^31-1: polls of an unpublished predecessor
+                              before a look-back wait (onesweep passes, the
+                              re-sort's cell scan) gives up (default 2^21,
+                              about a second); the step then reports
+                              BRT_ERR_TIMEOUT at the next sync or getter
+     "lookback_stall_tile" -1 or a tile index: that tile's look-back polls as
+                              if its predecessor never published (a status
+                              word that nothing sets), so tests can make the
+                              bounded wait run out; -1 (default) in normal use
+   None of these changes results (the two look-back options only when no wait
+   runs out); unknown keys return BRT_ERR_ARG. */
 int brt_engine_set_option(brt_engine* e, const char* key, int64_t value);
 /* Autotuner: times the sort digit width, then the flock kernel's block size
    and scan loop, then its list walk, on the engine's own state (graphs of
@@ -226,7 +236,11 @@ int brt_sync(brt_engine* e);
 /* ---- feature arrays (DeviceArrayWrapper::copyArrayToDevice /
         copyArrayFromDevice, Core/include/DeviceArrayWrapper.h:345-386) ---- */
 /* Any pointer may be NULL to leave that feature unchanged / not read.
-   pos4.w is ignored on input (the reference keeps w = 1); fwd4.w = speed. */
+   pos4.w is ignored on input (the reference keeps w = 1); fwd4.w = speed.
+   After a call reported a failed device check (BRT_ERR_TIMEOUT, or
+   BRT_ERR_STATE from the device error word) the engine state is undefined;
+   brt_set_state then also restores the identity slot order, and registered
+   arrays must be set again. */
 int brt_set_state(brt_engine* e, const float* pos4, const float* fwd4,
                   const float* acc4, const float* features, int where);
 int brt_get_state(brt_engine* e, float* pos4, float* fwd4,
@@ -429,6 +443,12 @@ int brt_adjoint_backward(brt_engine* e, const double* loss_scale,
    cohesion membership masks over list positions.  Sizes: nsteps * N *
    stride and nsteps * N * 4 uint32. */
 int brt_adjoint_get_tape(brt_engine* e, uint32_t* lists_by_id, uint32_t* flags_by_id, int where);
+/* With option "adjoint_export", also the input state of every step t as the
+   backward recomputed it (float4 per agent id: position, forward with speed
+   in w, smoothed acceleration; nsteps * N each, any pointer may be NULL).
+   An FP64 reverse linearised at these FP32 states separates the adjoint's
+   own rounding from the FP32 forward's.  No reference counterpart. */
+int brt_adjoint_get_tape_states(brt_engine* e, float* pos4, float* fwd4, float* acc4, int where);
 /* Per-flock steering weights (separationParams[0], alignmentParams[0],
    cohesionParams[0]; nflocks x 3 floats).  Setting them does not invalidate
    captured step graphs (the kernels read them from device memory). */

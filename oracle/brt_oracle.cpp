@@ -57,7 +57,18 @@ template <class R> inline R length(V3<R> a) { return std::sqrt(dot(a, a)); }
 // cutil_math normalize with the host rsqrtf = 1/sqrtf.
 template <class R> inline V3<R> normalize(V3<R> v) { R inv = R(1) / std::sqrt(dot(v, v)); return v * inv; }
 template <class R> inline R clampf(R f, R a, R b) { return std::fmax(a, std::fmin(f, b)); }
-template <class R> inline R powr(R x, R y) { return std::pow(x, y); }
+// x^20 of adjustRawSteeringForce's low-speed branch (the reference's
+// powf(range, 20), Core/common_resources.cu:251).  FP32 mode: computed in
+// double by repeated squaring (x^16 * x^4) and rounded to float once, the
+// operation sequence of the CUDA library's pow20f (the reference's powf is a
+// library routine whose last bit differs between CUDA and glibc; this form is
+// the correctly rounded power unless the exact value lies within ~6e-16 of a
+// float rounding boundary, and is the same on both sides).  FP64 mode: pow.
+inline float pow20(float x) {
+  const double d = (double)x, d2 = d * d, d4 = d2 * d2, d8 = d4 * d4, d16 = d8 * d8;
+  return (float)(d16 * d4);
+}
+inline double pow20(double x) { return std::pow(x, 20.0); }
 
 // Core/common_resources.cu:140-143
 template <class R> inline R interpolate(R alpha, R x0, R x1) { return x0 + ((x1 - x0) * alpha); }
@@ -96,7 +107,7 @@ template <class R> V3<R> adjustRawSteeringForce(V3<R> force, R speed, V3<R> forw
   R maxAdjustedSpeed = R(0.2f) * maxSpeed;
   if ((speed > maxAdjustedSpeed) || (force.x == 0 && force.y == 0 && force.z == 0)) return force;
   R range = speed / maxAdjustedSpeed;
-  R cosine = interpolate(powr(range, R(20)), R(1), R(-1));
+  R cosine = interpolate(pow20(range), R(1), R(-1));
   return vecLimitDeviationAngleUtility(force, cosine, forward);
 }
 

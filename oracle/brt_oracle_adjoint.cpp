@@ -396,20 +396,15 @@ int oracle_frozen_forward(uint32_t nflocks, const brt_params* params, const doub
   return BRT_OK;
 }
 
-// Reverse mode of oracle_frozen_forward.  g*_T: adjoint of the final state
-// (agent-id order; xyz of position / forward / acceleration, forward.w the
-// adjoint of the speed).  Writes the adjoint of the initial state (same
-// layout) and of the weights (nflocks * 3).
-int oracle_frozen_reverse(uint32_t nflocks, const brt_params* params, const double* weights, uint32_t T, double dt,
-                          const double* pos4, const double* fwd4, const double* acc4, const uint32_t* lists,
-                          const uint32_t* flags, const double* gpos4_T, const double* gfwd4_T, const double* gacc4_T,
-                          double* gpos4_0, double* gfwd4_0, double* gacc4_0, double* gw, int threads) {
-  for (uint32_t f = 0; f < nflocks; ++f)
-    if (params[f].maxNeighbors > 32) return BRT_ERR_CONFIG;
-  Setup su = makeSetup(nflocks, params, weights);
-  std::vector<std::vector<Agent>> traj(T);
-  std::vector<Agent> S = load(su.N, pos4, fwd4, acc4);
-  forwardSteps(su, T, dt, lists, flags, nullptr, &traj, S, threads);
+}  // extern "C"
+
+namespace {
+
+// The reverse sweep over a given trajectory (traj[t] = input state of step t).
+void reverseSweep(const Setup& su, uint32_t nflocks, uint32_t T, double dt, const uint32_t* lists,
+                  const uint32_t* flags, const std::vector<std::vector<Agent>>& traj, const double* gpos4_T,
+                  const double* gfwd4_T, const double* gacc4_T, double* gpos4_0, double* gfwd4_0, double* gacc4_0,
+                  double* gw) {
   std::vector<Agent> G = load(su.N, gpos4_T, gfwd4_T, gacc4_T);
   std::vector<double> gwAcc(3 * (size_t)nflocks, 0.0);
   const Agent zero{d3(0, 0, 0), d3(0, 0, 0), d3(0, 0, 0), 0.0};
@@ -428,6 +423,48 @@ int oracle_frozen_reverse(uint32_t nflocks, const brt_params* params, const doub
   }
   store(G, gpos4_0, gfwd4_0, gacc4_0, 0.0);
   std::memcpy(gw, gwAcc.data(), sizeof(double) * gwAcc.size());
+}
+
+}  // namespace
+
+extern "C" {
+
+// Reverse mode of oracle_frozen_forward.  g*_T: adjoint of the final state
+// (agent-id order; xyz of position / forward / acceleration, forward.w the
+// adjoint of the speed).  Writes the adjoint of the initial state (same
+// layout) and of the weights (nflocks * 3).
+int oracle_frozen_reverse(uint32_t nflocks, const brt_params* params, const double* weights, uint32_t T, double dt,
+                          const double* pos4, const double* fwd4, const double* acc4, const uint32_t* lists,
+                          const uint32_t* flags, const double* gpos4_T, const double* gfwd4_T, const double* gacc4_T,
+                          double* gpos4_0, double* gfwd4_0, double* gacc4_0, double* gw, int threads) {
+  for (uint32_t f = 0; f < nflocks; ++f)
+    if (params[f].maxNeighbors > 32) return BRT_ERR_CONFIG;
+  Setup su = makeSetup(nflocks, params, weights);
+  std::vector<std::vector<Agent>> traj(T);
+  std::vector<Agent> S = load(su.N, pos4, fwd4, acc4);
+  forwardSteps(su, T, dt, lists, flags, nullptr, &traj, S, threads);
+  reverseSweep(su, nflocks, T, dt, lists, flags, traj, gpos4_T, gfwd4_T, gacc4_T, gpos4_0, gfwd4_0, gacc4_0, gw);
+  return BRT_OK;
+}
+
+// The same reverse, linearised at a given trajectory instead of the FP64
+// forward's: pos4_t / fwd4_t / acc4_t hold the input state of every step
+// (T * N * 4 each, agent-id order), e.g. the FP32 states the GPU stepped
+// through.  Against oracle_frozen_reverse this separates the effect of the
+// trajectory (FP32 forward rounding) from the reverse arithmetic itself.
+int oracle_frozen_reverse_at(uint32_t nflocks, const brt_params* params, const double* weights, uint32_t T, double dt,
+                             const double* pos4_t, const double* fwd4_t, const double* acc4_t, const uint32_t* lists,
+                             const uint32_t* flags, const double* gpos4_T, const double* gfwd4_T,
+                             const double* gacc4_T, double* gpos4_0, double* gfwd4_0, double* gacc4_0, double* gw) {
+  for (uint32_t f = 0; f < nflocks; ++f)
+    if (params[f].maxNeighbors > 32) return BRT_ERR_CONFIG;
+  Setup su = makeSetup(nflocks, params, weights);
+  std::vector<std::vector<Agent>> traj(T);
+  for (uint32_t t = 0; t < T; ++t) {
+    const size_t o = (size_t)t * su.N * 4;
+    traj[t] = load(su.N, pos4_t + o, fwd4_t + o, acc4_t + o);
+  }
+  reverseSweep(su, nflocks, T, dt, lists, flags, traj, gpos4_T, gfwd4_T, gacc4_T, gpos4_0, gfwd4_0, gacc4_0, gw);
   return BRT_OK;
 }
 

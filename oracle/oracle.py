@@ -54,6 +54,9 @@ def lib():
         L.oracle_frozen_reverse.restype = C.c_int
         L.oracle_frozen_reverse.argtypes = [C.c_uint32, _vp, _vp, C.c_uint32, C.c_double, _vp, _vp, _vp, _vp,
                                             _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int]
+        L.oracle_frozen_reverse_at.restype = C.c_int
+        L.oracle_frozen_reverse_at.argtypes = [C.c_uint32, _vp, _vp, C.c_uint32, C.c_double, _vp, _vp, _vp, _vp,
+                                               _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
         _LIB = L
     return _LIB
 
@@ -215,6 +218,31 @@ def frozen_reverse(params: Sequence, pos, fwd, acc, lists, gpos_T, gfwd_T=None, 
                                      _p(out["acc"]), _p(out["weights"]), _threads(threads))
     if rc:
         raise RuntimeError("oracle_frozen_reverse failed: %d" % rc)
+    return out
+
+
+def frozen_reverse_at(params: Sequence, states, lists, gpos_T, gfwd_T=None, gacc_T=None, weights=None,
+                      flags=None, dt: float = 0.1) -> dict:
+    """frozen_reverse linearised at a given trajectory: states = (pos, fwd,
+    acc), each T x N x 4 (the input state of every step, by agent id)."""
+    from behavert_b200._abi import BrtParams
+    lists = np.ascontiguousarray(lists, np.uint32)
+    T, n = lists.shape[0], lists.shape[1]
+    pos_t, fwd_t, acc_t = (np.ascontiguousarray(x, np.float64).reshape(T, n, 4) for x in states)
+    z = np.zeros((n, 4))
+    gp = np.ascontiguousarray(gpos_T, np.float64)
+    gf = z if gfwd_T is None else np.ascontiguousarray(gfwd_T, np.float64)
+    ga = z if gacc_T is None else np.ascontiguousarray(gacc_T, np.float64)
+    w = None if weights is None else np.ascontiguousarray(weights, np.float64).reshape(-1)
+    fz = None if flags is None else np.ascontiguousarray(flags, np.uint32)
+    out = {"pos": np.empty((n, 4)), "fwd": np.empty((n, 4)), "acc": np.empty((n, 4)),
+           "weights": np.empty((len(params), 3))}
+    arr = (BrtParams * len(params))(*params)
+    rc = lib().oracle_frozen_reverse_at(len(params), C.cast(arr, _vp), _p(w), T, float(dt), _p(pos_t), _p(fwd_t),
+                                        _p(acc_t), _p(lists), _p(fz), _p(gp), _p(gf), _p(ga), _p(out["pos"]),
+                                        _p(out["fwd"]), _p(out["acc"]), _p(out["weights"]))
+    if rc:
+        raise RuntimeError("oracle_frozen_reverse_at failed: %d" % rc)
     return out
 
 
