@@ -6,10 +6,17 @@
 // baseline / reference arm may load it; the product library never does.
 //
 // Parity pinning: the reference ships no tests, fixtures or golden vectors
-// for this path, and its GPU code cannot be built here (cutil, texture
-// references, GL interop, MSVC-only constructs).  This restatement is therefore
-// "parity unpinned" against reference-produced outputs; each function cites
-// the reference lines it follows.
+// for this path, and its CUDA build cannot run here (cutil, texture
+// references, GL interop, MSVC-only constructs).  Its device functions and
+// per-agent kernels of this path do compile on the host with small
+// stand-ins (oracle/build_ref.py, oracle/ref_shim/): cell hash, neighbour
+// search in visit order with the maxNeighbors cap (first-M and kNN),
+// inBoidNeighborhood, separation / alignment / cohesion, adjustRawSteeringForce
+// and applySteeringForceSingle, and one whole frame of the flocking demo
+// through genericCalcNeighgborhoodD, genericSeparationD / AlignmentD /
+// CohesionD and genericApplySteeringForceD.  tests/test_oracle_reference.py
+// checks this restatement against them bit for bit.  Each function cites the
+// reference lines it follows.
 //
 // Two modes share one template:
 //   mode 0 (FP32): float arithmetic in the reference's operation order, built
