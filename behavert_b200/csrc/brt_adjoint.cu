@@ -23,9 +23,10 @@
 //           sends to the listed agent j, stored at the entry; the entry code
 //           goes into j's in-list (an inbox whose positions come from an
 //           atomic counter: the transposed neighbour list of the frozen step);
-//   gather  one thread per agent j: sorts its in-list by entry code (i, k),
-//           adds the stored contributions in that order to its own terms and
-//           stores its input adjoint (every canonical slot is written once).
+//   gather  one thread per agent j: adds the stored contributions of its
+//           in-list to its own terms with an exact, order-free sum (64-bit
+//           fixed point at a scale set by the largest term) and stores its
+//           input adjoint (every canonical slot is written once).
 // The weight adjoint is summed per agent over the steps in FP64 (each agent
 // by its own thread, in step order) and reduced per flock in a fixed tree at
 // the end.  Two runs from the same state give the same bits.
@@ -82,10 +83,6 @@ __device__ __forceinline__ f3 limitedDeviation(f3 source, float cosineOfConeAngl
   return mul3(add3(mul3(basis, cosineOfConeAngle), mul3(unitPerp, perpDist)), sourceLength);
 }
 
-// In-list entries a gather thread sorts in local memory; longer in-lists
-// (rare: that many agents listing one neighbour) are processed in ascending
-// order by repeated selection instead.
-constexpr uint32_t kGatherCap = 64;
 
 }  // namespace
 
@@ -313,12 +310,18 @@ __global__ void __launch_bounds__(kAdjointThreads) adjointStepKernel(AdjointStep
       }
       if ((mC >> k) & 1u) gp = add3(gp, gSc);
       const f3 gf = ((mA >> k) & 1u) ? gSa : mk3(0.f, 0.f, 0.f);
-      const uint32_t e = i * A.entryStride + k;
-      A.contrib[2 * (size_t)e + 0] = make_float4(gp.x, gp.y, gp.z, gf.x);
-      A.contrib[2 * (size_t)e + 1] = make_float4(gf.y, gf.z, 0.0f, 0.0f);
+      const float4 c0 = make_float4(gp.x, gp.y, gp.z, gf.x), c1 = make_float4(gf.y, gf.z, 0.0f, 0.0f);
       const uint32_t q = atomicAdd(&A.inCount[j], 1u);
-      if (q < A.inCap) A.inbox[(size_t)j * A.inCap + q] = e;
-      else A.ovNext[e] = atomicExch(&A.ovHead[j], e);
+      if (q < A.inCap) {
+        float4* slot = A.inbox + 2 * ((size_t)j * A.inCap + q);
+        slot[0] = c0;
+        slot[1] = c1;
+      } else {
+        const uint32_t e = i * A.entryStride + k;
+        A.contrib[2 * (size_t)e + 0] = c0;
+        A.contrib[2 * (size_t)e + 1] = c1;
+        A.ovNext[e] = atomicExch(&A.ovHead[j], e);
+      }
     }
     A.selfP[i] = make_float4(selfP.x, selfP.y, selfP.z, 0.0f);
     A.selfF[i] = make_float4(selfF.x, selfF.y, selfF.z, selfS);
@@ -344,66 +347,133 @@ __global__ void __launch_bounds__(kAdjointThreads) adjointStepKernel(AdjointStep
   }
 }
 
-// Adds in-list entry e's contribution (stored by its emitter) to this
-// agent's position and forward adjoints.
-__device__ __forceinline__ void addContribution(const float4 c0, const float4 c1, f3& tP, f3& tF) {
-  tP = add3(tP, xyz(c0));
-  tF = add3(tF, mk3(c0.w, c1.x, c1.y));
-}
-
-__global__ void __launch_bounds__(kAdjointThreads) adjointGatherKernel(AdjointStepArgs A) {
-  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= A.n) return;
-  const uint32_t cnt = A.inCount[j];
-  A.inCount[j] = 0u;  // clean for the next-earlier step
-  const float4 sp = A.selfP[j], sf = A.selfF[j];
-  f3 tP = xyz(sp), tF = xyz(sf);
-  if (cnt <= A.inCap && cnt <= kGatherCap) {
-    uint32_t buf[kGatherCap];
-    const uint32_t* box = A.inbox + (size_t)j * A.inCap;
-    for (uint32_t q = 0; q < cnt; ++q) buf[q] = box[q];
-    for (uint32_t q = 1; q < cnt; ++q) {  // insertion sort by entry code
-      const uint32_t v = buf[q];
-      uint32_t r = q;
-      while (r > 0 && buf[r - 1] > v) { buf[r] = buf[r - 1]; --r; }
-      buf[r] = v;
-    }
-    // four entries' loads in flight, their sums in entry order
-    for (uint32_t q = 0; q < cnt; q += 4) {
-      float4 c[4][2];
+// The gather's sums are exact and order-free.  Per component, every term
+// (the agent's own and each in-list entry's) is scaled by 2^sh, sh fixed by
+// the largest magnitude among them and the number of terms, rounded to an
+// integer and added in 64-bit integers, which is exact and associative; the
+// total is rounded to float once.  Terms below 2^-sh of the largest round to
+// zero (their share of the float result is below its last bit).  So the
+// result does not depend on the order the in-list was filled in, and no sort
+// is needed.
+struct ExactSum6 {
+  float mx[6];
+  int sh[6];
+  long long acc[6];
+  bool finite = true;
+  __device__ __forceinline__ void seeMax(const float* t) {
 #pragma unroll
-      for (uint32_t u = 0; u < 4; ++u)
-        if (q + u < cnt) {
-          c[u][0] = A.contrib[2 * (size_t)buf[q + u] + 0];
-          c[u][1] = A.contrib[2 * (size_t)buf[q + u] + 1];
-        }
+    for (int c = 0; c < 6; ++c) mx[c] = fmaxf(mx[c], fabsf(t[c]));
+  }
+  __device__ __forceinline__ void scales(uint32_t terms) {
+    const int headroom = 32 - __clz((int)terms);  // bits to hold the count of terms
 #pragma unroll
-      for (uint32_t u = 0; u < 4; ++u)
-        if (q + u < cnt) addContribution(c[u][0], c[u][1], tP, tF);
-    }
-  } else {
-    // ascending order by repeated selection over the inbox and the overflow list
-    const uint32_t head = A.ovHead[j];
-    A.ovHead[j] = kNoEntry;
-    const uint32_t* box = A.inbox + (size_t)j * A.inCap;
-    const uint32_t inBox = min(cnt, A.inCap);
-    uint32_t last = 0;
-    for (uint32_t q = 0; q < cnt; ++q) {
-      uint32_t best = kNoEntry;
-      for (uint32_t r = 0; r < inBox; ++r) {
-        const uint32_t e = box[r];
-        if ((q == 0 || e > last) && e < best) best = e;
-      }
-      for (uint32_t e = head; e != kNoEntry; e = A.ovNext[e])
-        if ((q == 0 || e > last) && e < best) best = e;
-      addContribution(A.contrib[2 * (size_t)best], A.contrib[2 * (size_t)best + 1], tP, tF);
-      last = best;
+    for (int c = 0; c < 6; ++c) {
+      if (!isfinite(mx[c])) finite = false;
+      int ex = 0;
+      if (mx[c] > 0.0f) frexpf(mx[c], &ex);
+      sh[c] = 62 - headroom - ex;  // |term| * 2^sh < 2^(62 - headroom)
+      acc[c] = 0;
     }
   }
-  const uint32_t t = __ldg(&A.prev[j]);
-  if (t >= A.n) return;  // only a corrupted step leaves such a source slot
-  A.gInP[t] = make_float4(tP.x, tP.y, tP.z, 0.0f);
-  A.gInF[t] = make_float4(tF.x, tF.y, tF.z, sf.w);
+  __device__ __forceinline__ void add(const float* t) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) acc[c] += __float2ll_rn(ldexpf(t[c], sh[c]));
+  }
+  __device__ __forceinline__ float value(int c) const { return ldexpf(__ll2float_rn(acc[c]), -sh[c]); }
+};
+
+__device__ __forceinline__ void termsOf(const float4 c0, const float4 c1, float* t) {
+  t[0] = c0.x; t[1] = c0.y; t[2] = c0.z; t[3] = c0.w; t[4] = c1.x; t[5] = c1.y;
+}
+
+// kGatherLanes consecutive lanes gather one agent: lane `sub` takes inbox
+// entries sub, sub + kGatherLanes, ... (the group reads the agent's inbox
+// block coalesced, once, and keeps its terms in registers for the second
+// pass) and every kGatherLanes-th overflow entry.  The maxima and the
+// integer sums combine across the lanes exactly (both are associative), so
+// the split changes no bit.
+constexpr uint32_t kGatherLanes = 8;
+constexpr uint32_t kGatherPerLane = 8;  // inbox entries a lane holds: inCap <= 64
+
+__global__ void __launch_bounds__(kAdjointThreads) adjointGatherKernel(AdjointStepArgs A) {
+  const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t j = gt / kGatherLanes, sub = gt % kGatherLanes;
+  const bool valid = j < A.n;
+  uint32_t cnt = 0, head = kNoEntry, inBox = 0;
+  float self[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  float selfS = 0.0f;
+  if (valid) {
+    cnt = A.inCount[j];
+    inBox = min(cnt, A.inCap);
+    if (cnt > A.inCap) head = A.ovHead[j];
+    const float4 sp = A.selfP[j], sf = A.selfF[j];
+    self[0] = sp.x; self[1] = sp.y; self[2] = sp.z; self[3] = sf.x; self[4] = sf.y; self[5] = sf.z;
+    selfS = sf.w;
+  }
+  // this lane's inbox terms, in registers
+  float tk[kGatherPerLane][6];
+  const float4* box = A.inbox + 2 * (size_t)j * A.inCap;
+  ExactSum6 S;
+#pragma unroll
+  for (int c = 0; c < 6; ++c) S.mx[c] = fabsf(self[c]);
+#pragma unroll
+  for (uint32_t r = 0; r < kGatherPerLane; ++r) {
+    const uint32_t q = sub + r * kGatherLanes;
+    if (q < inBox) {
+      termsOf(box[2 * q], box[2 * q + 1], tk[r]);
+      S.seeMax(tk[r]);
+    }
+  }
+  float t[6];
+  uint32_t r = 0;
+  for (uint32_t e = head; e != kNoEntry; e = A.ovNext[e], ++r)
+    if (r % kGatherLanes == sub) { termsOf(A.contrib[2 * (size_t)e], A.contrib[2 * (size_t)e + 1], t); S.seeMax(t); }
+  // the group's maxima (the lanes of one agent are consecutive in the warp)
+#pragma unroll
+  for (int c = 0; c < 6; ++c)
+#pragma unroll
+    for (uint32_t o = 1; o < kGatherLanes; o <<= 1) S.mx[c] = fmaxf(S.mx[c], __shfl_xor_sync(0xFFFFFFFFu, S.mx[c], o));
+  S.scales(cnt + 1u);
+  const bool finite = S.finite;  // the same in every lane of the group (same maxima)
+  if (finite) {
+    if (sub == 0) S.add(self);
+#pragma unroll
+    for (uint32_t rr = 0; rr < kGatherPerLane; ++rr)
+      if (sub + rr * kGatherLanes < inBox) S.add(tk[rr]);
+    r = 0;
+    for (uint32_t e = head; e != kNoEntry; e = A.ovNext[e], ++r)
+      if (r % kGatherLanes == sub) { termsOf(A.contrib[2 * (size_t)e], A.contrib[2 * (size_t)e + 1], t); S.add(t); }
+  }
+#pragma unroll
+  for (int c = 0; c < 6; ++c)
+#pragma unroll
+    for (uint32_t o = 1; o < kGatherLanes; o <<= 1) S.acc[c] += __shfl_xor_sync(0xFFFFFFFFu, S.acc[c], o);
+  if (!valid || sub != 0) return;
+  A.inCount[j] = 0u;  // clean for the next-earlier step
+  if (cnt > A.inCap) A.ovHead[j] = kNoEntry;
+  float res[6];
+  if (finite) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) res[c] = S.value(c);
+  } else {
+    // a non-finite term: no exact sum; a plain one (not finite either)
+#pragma unroll
+    for (int c = 0; c < 6; ++c) res[c] = self[c];
+    for (uint32_t q = 0; q < inBox; ++q) {
+      termsOf(box[2 * q], box[2 * q + 1], t);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) res[c] += t[c];
+    }
+    for (uint32_t e = head; e != kNoEntry; e = A.ovNext[e]) {
+      termsOf(A.contrib[2 * (size_t)e], A.contrib[2 * (size_t)e + 1], t);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) res[c] += t[c];
+    }
+  }
+  const uint32_t tj = __ldg(&A.prev[j]);
+  if (tj >= A.n) return;  // only a corrupted step leaves such a source slot
+  A.gInP[tj] = make_float4(res[0], res[1], res[2], 0.0f);
+  A.gInF[tj] = make_float4(res[3], res[4], res[5], selfS);
 }
 
 // Per-flock sums of `width` doubles per item over flock f's items
@@ -508,11 +578,13 @@ __global__ void __launch_bounds__(256) adjointOutKernel(OutArgs A) {
 cudaError_t launchAdjointStep(const AdjointStepArgs& A, cudaStream_t st) {
   if (A.n == 0) return cudaSuccess;
   if (A.entryStride == 0 || A.entryStride > 32) return cudaErrorInvalidValue;
+  if (A.inCap > kGatherLanes * kGatherPerLane) return cudaErrorInvalidValue;
   const uint32_t blocks = (A.n + kAdjointThreads - 1) / kAdjointThreads;
   adjointStepKernel<<<blocks, kAdjointThreads, 0, st>>>(A);
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) return err;
-  adjointGatherKernel<<<blocks, kAdjointThreads, 0, st>>>(A);
+  const uint32_t gatherBlocks = (uint32_t)(((size_t)A.n * kGatherLanes + kAdjointThreads - 1) / kAdjointThreads);
+  adjointGatherKernel<<<gatherBlocks, kAdjointThreads, 0, st>>>(A);
   return cudaGetLastError();
 }
 cudaError_t launchFlockReduce(const FlockReduceArgs& A, cudaStream_t st) {

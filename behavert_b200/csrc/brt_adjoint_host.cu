@@ -35,9 +35,16 @@ struct AdjointState {
   float4 *finPos = nullptr, *finFwd = nullptr, *finAcc = nullptr;
   uint32_t* finId = nullptr;
   float* finFeat = nullptr;
-  // k-step tape
-  float4 *tPos = nullptr, *tFwd = nullptr, *tAcc = nullptr;
-  uint32_t *tPrev = nullptr, *tId = nullptr, *tLists = nullptr;
+  // two k-step tapes: the backward recomputes segment c - 1 into one while
+  // the reverse of segment c reads the other
+  struct Tape {
+    float4 *pos = nullptr, *fwd = nullptr, *acc = nullptr;
+    uint32_t *prev = nullptr, *id = nullptr, *lists = nullptr;
+  } tape[2];
+  // the reverse chain's stream and the events that order it against the
+  // recompute chain on the engine stream (2 per checkpoint segment)
+  cudaStream_t revStream = nullptr;
+  std::vector<cudaEvent_t> events;
   // adjoint buffers
   float4* g[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
   float4* gT = nullptr;
@@ -51,7 +58,8 @@ struct AdjointState {
   // emit -> gather hand-over of one reverse step, and the weight sums
   float4 *contrib = nullptr, *selfP = nullptr, *selfF = nullptr;
   double* partial = nullptr;  // per-flock reduction parts
-  uint32_t *inCount = nullptr, *inbox = nullptr, *ovHead = nullptr, *ovNext = nullptr;
+  uint32_t *inCount = nullptr, *ovHead = nullptr, *ovNext = nullptr;
+  float4* inbox = nullptr;
   uint32_t inCap = 0;
   double* accW = nullptr;
   // graphs: (kind, T, k, dt bits, params version, variant bits)
@@ -62,6 +70,8 @@ void freeAdjoint(AdjointState* a) {
   if (!a) return;
   for (auto& kv : a->graphs) cudaGraphExecDestroy(kv.second);
   for (void* p : a->mem) cudaFree(p);
+  for (cudaEvent_t ev : a->events) cudaEventDestroy(ev);
+  if (a->revStream) cudaStreamDestroy(a->revStream);
   delete a;
 }
 
@@ -125,7 +135,7 @@ int ensureCapacity(brt_engine* e, uint32_t nck, uint32_t k, uint32_t T) {
     // rest overflows into a linked list
     a->inCap = std::min(64u, 2u * e->Mmax);
     if ((rc = adjAlloc(a, &a->inCount, n))) return rc;
-    if ((rc = adjAlloc(a, &a->inbox, n * (size_t)a->inCap))) return rc;
+    if ((rc = adjAlloc(a, &a->inbox, 2 * n * (size_t)a->inCap))) return rc;
     if ((rc = adjAlloc(a, &a->ovHead, n))) return rc;
     if ((rc = adjAlloc(a, &a->ovNext, n * (size_t)e->Mmax))) return rc;
     if ((rc = adjAlloc(a, &a->accW, 3 * n))) return rc;
@@ -147,11 +157,18 @@ int ensureCapacity(brt_engine* e, uint32_t nck, uint32_t k, uint32_t T) {
   }
   if (k > a->capK) {
     BRT_CUDA_TRY(cudaStreamSynchronize(e->stream));
-    if ((rc = regrow(&a->tPos, n * k)) || (rc = regrow(&a->tFwd, n * k)) || (rc = regrow(&a->tAcc, n * k)) ||
-        (rc = regrow(&a->tPrev, n * k)) || (rc = regrow(&a->tId, n * k)) || (rc = regrow(&a->tLists, n * k * e->listStride)))
-      return rc;
+    for (auto& t : a->tape)
+      if ((rc = regrow(&t.pos, n * k)) || (rc = regrow(&t.fwd, n * k)) || (rc = regrow(&t.acc, n * k)) ||
+          (rc = regrow(&t.prev, n * k)) || (rc = regrow(&t.id, n * k)) || (rc = regrow(&t.lists, n * k * e->listStride)))
+        return rc;
     a->capK = k;
     changed = true;
+  }
+  if (!a->revStream) BRT_CUDA_TRY(cudaStreamCreateWithFlags(&a->revStream, cudaStreamNonBlocking));
+  while (a->events.size() < 2 * (size_t)nck) {
+    cudaEvent_t ev = nullptr;
+    BRT_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    a->events.push_back(ev);
   }
   if (e->adjointExport && T > a->capExport) {
     BRT_CUDA_TRY(cudaStreamSynchronize(e->stream));
@@ -205,9 +222,9 @@ int enqueueForward(brt_engine* e) {
   return BRT_OK;
 }
 
-// Re-runs one segment's steps with the tape as the step's sorted-state and
+// Re-runs one segment's steps with a tape as the step's sorted-state and
 // list buffers.
-int enqueueRecompute(brt_engine* e, uint32_t steps) {
+int enqueueRecompute(brt_engine* e, uint32_t steps, const AdjointState::Tape& tp) {
   AdjointState* a = e->adj;
   const size_t n = e->N;
   float4 *posS = e->posS, *fwdS = e->fwdS, *accS = e->accS;
@@ -218,10 +235,10 @@ int enqueueRecompute(brt_engine* e, uint32_t steps) {
   e->userFrozen = true;
   int rc = BRT_OK;
   for (uint32_t s = 0; s < steps && !rc; ++s) {
-    e->posS = a->tPos + s * n; e->fwdS = a->tFwd + s * n; e->accS = a->tAcc + s * n;
-    e->idS = a->tId + s * n;
-    e->lists = a->tLists + s * n * e->listStride;
-    e->tapePrev = a->tPrev + s * n;
+    e->posS = tp.pos + s * n; e->fwdS = tp.fwd + s * n; e->accS = tp.acc + s * n;
+    e->idS = tp.id + s * n;
+    e->lists = tp.lists + s * n * e->listStride;
+    e->tapePrev = tp.prev + s * n;
     rc = engineEnqueueStep(e, a->dt, true);
   }
   e->posS = posS; e->fwdS = fwdS; e->accS = accS; e->idS = idS; e->lists = lists;
@@ -250,18 +267,37 @@ int enqueueBackward(brt_engine* e, uint32_t variant) {
   BRT_CUDA_TRY(cudaMemsetAsync(a->accW, 0, 24 * n, e->stream));
   BRT_CUDA_TRY(cudaMemsetAsync(a->inCount, 0, 4 * n, e->stream));     // empty in-lists
   BRT_CUDA_TRY(cudaMemsetAsync(a->ovHead, 0xFF, 4 * n, e->stream));    // kNoEntry
-  for (int c = (int)a->nck - 1; c >= 0; --c) {
-    if ((rc = copyState(e, e->posA, e->fwdA, e->accA, e->idA, a->ckPos + c * n, a->ckFwd + c * n, a->ckAcc + c * n,
-                        a->ckId + c * n)))
-      return rc;
+  // Two chains: the recompute of each checkpoint segment on the engine
+  // stream (it owns the engine's buffers) and the reverse steps on revStream.
+  // Segment c's reverse waits for its recompute; the recompute of c - 1 runs
+  // beside it into the other tape, once the reverse of c + 1 (the last
+  // reader of that tape) is done.  Both are latency-bound at these sizes, so
+  // the two overlap on the GPU; the results are those of running them in
+  // sequence.
+  cudaStream_t rs = a->revStream;
+  auto evRecomputed = [a](int c) { return a->events[2 * (size_t)c]; };
+  auto evReversed = [a](int c) { return a->events[2 * (size_t)c + 1]; };
+  auto recompute = [&](int c) -> int {
+    if (c + 2 < (int)a->nck) BRT_CUDA_TRY(cudaStreamWaitEvent(e->stream, evReversed(c + 2), 0));
+    int r = copyState(e, e->posA, e->fwdA, e->accA, e->idA, a->ckPos + c * n, a->ckFwd + c * n, a->ckAcc + c * n,
+                      a->ckId + c * n);
+    if (r) return r;
     const uint32_t steps = std::min(a->k, a->T - (uint32_t)c * a->k);
-    if ((rc = enqueueRecompute(e, steps))) return rc;
+    if ((r = enqueueRecompute(e, steps, a->tape[c & 1]))) return r;
+    BRT_CUDA_TRY(cudaEventRecord(evRecomputed(c), e->stream));
+    return BRT_OK;
+  };
+  if ((rc = recompute((int)a->nck - 1))) return rc;
+  for (int c = (int)a->nck - 1; c >= 0; --c) {
+    BRT_CUDA_TRY(cudaStreamWaitEvent(rs, evRecomputed(c), 0));
+    const AdjointState::Tape& tp = a->tape[c & 1];
+    const uint32_t steps = std::min(a->k, a->T - (uint32_t)c * a->k);
     for (int s = (int)steps - 1; s >= 0; --s) {
       AdjointStepArgs R;
       std::memset(&R, 0, sizeof(R));
-      R.posS = a->tPos + s * n; R.fwdS = a->tFwd + s * n; R.accS = a->tAcc + s * n;
-      R.lists = a->tLists + s * n * e->listStride; R.listStride = e->listStride;
-      R.prev = a->tPrev + s * n; R.idS = a->tId + s * n;
+      R.posS = tp.pos + s * n; R.fwdS = tp.fwd + s * n; R.accS = tp.acc + s * n;
+      R.lists = tp.lists + s * n * e->listStride; R.listStride = e->listStride;
+      R.prev = tp.prev + s * n; R.idS = tp.id + s * n;
       R.flocks = e->flocks; R.agentBase = e->agentBase; R.obstacles = e->obstacles; R.obsMask = e->obsMask;
       R.nflocks = e->nflocks; R.n = e->N; R.dt = a->dt;
       R.gOutP = a->g[cur][0]; R.gOutF = a->g[cur][1]; R.gOutA = a->g[cur][2];
@@ -276,10 +312,13 @@ int enqueueBackward(brt_engine* e, uint32_t variant) {
         R.exportFlags = a->expFlags + t * n * 4;
         R.exportState = a->expState + t * n * 3;
       }
-      BRT_CUDA_TRY(launchAdjointStep(R, e->stream));
+      BRT_CUDA_TRY(launchAdjointStep(R, rs));
       cur ^= 1;
     }
+    BRT_CUDA_TRY(cudaEventRecord(evReversed(c), rs));
+    if (c > 0 && (rc = recompute(c - 1))) return rc;
   }
+  BRT_CUDA_TRY(cudaStreamWaitEvent(e->stream, evReversed(0), 0));
   FlockReduceArgs W;
   W.vals = a->accW; W.width = 3; W.agentBase = e->agentBase; W.nflocks = e->nflocks; W.out = a->gW;
   W.partial = a->partial;

@@ -137,16 +137,18 @@ struct AdjointStepArgs {
   const float4* gOutP; const float4* gOutF; const float4* gOutA; // output adjoint by sorted slot
   float4* gInP; float4* gInF; float4* gInA;                      // input adjoint by canonical slot
   // Emit -> gather hand-over of one step (sorted slots of this step):
-  float4* contrib;      // 2 per list entry e = i * entryStride + k: the position adjoint (xyz)
-                        // and forward adjoint (w, then xy) that agent i sends the agent it lists at k
+  float4* contrib;      // 2 per list entry e = i * entryStride + k, for in-list overflow only: the
+                        // position adjoint (xyz) and forward adjoint (w, then xy) agent i sends
+                        // the agent it lists at k
   float4* selfP;        // per slot: the agent's own position adjoint terms
   float4* selfF;        // per slot: the agent's own forward adjoint terms (w: speed)
-  // In-lists (the transposed neighbour list of the step): agent j's entries
-  // e = i * entryStride + k (agent i lists j at position k) go to
-  // inbox[j * inCap + q] at q = atomicAdd(&inCount[j], 1); entries beyond
-  // inCap go to a linked overflow list (ovHead[j], ovNext[e]).  The gather
-  // resets inCount and ovHead for the next-earlier step.
-  uint32_t* inCount; uint32_t* inbox; uint32_t inCap;
+  // In-lists (the transposed neighbour list of the step): the contribution
+  // of entry e = i * entryStride + k (agent i lists j at position k) goes to
+  // inbox[2 * (j * inCap + q)] (two float4) at q = atomicAdd(&inCount[j], 1);
+  // entries beyond inCap go to contrib[2 * e] and a linked overflow list
+  // (ovHead[j], ovNext[e]).  The gather resets inCount and ovHead for the
+  // next-earlier step.
+  uint32_t* inCount; float4* inbox; uint32_t inCap;
   uint32_t* ovHead; uint32_t* ovNext;
   uint32_t entryStride; // list positions per slot in the entry code (maxNeighbors, <= 32)
   double* accW;         // per agent id: the weight adjoint summed over the steps (3 doubles)
