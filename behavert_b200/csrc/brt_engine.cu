@@ -190,6 +190,8 @@ void freeAll(brt_engine* e) {
                   e->membership[0], e->membership[1], e->resortMem};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  if (e->tiles) cudaFree(e->tiles);
+  if (e->tileCounter) cudaFree(e->tileCounter);
   for (auto& u : e->user) {
     cudaFree(u.a);
     cudaFree(u.s);
@@ -351,6 +353,7 @@ int enqueueStep(brt_engine* e, float dt, bool record) {
   F.lists = record ? e->lists : nullptr; F.listStride = e->listStride;
   F.nflocks = e->nflocks; F.n = e->N; F.Mmax = e->Mmax; F.Fs = e->Fs; F.dt = dt;
   F.scanVariant = e->scanVariant;
+  F.tiles = e->tiles; F.numTiles = e->numTiles; F.tileCounter = e->tileCounter; F.tileBlocks = e->tileBlocks;
   F.stepCounter = e->stepCounter;
   // The single-pass kernel covers every flock unless one needs kNN
   // replacement or clustering steering (both need the whole list first).
@@ -411,6 +414,28 @@ int checkDeviceError(brt_engine* e, bool clear) {
 int syncAndCheck(brt_engine* e) { return checkDeviceError(e, true); }
 
 int configureKernels(brt_engine* e);
+
+// The (flock, row segment) tiles of scan variant 6: every x-row of every
+// flock cut into segments of at most kTileMaxCells home cells.
+int buildTiles(brt_engine* e) {
+  std::vector<uint4> tiles;
+  for (uint32_t f = 0; f < e->nflocks; ++f) {
+    const FlockDev& d = e->flocksHost[f];
+    const uint32_t G = d.G;
+    const uint32_t R = std::min<uint32_t>(G, kTileMaxCells);
+    for (uint32_t z = 0; z < G; ++z)
+      for (uint32_t y = 0; y < G; ++y)
+        for (uint32_t x0 = 0; x0 < G; x0 += R)
+          tiles.push_back(make_uint4(f, y | (z << 16), x0 | (std::min(R, G - x0) << 16), 0u));
+  }
+  e->numTiles = (uint32_t)tiles.size();
+  if (tiles.empty()) return BRT_OK;
+  BRT_CUDA_TRY(cudaMalloc(&e->tiles, tiles.size() * sizeof(uint4)));
+  BRT_CUDA_TRY(cudaMalloc(&e->tileCounter, 4));
+  BRT_CUDA_TRY(cudaMemcpy(e->tiles, tiles.data(), tiles.size() * sizeof(uint4), cudaMemcpyHostToDevice));
+  e->tileBlocks = std::min<uint32_t>(e->numTiles, tileFlockBlocks(e->Mmax, e->Fs, (int)e->smCount));
+  return BRT_OK;
+}
 
 }  // namespace
 
@@ -613,6 +638,8 @@ int brt_engine_create(const brt_params* flocks, uint32_t num_flocks, int device,
   }
   rc = configureKernels(e);
   if (rc) { freeAll(e); delete e; return rc; }
+  rc = buildTiles(e);
+  if (rc) { freeAll(e); delete e; return rc; }
   BRT_CUDA_TRY(cudaStreamSynchronize(st));
   *out = e;
   return BRT_OK;
@@ -694,7 +721,7 @@ int brt_engine_set_option(brt_engine* e, const char* key, int64_t value) {
     if (value < 0 || value > 2) { setLastError("phase2_variant must be in [0, 2]"); return BRT_ERR_ARG; }
     e->phase2Variant = (int)value;
   } else if (k == "scan_variant") {
-    if (value < 0 || value > 5) { setLastError("scan_variant must be in [0, 5]"); return BRT_ERR_ARG; }
+    if (value < 0 || value > 6) { setLastError("scan_variant must be in [0, 6]"); return BRT_ERR_ARG; }
     e->scanVariant = (int)value;
   } else if (k == "incremental_sort") {
     e->resortOn = value != 0;
@@ -1060,14 +1087,23 @@ int brt_engine_autotune(brt_engine* e, float elapsedTime, uint32_t steps, char* 
           if (!rc) chk(trial(names[s][w], bs, &ms));
           if (!rc && ms < bestMs) { bestMs = ms; bestBlock = bs; bestScan = scans[s]; bestP2 = p2; }
         }
+    // the staged tile kernel (its block is fixed)
+    for (int w = 0; w < 2 && !rc; ++w) {
+      const int p2 = w == 0 ? 0 : 2;
+      if (p2 == 2 && !anyFeatures) continue;
+      chk(brt_engine_set_option(e, "scan_variant", 6));
+      chk(brt_engine_set_option(e, "phase2_variant", p2));
+      if (!rc) chk(trial(w == 0 ? "scan6/walk0" : "scan6/walk2", kTileThreads, &ms));
+      if (!rc && ms < bestMs) { bestMs = ms; bestScan = 6; bestP2 = p2; }
+    }
     if (!rc) {
       chk(brt_engine_set_option(e, "block_size", bestBlock));
       chk(brt_engine_set_option(e, "scan_variant", bestScan));
       chk(brt_engine_set_option(e, "phase2_variant", bestP2));
     }
-    // 48 and 40 only change the cooperative scan's build
+    // 48 and 40 only change the cooperative scan's build; the tile kernel has one
     const int budgets[4] = {64, 128, 48, 40};
-    const int nBudgets = bestScan >= 4 ? 4 : 2;
+    const int nBudgets = bestScan == 6 ? 0 : (bestScan >= 4 ? 4 : 2);
     bestMs = 1e30;
     for (int r = 0; r < nBudgets && !rc; ++r) {
       chk(brt_engine_set_option(e, "registers", budgets[r]));

@@ -35,6 +35,11 @@ struct brt_engine {
   // 1M-agent flock and the 1,024-flock batch.
   int phase2Variant = 2;      // option "phase2_variant": list walk shape (2: geometry, then features)
   int scanVariant = 5;        // option "scan_variant": neighbour-scan loop shape (5: warp-cooperative, windowed)
+  // scan variant 6: the (flock, row segment) tiles of the staged tile kernel
+  uint4* tiles = nullptr;
+  uint32_t numTiles = 0;
+  uint32_t* tileCounter = nullptr;
+  uint32_t tileBlocks = 0;
   uint32_t fusedBlock = 64;   // option "block_size": threads per block of the single-pass flock kernel
   int regBudget = 64;         // option "registers" (or "wide_registers"): registers a thread of that kernel
   // state

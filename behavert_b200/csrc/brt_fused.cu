@@ -21,6 +21,8 @@
 #include "brt_agent.cuh"
 #include "brt_kernels.cuh"
 
+#include <algorithm>
+
 namespace brt {
 
 // List entries are plain sorted slots; the walk recomputes each neighbour's
@@ -42,50 +44,15 @@ constexpr int kCoopCachedRounds = 3;
 // are short.  16 measured between the two.
 constexpr int kCoopWindowAgents = 8;
 
-template <int FP, int P2, int MINB, int SCAN>
-__global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs A) {
-  extern __shared__ uint32_t sList[];
-  const uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool active = i0 < A.n;
-  // The warp-cooperative scans need every lane of the warp; inactive lanes
-  // take part read-only (mirroring the last agent) and leave after it.
-  constexpr bool coop = SCAN != 0;
-  if (!coop && !active) return;
-  const uint32_t i = active ? i0 : A.n - 1;
-  const uint32_t f = A.nflocks == 1 ? 0u : flockOfSlot(A.agentBase, A.nflocks, i);
-  const FlockDev& fl = A.flocks[f];
-  const float4 p4 = __ldg(&A.posS[i]);
+// Phase 2 of the flock kernels: steering and feature sums over agent i's
+// list (list[k * ls], k < n; sorted slots in the reference's visit order),
+// then the clustering feature update and the integration of sorted slot i
+// into canonical slot i.  Shared by flockKernel and tileFlockKernel, so
+// every scan variant walks and integrates with the same code.
+template <int FP, int P2>
+__device__ __forceinline__ void flockWalk(const FusedArgs& A, uint32_t i, const float4 p4, const FlockDev& fl,
+                                          const uint32_t* list, uint32_t ls, uint32_t n) {
   const f3 p = xyz(p4);
-  const uint32_t G = fl.G;
-  const int gx = gridCoord(p.x, fl.cell, G), gy = gridCoord(p.y, fl.cell, G), gz = gridCoord(p.z, fl.cell, G);
-  const int hi = (int)G - 1;
-  const bool interior = gx > 0 && gx < hi && gy > 0 && gy < hi && gz > 0 && gz < hi;
-  const uint32_t M = fl.M;
-  uint32_t* list = sList + threadIdx.x;
-  // The cooperative scan stores 32 rows of one agent's column per vote: an
-  // odd stride puts those rows in distinct shared-memory banks.
-  const uint32_t ls = blockDim.x + (SCAN >= 4 ? 1u : 0u);
-
-  // Phase 1: the neighbour list in the reference's visit order.
-  (void)M;
-  uint32_t n;
-  if (SCAN >= 4) {
-    const uint32_t key = fl.cellBase + ((uint32_t)gz * G + (uint32_t)gy) * G + (uint32_t)gx;
-    n = scanNeighborsCooperative<kCoopCachedRounds, SCAN == 5 ? kCoopWindowAgents : 0>(active, i, p, key, A.flocks, f, A.cellStart, A.cellEnd, A.posS, sList, ls,
-                                 threadIdx.x & ~31u);
-    if (!active) return;
-  } else {
-    n = A.scanVariant == 0 ? scanNeighborsPipelined<4, true>(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls)
-      : A.scanVariant == 1 ? scanNeighborsPipelined<2, true>(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls)
-      : A.scanVariant == 2 ? scanNeighborsPipelined<4, false>(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls)
-                           : scanNeighborsFlat(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls);
-  }
-  if (A.lists) {
-    uint32_t* out = A.lists + (size_t)i * A.listStride;
-    out[0] = n;
-    for (uint32_t k = 0; k < n; ++k) out[1 + k] = list[k * ls];
-  }
-
   // Phase 2: steering and feature sums over the list, in list order.
   const float4 w4 = __ldg(&A.fwdS[i]);
   const float4 a4 = __ldg(&A.accS[i]);
@@ -112,7 +79,6 @@ __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs 
   f3 sSep = mk3(0.f, 0.f, 0.f), sAli = mk3(0.f, 0.f, 0.f), sCoh = mk3(0.f, 0.f, 0.f);
   uint32_t cSep = 0, cAli = 0, cCoh = 0;
   const AgentCtx a = makeCtx(p4, w4, fl);
-  (void)interior;
   // One listed neighbour: its image position, forward and features are
   // loaded by the caller so that several neighbours' loads can be in flight.
   auto visitGeom = [&](const float4 q4, const float4 wj) {
@@ -254,6 +220,253 @@ __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs 
   A.idA[i] = __ldg(&A.idS[i]);
 }
 
+template <int FP, int P2, int MINB, int SCAN>
+__global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs A) {
+  extern __shared__ uint32_t sList[];
+  const uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = i0 < A.n;
+  // The warp-cooperative scans need every lane of the warp; inactive lanes
+  // take part read-only (mirroring the last agent) and leave after it.
+  constexpr bool coop = SCAN != 0;
+  if (!coop && !active) return;
+  const uint32_t i = active ? i0 : A.n - 1;
+  const uint32_t f = A.nflocks == 1 ? 0u : flockOfSlot(A.agentBase, A.nflocks, i);
+  const FlockDev& fl = A.flocks[f];
+  const float4 p4 = __ldg(&A.posS[i]);
+  const f3 p = xyz(p4);
+  const uint32_t G = fl.G;
+  const int gx = gridCoord(p.x, fl.cell, G), gy = gridCoord(p.y, fl.cell, G), gz = gridCoord(p.z, fl.cell, G);
+  const uint32_t M = fl.M;
+  uint32_t* list = sList + threadIdx.x;
+  // The cooperative scan stores 32 rows of one agent's column per vote: an
+  // odd stride puts those rows in distinct shared-memory banks.
+  const uint32_t ls = blockDim.x + (SCAN >= 4 ? 1u : 0u);
+
+  // Phase 1: the neighbour list in the reference's visit order.
+  (void)M;
+  uint32_t n;
+  if (SCAN >= 4) {
+    const uint32_t key = fl.cellBase + ((uint32_t)gz * G + (uint32_t)gy) * G + (uint32_t)gx;
+    n = scanNeighborsCooperative<kCoopCachedRounds, SCAN == 5 ? kCoopWindowAgents : 0>(active, i, p, key, A.flocks, f, A.cellStart, A.cellEnd, A.posS, sList, ls,
+                                 threadIdx.x & ~31u);
+    if (!active) return;
+  } else {
+    n = A.scanVariant == 0 ? scanNeighborsPipelined<4, true>(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls)
+      : A.scanVariant == 1 ? scanNeighborsPipelined<2, true>(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls)
+      : A.scanVariant == 2 ? scanNeighborsPipelined<4, false>(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls)
+                           : scanNeighborsFlat(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls);
+  }
+  if (A.lists) {
+    uint32_t* out = A.lists + (size_t)i * A.listStride;
+    out[0] = n;
+    for (uint32_t k = 0; k < n; ++k) out[1 + k] = list[k * ls];
+  }
+
+  flockWalk<FP, P2>(A, i, p4, fl, list, ls, n);
+}
+
+// Exclusive scan of one value per thread across a kTileThreads block.
+__device__ __forceinline__ uint32_t ctaExclusiveScanTile(uint32_t v, uint32_t* sWarp, uint32_t* total) {
+  constexpr uint32_t WARPS = kTileThreads / 32;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= (uint32_t)o) x += y;
+  }
+  if (lane == 31) sWarp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t w = lane < WARPS ? sWarp[lane] : 0u;
+    uint32_t wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= (uint32_t)o) wi += y;
+    }
+    if (lane < WARPS) sWarp[lane] = wi - w;
+    if (lane == WARPS - 1) sWarp[WARPS] = wi;
+  }
+  __syncthreads();
+  const uint32_t r = sWarp[warp] + x - v;
+  *total = sWarp[WARPS];
+  __syncthreads();
+  return r;
+}
+
+// ---------------------------------------------------------------------------
+// Scan variant 6: a persistent work queue over (flock, row segment) tiles.
+//
+// A tile is up to kTileMaxCells consecutive home cells of one x-row of one
+// flock; its agents are one contiguous range of sorted slots.  A block takes
+// tiles from an atomic counter, stages the positions of the tile's
+// 9 x (cells + 2) neighbour cells (the union of its agents' 27-cell
+// neighbourhoods, each cell once) in shared memory, then every thread scans
+// its own agent's 27 cells in the reference's visit order out of shared
+// memory: a candidate is loaded from global memory once per tile instead of
+// once per home cell.  The list is the same as every other scan's (same
+// candidates, same order, same test).  A tile whose neighbourhood holds more
+// than kTileStage candidates (dense blobs) is scanned by the warp-cooperative
+// scan from global memory instead.  Phase 2 is flockWalk, as for flockKernel.
+constexpr uint32_t kTileTable = 9 * (kTileMaxCells + 2);
+constexpr uint32_t kTileStage = 1024;
+
+// Agent `self`'s list from the staged tile: sCnt / sOff per table entry
+// e = ((oy + 1) * 3 + (oz + 1)) * W + column, column = gx - x0 + 1 + ox.
+__device__ __forceinline__ uint32_t scanTileStaged(uint32_t self, f3 p, int gx, int gy, int gz, uint32_t x0, uint32_t W,
+                                                   const FlockDev& fl, const float4* sStage, const uint32_t* sOff,
+                                                   const uint32_t* sCnt, uint32_t* list, uint32_t ls) {
+  const uint32_t M = fl.M;
+  const float thr = fl.r2thr;
+  uint32_t n = 0;
+  for (int ox = -1; ox <= 1; ++ox) {
+    const uint32_t col = (uint32_t)(gx - (int)x0 + 1 + ox);
+    const float sx = imageShift(gx, ox, fl.G, fl.L);
+    for (int oy = -1; oy <= 1; ++oy) {
+      const float sy = imageShift(gy, oy, fl.G, fl.L);
+      for (int oz = -1; oz <= 1; ++oz) {
+        const float sz = imageShift(gz, oz, fl.G, fl.L);
+        const uint32_t e = (uint32_t)((oy + 1) * 3 + (oz + 1)) * W + col;
+        const uint32_t cnt = sCnt[e], base = sOff[e];
+        for (uint32_t k = 0; k < cnt; ++k) {
+          const float4 q = sStage[base + k];
+          const uint32_t slot = __float_as_uint(q.w);
+          const float dx = (q.x + sx) - p.x, dy = (q.y + sy) - p.y, dz = (q.z + sz) - p.z;
+          const float d2 = dx * dx + dy * dy + dz * dz;
+          if (!(d2 > thr) && slot != self) {
+            list[(n++) * ls] = slot;
+            if (n == M) return n;
+          }
+        }
+      }
+    }
+  }
+  return n;
+}
+
+template <int FP, int P2>
+__global__ void __launch_bounds__(kTileThreads, 4) tileFlockKernel(FusedArgs A) {
+  extern __shared__ uint32_t sList[];  // (kTileThreads + 1) * Mmax words, a column per thread
+  __shared__ float4 sStage[kTileStage];
+  __shared__ uint32_t sOff[kTileTable], sCnt[kTileTable], sBeg[kTileTable];
+  __shared__ uint32_t sScan[kTileThreads / 32 + 1];
+  __shared__ uint32_t sTile, sLo, sHi, sStaged, sStagedEntries;
+  constexpr uint32_t kPer = (kTileTable + kTileThreads - 1) / kTileThreads;  // table entries a thread counts
+  const uint32_t tid = threadIdx.x, lane = tid & 31u;
+  const uint32_t ls = kTileThreads + 1;
+  for (;;) {
+    if (tid == 0) sTile = atomicAdd(A.tileCounter, 1u);
+    __syncthreads();
+    const uint32_t t = sTile;
+    if (t >= A.numTiles) return;
+    const uint4 d = __ldg(&A.tiles[t]);
+    const uint32_t f = d.x, ty = d.y & 0xFFFFu, tz = d.y >> 16, x0 = d.z & 0xFFFFu, R = d.z >> 16;
+    const FlockDev& fl = A.flocks[f];
+    const uint32_t G = fl.G;
+    const uint32_t W = R + 2;
+    // the tile's slot range [lo, hi): its home cells' ranges are consecutive
+    if (tid < 32) {
+      uint32_t lo = 0xFFFFFFFFu, hi = 0u;
+      if (lane < R) {
+        const uint32_t h = fl.cellBase + (tz * G + ty) * G + x0 + lane;
+        const uint32_t st = __ldg(&A.cellStart[h]), en = __ldg(&A.cellEnd[h]);
+        if (usableRange(fl, st, en)) { lo = st; hi = en; }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, o));
+        hi = max(hi, __shfl_xor_sync(0xFFFFFFFFu, hi, o));
+      }
+      if (lane == 0) { sLo = lo; sHi = hi; }
+    }
+    // the table: counts in table order, their exclusive prefix, staged flags
+    uint32_t cnt[kPer], beg[kPer];
+    uint32_t mine = 0;
+#pragma unroll
+    for (uint32_t r = 0; r < kPer; ++r) {
+      const uint32_t e = tid * kPer + r;
+      cnt[r] = 0;
+      beg[r] = 0;
+      if (e < 9 * W) {
+        const uint32_t row = e / W, col = e - row * W;
+        const int oy = (int)(row / 3) - 1, oz = (int)(row % 3) - 1;
+        const int cx = wrapCoord((int)x0 - 1 + (int)col, G), cy = wrapCoord((int)ty + oy, G), cz = wrapCoord((int)tz + oz, G);
+        const uint32_t h = fl.cellBase + ((uint32_t)cz * G + (uint32_t)cy) * G + (uint32_t)cx;
+        const uint32_t st = __ldg(&A.cellStart[h]);
+        uint32_t en = __ldg(&A.cellEnd[h]);
+        if (usableRange(fl, st, en)) {
+          if (fl.maxPerCell && en - st > fl.maxPerCell) en = st + fl.maxPerCell;
+          cnt[r] = en - st;
+          beg[r] = st;
+        }
+      }
+      mine += cnt[r];
+    }
+    uint32_t total;
+    uint32_t off = ctaExclusiveScanTile(mine, sScan, &total);
+#pragma unroll
+    for (uint32_t r = 0; r < kPer; ++r) {
+      const uint32_t e = tid * kPer + r;
+      if (e < kTileTable) {
+        sOff[e] = off;
+        sCnt[e] = cnt[r];
+        sBeg[e] = beg[r];
+      }
+      off += cnt[r];
+    }
+    if (tid == 0) sStaged = total <= kTileStage ? total : 0xFFFFFFFFu;
+    __syncthreads();
+    const uint32_t lo = sLo, hi = sHi;
+    const bool staged = sStaged != 0xFFFFFFFFu;
+    if (lo < hi && staged) {
+      // copy the candidates: entry of q by binary search on the offsets
+      const uint32_t entries = 9 * W;
+      for (uint32_t q = tid; q < total; q += kTileThreads) {
+        uint32_t a = 0, b = entries;  // last entry with sOff <= q
+        while (b - a > 1) {
+          const uint32_t m = (a + b) >> 1;
+          if (sOff[m] <= q) a = m; else b = m;
+        }
+        const uint32_t slot = sBeg[a] + (q - sOff[a]);
+        const float4 v = __ldg(&A.posS[slot]);
+        sStage[q] = make_float4(v.x, v.y, v.z, __uint_as_float(slot));
+      }
+    }
+    __syncthreads();
+    for (uint32_t base = lo; base < hi; base += kTileThreads) {
+      const uint32_t i0 = base + tid;
+      const bool active = i0 < hi;
+      const uint32_t i = active ? i0 : hi - 1;  // inactive lanes mirror the last agent (read-only)
+      const float4 p4 = __ldg(&A.posS[i]);
+      const f3 p = xyz(p4);
+      const int gx = gridCoord(p.x, fl.cell, G), gy = gridCoord(p.y, fl.cell, G), gz = gridCoord(p.z, fl.cell, G);
+      uint32_t n = 0;
+      if (staged) {
+        // an agent outside the tile's cells only follows a corrupted step
+        // (reported by the device error word): no list, no read past the table
+        const bool inTile = gx >= (int)x0 && gx < (int)(x0 + R) && gy == (int)ty && gz == (int)tz;
+        if (active && inTile) n = scanTileStaged(i, p, gx, gy, gz, x0, W, fl, sStage, sOff, sCnt, sList + tid, ls);
+      } else {
+        const uint32_t key = fl.cellBase + ((uint32_t)gz * G + (uint32_t)gy) * G + (uint32_t)gx;
+        n = scanNeighborsCooperative<kCoopCachedRounds, kCoopWindowAgents>(active, i, p, key, A.flocks, f, A.cellStart,
+                                                                            A.cellEnd, A.posS, sList, ls, tid & ~31u);
+      }
+      if (active) {
+        uint32_t* list = sList + tid;
+        if (A.lists) {
+          uint32_t* out = A.lists + (size_t)i * A.listStride;
+          out[0] = n;
+          for (uint32_t k = 0; k < n; ++k) out[1 + k] = list[k * ls];
+        }
+        flockWalk<FP, P2>(A, i, p4, fl, list, ls, n);
+      }
+      __syncwarp();
+    }
+    __syncthreads();  // the next tile reuses the staging and the table
+  }
+}
+
 namespace {
 template <int FP, int SCAN>
 void launchFlockScan(const FusedArgs& A, uint32_t blocks, uint32_t block, size_t smem, int phase2, int regs,
@@ -324,8 +537,51 @@ cudaError_t configureFlockFP(int smem) {
 // in [32, 256].  regs: the register budget a thread is compiled for, 128 (2
 // resident 256-thread blocks per SM), 64 (4 blocks), or for the cooperative
 // scan also 48 and 40 (5 and 6 blocks, more resident warps for some spills).
+namespace {
+template <int FP>
+cudaError_t launchTileFP(const FusedArgs& A, int phase2, cudaStream_t st) {
+  const size_t smem = (size_t)(kTileThreads + 1) * A.Mmax * 4;
+  cudaError_t e = cudaMemsetAsync(A.tileCounter, 0, 4, st);
+  if (e != cudaSuccess) return e;
+  if (FP > 0 && phase2 == 2) tileFlockKernel<FP, 2><<<A.tileBlocks, kTileThreads, smem, st>>>(A);
+  else tileFlockKernel<FP, 0><<<A.tileBlocks, kTileThreads, smem, st>>>(A);
+  return cudaGetLastError();
+}
+template <int FP>
+cudaError_t configureTileFP(int smem) {
+  cudaError_t e = cudaFuncSetAttribute(tileFlockKernel<FP, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e == cudaSuccess && FP > 0)
+    e = cudaFuncSetAttribute(tileFlockKernel<FP, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  return e;
+}
+}  // namespace
+
+// Persistent blocks of the tile kernel a launch should start: the resident
+// blocks per SM (shared memory bounds them) times the SMs.
+uint32_t tileFlockBlocks(uint32_t Mmax, uint32_t Fs, int smCount) {
+  const size_t smem = (size_t)(kTileThreads + 1) * Mmax * 4;
+  int per = 0;
+  cudaError_t e;
+  if (Fs == 0) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, tileFlockKernel<0, 0>, kTileThreads, smem);
+  else if (Fs <= 4) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, tileFlockKernel<4, 2>, kTileThreads, smem);
+  else if (Fs <= 8) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, tileFlockKernel<8, 2>, kTileThreads, smem);
+  else if (Fs <= 16) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, tileFlockKernel<16, 2>, kTileThreads, smem);
+  else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, tileFlockKernel<32, 2>, kTileThreads, smem);
+  if (e != cudaSuccess || per < 1) per = 1;
+  return (uint32_t)(per * std::max(1, smCount));
+}
+
 cudaError_t launchFlock(const FusedArgs& A, int phase2, uint32_t block, int regs, cudaStream_t st) {
   if (A.n == 0) return cudaSuccess;
+  if (A.scanVariant == 6) {
+    if (!A.tiles || !A.tileCounter || A.tileBlocks == 0) return cudaErrorInvalidValue;
+    const uint32_t fp = A.Fs;
+    if (fp == 0) return launchTileFP<0>(A, phase2, st);
+    if (fp <= 4) return launchTileFP<4>(A, phase2, st);
+    if (fp <= 8) return launchTileFP<8>(A, phase2, st);
+    if (fp <= 16) return launchTileFP<16>(A, phase2, st);
+    return launchTileFP<32>(A, phase2, st);
+  }
   if (block < 32 || block > kFlockMaxThreads || block % 32) return cudaErrorInvalidValue;
   const uint32_t blocks = (A.n + block - 1) / block;
   const uint32_t fp = A.Fs;
@@ -344,7 +600,13 @@ cudaError_t configureFlockKernels(uint32_t Mmax) {
   if ((e = configureFlockFP<4>(smem))) return e;
   if ((e = configureFlockFP<8>(smem))) return e;
   if ((e = configureFlockFP<16>(smem))) return e;
-  return configureFlockFP<32>(smem);
+  if ((e = configureFlockFP<32>(smem))) return e;
+  const int tsmem = (int)((size_t)(kTileThreads + 1) * Mmax * 4);
+  if ((e = configureTileFP<0>(tsmem))) return e;
+  if ((e = configureTileFP<4>(tsmem))) return e;
+  if ((e = configureTileFP<8>(tsmem))) return e;
+  if ((e = configureTileFP<16>(tsmem))) return e;
+  return configureTileFP<32>(tsmem);
 }
 
 }  // namespace brt

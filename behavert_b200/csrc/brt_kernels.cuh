@@ -61,9 +61,18 @@ struct FusedArgs {
   uint32_t nflocks, n, Mmax, Fs;
   float dt;
   int scanVariant;             // 0: pipelined x4 + cell culling, 1: x2 + culling, 2: x4, 3: flat loop,
-                               // 4: warp-cooperative, 5: warp-cooperative with windows
+                               // 4: warp-cooperative, 5: warp-cooperative with windows,
+                               // 6: staged tiles (tileFlockKernel)
   const uint32_t* stepCounter; // random-stream step of the Schooling move
+  // scan variant 6: the (flock, row segment) tiles and the work-queue counter
+  const uint4* tiles;          // x flock, y row y | z << 16, z first x | cells << 16
+  uint32_t numTiles;
+  uint32_t* tileCounter;       // zeroed before each launch
+  uint32_t tileBlocks;         // persistent blocks of the launch
 };
+// Home cells per tile (one row segment) and staged candidates per tile.
+constexpr uint32_t kTileMaxCells = 32;
+constexpr uint32_t kTileThreads = 128;
 
 struct StageArgs {
   const float4* posS; const float4* fwdS; const float4* accS;
@@ -200,6 +209,7 @@ cudaError_t launchHash(const HashArgs& A, uint32_t maxBlocks, cudaStream_t st);
 cudaError_t launchReorder(const ReorderArgs& A, cudaStream_t st);
 cudaError_t launchFused(const FusedArgs& A, bool knn, cudaStream_t st);
 cudaError_t launchFlock(const FusedArgs& A, int phase2, uint32_t block, int regs, cudaStream_t st);
+uint32_t tileFlockBlocks(uint32_t Mmax, uint32_t Fs, int smCount);
 cudaError_t launchLists(const StageArgs& A, bool knn, cudaStream_t st);
 cudaError_t launchSteerStage(const StageArgs& A, int which, cudaStream_t st);
 cudaError_t launchIntegrateStage(const StageArgs& A, float dt, cudaStream_t st);

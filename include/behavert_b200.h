@@ -189,14 +189,19 @@ int brt_engine_set_params(brt_engine* e, uint32_t flock, const brt_params* p);
                               when the single-pass kernel applies (default 0)
      "block_size"       32..256, multiple of 32: threads per block of the
                               single-pass flock kernel (default 64)
-     "scan_variant"     0..5  neighbour-scan loop: 0 four candidates in flight
+     "scan_variant"     0..6  neighbour-scan loop: 0 four candidates in flight
                               with exact cell culling, 1 two in flight with
                               culling, 2 four without culling, 3 one at a time,
                               4 warp-cooperative (a warp tests 32 candidates of
                               a home cell's neighbourhood per step, the first
                               96 held in registers), 5 as 4, with further
                               96-candidate windows while 8 or more of a home
-                              cell's agents still need neighbours (default)
+                              cell's agents still need neighbours (default),
+                              6 a persistent work queue over (flock, row
+                              segment) tiles: each block stages a tile's
+                              neighbour cells in shared memory once and every
+                              thread scans its agent's 27 cells from there
+                              (dense tiles that do not fit take scan 5)
      "phase2_variant"   0..2  list walk: 0 one neighbour at a time, 1 two at a
                               time (per-agent scans 0..3 only), 2 (default)
                               two walks, geometry then feature sums (with

@@ -38,11 +38,14 @@ def _variant_workloads():
     flat = workloads.plain(n=3000, L=32.0, steps=2)
     flat.params[0].use2DProjection = 1
     odd = workloads.plain(n=1000, L=32.0, steps=2)          # not a multiple of the warp size
-    return {"large": big, "batched": bat, "cap": cap, "seam": seam, "2d": flat, "odd": odd}
+    # dense rows: the staged tile kernel's neighbourhood overflows its shared
+    # memory in some tiles and not in others
+    dense = workloads.large(n=1 << 15, L=48.0, blobs=3, blob_fraction=0.6, steps=2)
+    return {"large": big, "batched": bat, "cap": cap, "seam": seam, "2d": flat, "odd": odd, "dense": dense}
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5])
-@pytest.mark.parametrize("name", ["large", "batched", "cap", "seam", "2d", "odd"])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("name", ["large", "batched", "cap", "seam", "2d", "odd", "dense"])
 def test_scan_variants_are_bit_identical(name, variant):
     wl = _variant_workloads()[name]
 
@@ -66,7 +69,7 @@ def test_scan_variants_are_bit_identical(name, variant):
             assert np.array_equal(a, b)
 
 
-@pytest.mark.parametrize("scan,phase2", [(0, 1), (4, 2), (4, 1), (5, 2)])
+@pytest.mark.parametrize("scan,phase2", [(0, 1), (4, 2), (4, 1), (5, 2), (6, 2)])
 @pytest.mark.parametrize("name", ["large", "batched", "seam"])
 def test_list_walk_variants_are_bit_identical(name, scan, phase2):
     wl = _variant_workloads()[name]
