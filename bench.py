@@ -524,6 +524,8 @@ def main():
                     help="run W warm-up + this many single steps and exit (for ncu)")
     ap.add_argument("--profile-adjoint", type=int, default=0,
                     help="run this many config-3 adjoint iterations (taped forward + backward) and exit (for ncu)")
+    ap.add_argument("--profile-fit", type=int, default=0,
+                    help="run this many config-4 adjoint iterations (taped forward + backward) and exit (for ncu)")
     ap.add_argument("--profile-flocks", type=int, default=0,
                     help="with --profile-steps: step the config-2 batched workload cut to this many flocks")
     ap.add_argument("--options", default="",
@@ -554,6 +556,17 @@ def main():
             for _ in range(args.profile_adjoint):
                 eng.set_state(a.pos, a.fwd, a.acc)
                 eng.adjoint_forward(target, a.steps, a.meta["checkpoint_every"], a.dt)
+                eng.adjoint_backward()
+        return 0
+
+    if args.profile_fit:
+        fw = workloads.fitting()
+        with Engine(fw.params, device=local) as eng:
+            target = np.zeros((fw.num_agents, 4), np.float32)
+            target[:, :3] = fw.pos[:, :3]
+            for _ in range(args.profile_fit):
+                eng.set_state(fw.pos, fw.fwd, fw.acc)
+                eng.adjoint_forward(target, fw.steps, 10, fw.dt)
                 eng.adjoint_backward()
         return 0
 
