@@ -254,17 +254,37 @@ __device__ __forceinline__ uint32_t scanNeighborsPipelined(uint32_t self, f3 p, 
 // open; rounds after that go round-major as with R = 0.  Each agent's list
 // gets the same candidates in the same order either way.
 //
+// With CULL, candidates are first tested against the run's bounding box (the
+// smallest box holding the run's agents): a candidate whose squared distance
+// to the box exceeds the radius threshold fails every agent's test, and is
+// dropped before the votes.  The squared box distance is built like an
+// agent's d2, (ex * ex + ey * ey) + ez * ez with ex = max(lo - q, q - hi, 0),
+// and rounding is monotone, so it is never above any agent's d2: no
+// candidate an agent accepts is dropped.  The survivors keep their order in
+// a per-warp staging buffer cbuf ((R + 1) * 32 entries: x, y, z with the
+// image shift, slot in w) and are voted on R rounds at a time, agent-major.
+// The lists are the same as without culling.
+//
 // Called by all 32 lanes of a warp; `active` lanes own an agent (sorted slot
 // `self`, position p, home cell key `key`, flock `flock`).  Each agent's list
 // goes to column laneCol0 + lane of the shared array sList (stride ls).
 // Returns the lane's list length.
-template <int R, int WINT = 0>
+__device__ __forceinline__ uint32_t orderedBits(float x) {
+  const uint32_t u = __float_as_uint(x);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float fromOrderedBits(uint32_t u) {
+  return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u);
+}
+
+template <int R, int WINT = 0, bool CULL = false>
 __device__ __forceinline__ uint32_t scanNeighborsCooperative(bool active, uint32_t self, f3 p, uint32_t key,
                                                              const FlockDev* __restrict__ flocks, uint32_t flock,
                                                              const uint32_t* __restrict__ cellStart,
                                                              const uint32_t* __restrict__ cellEnd,
                                                              const float4* __restrict__ posS, uint32_t* sList,
-                                                             uint32_t ls, uint32_t laneCol0) {
+                                                             uint32_t ls, uint32_t laneCol0, float4* cbuf = nullptr) {
+  static_assert(!CULL || R > 0, "the culled scan votes on register-held rounds");
   const uint32_t full = 0xFFFFFFFFu;
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t myKey = active ? key : 0xFFFFFFFFu;
@@ -273,6 +293,19 @@ __device__ __forceinline__ uint32_t scanNeighborsCooperative(bool active, uint32
   uint32_t heads = __ballot_sync(full, head);
   const uint32_t activeMask = __ballot_sync(full, active);
   uint32_t n = 0;
+  // bounding box of the lane's run: lanes of equal key (a run, or with a
+  // corrupted order a superset of it, which only culls less)
+  float bLo[3] = {0.f, 0.f, 0.f}, bHi[3] = {0.f, 0.f, 0.f};
+  if constexpr (CULL) {
+    const uint32_t grp = __match_any_sync(full, myKey);
+    const uint32_t ox = orderedBits(p.x), oy = orderedBits(p.y), oz = orderedBits(p.z);
+    bLo[0] = fromOrderedBits(__reduce_min_sync(grp, ox));
+    bLo[1] = fromOrderedBits(__reduce_min_sync(grp, oy));
+    bLo[2] = fromOrderedBits(__reduce_min_sync(grp, oz));
+    bHi[0] = fromOrderedBits(__reduce_max_sync(grp, ox));
+    bHi[1] = fromOrderedBits(__reduce_max_sync(grp, oy));
+    bHi[2] = fromOrderedBits(__reduce_max_sync(grp, oz));
+  }
   while (heads) {
     const uint32_t g0 = __ffs(heads) - 1;
     heads &= heads - 1;
@@ -315,6 +348,97 @@ __device__ __forceinline__ uint32_t scanNeighborsCooperative(bool active, uint32
     const uint32_t total = __shfl_sync(full, incl, 31);
     uint32_t open = groupMask;  // group agents whose list is not full yet
     uint32_t base0 = 0;
+    if constexpr (CULL) {
+      constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
+      const uint32_t below = (1u << lane) - 1u;
+      const float lx = __shfl_sync(full, bLo[0], g0), ly = __shfl_sync(full, bLo[1], g0), lz = __shfl_sync(full, bLo[2], g0);
+      const float hx = __shfl_sync(full, bHi[0], g0), hy = __shfl_sync(full, bHi[1], g0), hz = __shfl_sync(full, bHi[2], g0);
+      uint32_t raw = 0;       // next candidate of the run's sequence to test against the box
+      uint32_t buffered = 0;  // survivors staged in cbuf[0, buffered), in sequence order
+      for (;;) {
+        // stage survivors until R rounds' worth are buffered (at most
+        // R * 32 - 1 + 32 entries: the buffer holds (R + 1) * 32)
+        while (buffered < (uint32_t)R * 32u && raw < total) {
+          const uint32_t t = raw + lane;
+          uint32_t c = 0;
+#pragma unroll
+          for (int step = 16; step > 0; step >>= 1) {
+            const uint32_t cand = c + (uint32_t)step;
+            const uint32_t e = __shfl_sync(full, excl, cand & 31u);
+            if (cand < 27u && e <= t) c = cand;
+          }
+          const uint32_t cStart = __shfl_sync(full, segStart, c), cExcl = __shfl_sync(full, excl, c);
+          const float csx = __shfl_sync(full, sx, c), csy = __shfl_sync(full, sy, c), csz = __shfl_sync(full, sz, c);
+          bool keep = false;
+          float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (t < total) {
+            const uint32_t slot = cStart + (t - cExcl);
+            const float4 q = __ldg(&posS[slot]);
+            v = make_float4(q.x + csx, q.y + csy, q.z + csz, __uint_as_float(slot));
+            const float ex = fmaxf(fmaxf(lx - v.x, v.x - hx), 0.0f);
+            const float ey = fmaxf(fmaxf(ly - v.y, v.y - hy), 0.0f);
+            const float ez = fmaxf(fmaxf(lz - v.z, v.z - hz), 0.0f);
+            const float b2 = ex * ex + ey * ey + ez * ez;
+            keep = !(b2 > thr);
+          }
+          const uint32_t bal = __ballot_sync(full, keep);
+          if (keep) cbuf[buffered + (uint32_t)__popc(bal & below)] = v;
+          buffered += (uint32_t)__popc(bal);
+          raw += 32u;
+        }
+        __syncwarp();
+        const uint32_t take = min(buffered, (uint32_t)R * 32u);
+        float cqx[R], cqy[R], cqz[R];
+        uint32_t cslot[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const uint32_t idx = (uint32_t)r * 32u + lane;
+          cqx[r] = cqy[r] = cqz[r] = 0.0f;
+          cslot[r] = kNoSlot;
+          if (idx < take) {
+            const float4 v = cbuf[idx];
+            cqx[r] = v.x;
+            cqy[r] = v.y;
+            cqz[r] = v.z;
+            cslot[r] = __float_as_uint(v.w);
+          }
+        }
+        __syncwarp();
+        // the (at most 31) survivors past R rounds move to the front; when
+        // there are any, take = R * 32 >= 32, so no lane reads an entry
+        // another lane writes
+        const uint32_t rest = buffered - take;
+        if (lane < rest) cbuf[lane] = cbuf[take + lane];
+        buffered = rest;
+        for (uint32_t todo = open; todo; todo &= todo - 1u) {
+          const uint32_t a = __ffs(todo) - 1u;
+          const float ax = __shfl_sync(full, p.x, a), ay = __shfl_sync(full, p.y, a), az = __shfl_sync(full, p.z, a);
+          const uint32_t aSelf = __shfl_sync(full, self, a);
+          uint32_t an = __shfl_sync(full, n, a);
+          uint32_t* col = sList + laneCol0 + a;
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            if ((uint32_t)r * 32u >= take) break;
+            const float dx = cqx[r] - ax, dy = cqy[r] - ay, dz = cqz[r] - az;
+            const float d2 = dx * dx + dy * dy + dz * dz;
+            const bool acc = cslot[r] != kNoSlot && !(d2 > thr) && cslot[r] != aSelf;
+            const uint32_t bal = __ballot_sync(full, acc);
+            if (acc) {
+              const uint32_t pos = an + (uint32_t)__popc(bal & below);
+              if (pos < M) col[pos * ls] = cslot[r];
+            }
+            an += (uint32_t)__popc(bal);
+            if (an >= M) break;
+          }
+          an = min(an, M);
+          if (lane == a) n = an;
+          if (an >= M) open &= ~(1u << a);
+        }
+        __syncwarp();
+        if (!open || (raw >= total && buffered == 0)) break;
+      }
+      continue;  // the next run
+    }
     if constexpr (R > 0) {
       constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
       const uint32_t below = (1u << lane) - 1u;

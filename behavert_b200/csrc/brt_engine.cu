@@ -721,7 +721,7 @@ int brt_engine_set_option(brt_engine* e, const char* key, int64_t value) {
     if (value < 0 || value > 2) { setLastError("phase2_variant must be in [0, 2]"); return BRT_ERR_ARG; }
     e->phase2Variant = (int)value;
   } else if (k == "scan_variant") {
-    if (value < 0 || value > 6) { setLastError("scan_variant must be in [0, 6]"); return BRT_ERR_ARG; }
+    if (value < 0 || value > 7) { setLastError("scan_variant must be in [0, 7]"); return BRT_ERR_ARG; }
     e->scanVariant = (int)value;
   } else if (k == "incremental_sort") {
     e->resortOn = value != 0;
@@ -1068,16 +1068,18 @@ int brt_engine_autotune(brt_engine* e, float elapsedTime, uint32_t steps, char* 
     // per-agent scans, walk 2 (geometry, then feature sums) for the
     // cooperative scan of flocks with features.
     const uint32_t blocks[3] = {64, 128, 256};
-    // per agent with / without cell culling, warp-cooperative, cooperative with windows
-    const int scans[4] = {0, 2, 4, 5};
-    const char* names[4][2] = {{"block_size/scan0/walk0", "block_size/scan0/walk1"},
+    // per agent with / without cell culling, warp-cooperative, cooperative
+    // with windows, cooperative with bounding-box culling
+    const int scans[5] = {0, 2, 4, 5, 7};
+    const char* names[5][2] = {{"block_size/scan0/walk0", "block_size/scan0/walk1"},
                                {"block_size/scan2/walk0", "block_size/scan2/walk1"},
                                {"block_size/scan4/walk0", "block_size/scan4/walk2"},
-                               {"block_size/scan5/walk0", "block_size/scan5/walk2"}};
+                               {"block_size/scan5/walk0", "block_size/scan5/walk2"},
+                               {"block_size/scan7/walk0", "block_size/scan7/walk2"}};
     bool anyFeatures = false;
     for (const FlockDev& d : e->flocksHost) anyFeatures = anyFeatures || (d.F > 0 && d.relax != 0.0f);
     for (uint32_t bs : blocks)
-      for (int s = 0; s < 4 && !rc; ++s)
+      for (int s = 0; s < 5 && !rc; ++s)
         for (int w = 0; w < 2 && !rc; ++w) {
           const int p2 = w == 0 ? 0 : (scans[s] >= 4 ? 2 : 1);
           if (p2 == 2 && !anyFeatures) continue;

@@ -43,6 +43,15 @@ constexpr int kCoopCachedRounds = 3;
 // faster on config 1, 1% slower on the uniform batched workload, where runs
 // are short.  16 measured between the two.
 constexpr int kCoopWindowAgents = 8;
+// Scan 7 (the cooperative scan with bounding-box culling) stages each run's
+// surviving candidates in shared memory after the lists: (R + 1) rounds of
+// float4 per warp, from a 16-byte aligned word offset.
+constexpr uint32_t kCullBufPerWarp = (kCoopCachedRounds + 1) * 32;
+__host__ __device__ constexpr uint32_t cullBufOffsetWords(uint32_t ls, uint32_t Mmax) { return (ls * Mmax + 3u) & ~3u; }
+__host__ __device__ constexpr size_t flockSmemBytes(uint32_t block, uint32_t Mmax, int scan) {
+  return scan == 7 ? (size_t)cullBufOffsetWords(block + 1, Mmax) * 4 + (size_t)(block / 32) * kCullBufPerWarp * 16
+                   : (size_t)(block + (scan >= 4 ? 1u : 0u)) * Mmax * 4;
+}
 
 // Phase 2 of the flock kernels: steering and feature sums over agent i's
 // list (list[k * ls], k < n; sorted slots in the reference's visit order),
@@ -222,7 +231,7 @@ __device__ __forceinline__ void flockWalk(const FusedArgs& A, uint32_t i, const 
 
 template <int FP, int P2, int MINB, int SCAN>
 __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs A) {
-  extern __shared__ uint32_t sList[];
+  extern __shared__ __align__(16) uint32_t sList[];
   const uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = i0 < A.n;
   // The warp-cooperative scans need every lane of the warp; inactive lanes
@@ -247,8 +256,14 @@ __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs 
   uint32_t n;
   if (SCAN >= 4) {
     const uint32_t key = fl.cellBase + ((uint32_t)gz * G + (uint32_t)gy) * G + (uint32_t)gx;
-    n = scanNeighborsCooperative<kCoopCachedRounds, SCAN == 5 ? kCoopWindowAgents : 0>(active, i, p, key, A.flocks, f, A.cellStart, A.cellEnd, A.posS, sList, ls,
-                                 threadIdx.x & ~31u);
+    if constexpr (SCAN == 7) {
+      float4* cbuf = reinterpret_cast<float4*>(sList + cullBufOffsetWords(ls, A.Mmax)) + (threadIdx.x >> 5) * kCullBufPerWarp;
+      n = scanNeighborsCooperative<kCoopCachedRounds, 0, true>(active, i, p, key, A.flocks, f, A.cellStart, A.cellEnd,
+                                                               A.posS, sList, ls, threadIdx.x & ~31u, cbuf);
+    } else {
+      n = scanNeighborsCooperative<kCoopCachedRounds, SCAN == 5 ? kCoopWindowAgents : 0>(
+          active, i, p, key, A.flocks, f, A.cellStart, A.cellEnd, A.posS, sList, ls, threadIdx.x & ~31u);
+    }
     if (!active) return;
   } else {
     n = A.scanVariant == 0 ? scanNeighborsPipelined<4, true>(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls)
@@ -351,7 +366,7 @@ __global__ void __launch_bounds__(kTileThreads, 4) tileFlockKernel(FusedArgs A) 
   __shared__ float4 sStage[kTileStage];
   __shared__ uint32_t sOff[kTileTable], sCnt[kTileTable], sBeg[kTileTable];
   __shared__ uint32_t sScan[kTileThreads / 32 + 1];
-  __shared__ uint32_t sTile, sLo, sHi, sStaged, sStagedEntries;
+  __shared__ uint32_t sTile, sLo, sHi, sStaged;
   constexpr uint32_t kPer = (kTileTable + kTileThreads - 1) / kTileThreads;  // table entries a thread counts
   const uint32_t tid = threadIdx.x, lane = tid & 31u;
   const uint32_t ls = kTileThreads + 1;
@@ -497,6 +512,7 @@ cudaError_t launchFlockFP(const FusedArgs& A, uint32_t blocks, uint32_t block, s
                           cudaStream_t st) {
   if (A.scanVariant == 4) launchFlockScan<FP, 4>(A, blocks, block, smem, phase2, regs, st);
   else if (A.scanVariant == 5) launchFlockScan<FP, 5>(A, blocks, block, smem, phase2, regs, st);
+  else if (A.scanVariant == 7) launchFlockScan<FP, 7>(A, blocks, block, smem, phase2, regs, st);
   else launchFlockScan<FP, 0>(A, blocks, block, smem, phase2, regs, st);
   return cudaGetLastError();
 }
@@ -518,7 +534,7 @@ cudaError_t configureCoopScan(int smem) {
   return cudaSuccess;
 }
 template <int FP>
-cudaError_t configureFlockFP(int smem) {
+cudaError_t configureFlockFP(int smem, int smemCull) {
   const void* fns[4] = {(const void*)flockKernel<FP, 0, 4, 0>, (const void*)flockKernel<FP, 1, 4, 0>,
                         (const void*)flockKernel<FP, 0, 2, 0>, (const void*)flockKernel<FP, 1, 2, 0>};
   for (const void* fn : fns) {
@@ -526,7 +542,8 @@ cudaError_t configureFlockFP(int smem) {
     if (e != cudaSuccess) return e;
   }
   cudaError_t e = configureCoopScan<FP, 4>(smem);
-  return e == cudaSuccess ? configureCoopScan<FP, 5>(smem) : e;
+  if (e == cudaSuccess) e = configureCoopScan<FP, 5>(smem);
+  return e == cudaSuccess ? configureCoopScan<FP, 7>(smemCull) : e;
 }
 }  // namespace
 
@@ -585,7 +602,7 @@ cudaError_t launchFlock(const FusedArgs& A, int phase2, uint32_t block, int regs
   if (block < 32 || block > kFlockMaxThreads || block % 32) return cudaErrorInvalidValue;
   const uint32_t blocks = (A.n + block - 1) / block;
   const uint32_t fp = A.Fs;
-  const size_t smem = (size_t)(block + (A.scanVariant >= 4 ? 1u : 0u)) * A.Mmax * 4;
+  const size_t smem = flockSmemBytes(block, A.Mmax, A.scanVariant);
   if (fp == 0) return launchFlockFP<0>(A, blocks, block, smem, phase2, regs, st);
   if (fp <= 4) return launchFlockFP<4>(A, blocks, block, smem, phase2, regs, st);
   if (fp <= 8) return launchFlockFP<8>(A, blocks, block, smem, phase2, regs, st);
@@ -594,13 +611,14 @@ cudaError_t launchFlock(const FusedArgs& A, int phase2, uint32_t block, int regs
 }
 
 cudaError_t configureFlockKernels(uint32_t Mmax) {
-  const int smem = (int)((size_t)(kFlockMaxThreads + 1) * Mmax * 4);
+  const int smem = (int)flockSmemBytes(kFlockMaxThreads, Mmax, 5);
+  const int smemCull = (int)flockSmemBytes(kFlockMaxThreads, Mmax, 7);
   cudaError_t e = cudaSuccess;
-  if ((e = configureFlockFP<0>(smem))) return e;
-  if ((e = configureFlockFP<4>(smem))) return e;
-  if ((e = configureFlockFP<8>(smem))) return e;
-  if ((e = configureFlockFP<16>(smem))) return e;
-  if ((e = configureFlockFP<32>(smem))) return e;
+  if ((e = configureFlockFP<0>(smem, smemCull))) return e;
+  if ((e = configureFlockFP<4>(smem, smemCull))) return e;
+  if ((e = configureFlockFP<8>(smem, smemCull))) return e;
+  if ((e = configureFlockFP<16>(smem, smemCull))) return e;
+  if ((e = configureFlockFP<32>(smem, smemCull))) return e;
   const int tsmem = (int)((size_t)(kTileThreads + 1) * Mmax * 4);
   if ((e = configureTileFP<0>(tsmem))) return e;
   if ((e = configureTileFP<4>(tsmem))) return e;

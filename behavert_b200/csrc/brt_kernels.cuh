@@ -62,7 +62,8 @@ struct FusedArgs {
   float dt;
   int scanVariant;             // 0: pipelined x4 + cell culling, 1: x2 + culling, 2: x4, 3: flat loop,
                                // 4: warp-cooperative, 5: warp-cooperative with windows,
-                               // 6: staged tiles (tileFlockKernel)
+                               // 6: staged tiles (tileFlockKernel), 7: warp-cooperative with
+                               // bounding-box culling
   const uint32_t* stepCounter; // random-stream step of the Schooling move
   // scan variant 6: the (flock, row segment) tiles and the work-queue counter
   const uint4* tiles;          // x flock, y row y | z << 16, z first x | cells << 16

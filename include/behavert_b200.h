@@ -189,7 +189,7 @@ int brt_engine_set_params(brt_engine* e, uint32_t flock, const brt_params* p);
                               when the single-pass kernel applies (default 0)
      "block_size"       32..256, multiple of 32: threads per block of the
                               single-pass flock kernel (default 64)
-     "scan_variant"     0..6  neighbour-scan loop: 0 four candidates in flight
+     "scan_variant"     0..7  neighbour-scan loop: 0 four candidates in flight
                               with exact cell culling, 1 two in flight with
                               culling, 2 four without culling, 3 one at a time,
                               4 warp-cooperative (a warp tests 32 candidates of
@@ -201,16 +201,19 @@ int brt_engine_set_params(brt_engine* e, uint32_t flock, const brt_params* p);
                               segment) tiles: each block stages a tile's
                               neighbour cells in shared memory once and every
                               thread scans its agent's 27 cells from there
-                              (dense tiles that do not fit take scan 5)
+                              (dense tiles that do not fit take scan 5),
+                              7 as 4, with each home cell's candidates first
+                              tested against the bounding box of the cell's
+                              agents and only the survivors voted on
      "phase2_variant"   0..2  list walk: 0 one neighbour at a time, 1 two at a
                               time (per-agent scans 0..3 only), 2 (default)
                               two walks, geometry then feature sums (with
-                              scan_variant 4 or 5 and features; otherwise as 0)
+                              scan_variant 4, 5 or 7 and features; otherwise as 0)
      "wide_registers"   0/1   the flock kernel built for 128 registers a thread
                               (2 resident 256-thread blocks per SM) instead of 64
      "registers"        128, 64, 48 or 40: the flock kernel's register budget
                               a thread (64 default; 48 and 40 trade spills for
-                              resident warps and apply to scan_variant 4 and 5)
+                              resident warps and apply to scan_variant 4, 5, 7)
      "adjoint_graphs"   0/1   capture the adjoint forward/backward as graphs (default 1)
      "adjoint_export"   0/1   keep the frozen lists and branch flags (brt_adjoint_get_tape)
      "random_step"      uint32 the step counter of the Schooling random stream

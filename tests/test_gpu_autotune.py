@@ -44,7 +44,7 @@ def _variant_workloads():
     return {"large": big, "batched": bat, "cap": cap, "seam": seam, "2d": flat, "odd": odd, "dense": dense}
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6, 7])
 @pytest.mark.parametrize("name", ["large", "batched", "cap", "seam", "2d", "odd", "dense"])
 def test_scan_variants_are_bit_identical(name, variant):
     wl = _variant_workloads()[name]
@@ -69,7 +69,7 @@ def test_scan_variants_are_bit_identical(name, variant):
             assert np.array_equal(a, b)
 
 
-@pytest.mark.parametrize("scan,phase2", [(0, 1), (4, 2), (4, 1), (5, 2), (6, 2)])
+@pytest.mark.parametrize("scan,phase2", [(0, 1), (4, 2), (4, 1), (5, 2), (6, 2), (7, 2), (7, 0)])
 @pytest.mark.parametrize("name", ["large", "batched", "seam"])
 def test_list_walk_variants_are_bit_identical(name, scan, phase2):
     wl = _variant_workloads()[name]
@@ -81,12 +81,13 @@ def test_list_walk_variants_are_bit_identical(name, scan, phase2):
                 assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("scan", [4, 7])
 @pytest.mark.parametrize("budget", [128, 48, 40])
 @pytest.mark.parametrize("name", ["large", "batched", "seam"])
-def test_register_budgets_are_bit_identical(name, budget):
+def test_register_budgets_are_bit_identical(name, budget, scan):
     wl = _variant_workloads()[name]
-    ref = _run(wl, 2, [("scan_variant", 4)])
-    out = _run(wl, 2, [("scan_variant", 4), ("registers", budget)])
+    ref = _run(wl, 2, [("scan_variant", scan)])
+    out = _run(wl, 2, [("scan_variant", scan), ("registers", budget)])
     for a, b in zip(ref, out):
         if a is not None:
             assert np.array_equal(a, b)
