@@ -297,30 +297,46 @@ __global__ void __launch_bounds__(kAdjointThreads) adjointStepKernel(AdjointStep
     // Every list entry (i, k) with a contribution: the adjoint it sends to
     // the agent j it lists, stored at the entry, and the entry into j's
     // in-list.  The separation term's own share goes to selfP (in list order).
-    for (uint32_t m = mS | mA | mC; m; m &= m - 1u) {
-      const uint32_t k = (uint32_t)__ffs(m) - 1u;
-      const uint32_t j = lst[1 + k];
-      f3 gp = mk3(0.f, 0.f, 0.f);
-      if ((mS >> k) & 1u) {
-        const f3 other = neighborImage(a, __ldg(&A.posS[j]), fl);
-        const f3 o = sub3(other, a.pos);
-        const f3 go = separationBar(o, dot3(o, o), gSs);
-        gp = add3(gp, go);
-        selfP = sub3(selfP, go);
+    // Entries go kEmitGroup at a time: the group's in-list positions are
+    // reserved by atomics issued back to back, so their round trips overlap
+    // (a store waiting on its own atomic would otherwise hold up the next
+    // entry's atomic).  Positions only place terms the gather sums order-free.
+    constexpr int kEmitGroup = 4;
+    for (uint32_t m = mS | mA | mC; m;) {
+      uint32_t kk[kEmitGroup], jj[kEmitGroup], q[kEmitGroup];
+#pragma unroll
+      for (int u = 0; u < kEmitGroup; ++u) {
+        kk[u] = m ? (uint32_t)__ffs(m) - 1u : kNoEntry;
+        m &= m - 1u;
+        jj[u] = kk[u] != kNoEntry ? lst[1 + kk[u]] : 0u;
       }
-      if ((mC >> k) & 1u) gp = add3(gp, gSc);
-      const f3 gf = ((mA >> k) & 1u) ? gSa : mk3(0.f, 0.f, 0.f);
-      const float4 c0 = make_float4(gp.x, gp.y, gp.z, gf.x), c1 = make_float4(gf.y, gf.z, 0.0f, 0.0f);
-      const uint32_t q = atomicAdd(&A.inCount[j], 1u);
-      if (q < A.inCap) {
-        float4* slot = A.inbox + 2 * ((size_t)j * A.inCap + q);
-        slot[0] = c0;
-        slot[1] = c1;
-      } else {
-        const uint32_t e = i * A.entryStride + k;
-        A.contrib[2 * (size_t)e + 0] = c0;
-        A.contrib[2 * (size_t)e + 1] = c1;
-        A.ovNext[e] = atomicExch(&A.ovHead[j], e);
+#pragma unroll
+      for (int u = 0; u < kEmitGroup; ++u) q[u] = kk[u] != kNoEntry ? atomicAdd(&A.inCount[jj[u]], 1u) : 0u;
+#pragma unroll
+      for (int u = 0; u < kEmitGroup; ++u) {
+        if (kk[u] == kNoEntry) break;
+        const uint32_t k = kk[u], j = jj[u];
+        f3 gp = mk3(0.f, 0.f, 0.f);
+        if ((mS >> k) & 1u) {
+          const f3 other = neighborImage(a, __ldg(&A.posS[j]), fl);
+          const f3 o = sub3(other, a.pos);
+          const f3 go = separationBar(o, dot3(o, o), gSs);
+          gp = add3(gp, go);
+          selfP = sub3(selfP, go);
+        }
+        if ((mC >> k) & 1u) gp = add3(gp, gSc);
+        const f3 gf = ((mA >> k) & 1u) ? gSa : mk3(0.f, 0.f, 0.f);
+        const float4 c0 = make_float4(gp.x, gp.y, gp.z, gf.x), c1 = make_float4(gf.y, gf.z, 0.0f, 0.0f);
+        if (q[u] < A.inCap) {
+          float4* slot = A.inbox + 2 * ((size_t)j * A.inCap + q[u]);
+          slot[0] = c0;
+          slot[1] = c1;
+        } else {
+          const uint32_t e = i * A.entryStride + k;
+          A.contrib[2 * (size_t)e + 0] = c0;
+          A.contrib[2 * (size_t)e + 1] = c1;
+          A.ovNext[e] = atomicExch(&A.ovHead[j], e);
+        }
       }
     }
     A.selfP[i] = make_float4(selfP.x, selfP.y, selfP.z, 0.0f);
@@ -358,6 +374,7 @@ __global__ void __launch_bounds__(kAdjointThreads) adjointStepKernel(AdjointStep
 struct ExactSum6 {
   float mx[6];
   int sh[6];
+  float up[6], down[6];  // 2^sh and 2^-sh when both are normal floats, else 0 (ldexpf then)
   long long acc[6];
   bool finite = true;
   __device__ __forceinline__ void seeMax(const float* t) {
@@ -369,17 +386,33 @@ struct ExactSum6 {
 #pragma unroll
     for (int c = 0; c < 6; ++c) {
       if (!isfinite(mx[c])) finite = false;
-      int ex = 0;
-      if (mx[c] > 0.0f) frexpf(mx[c], &ex);
+      // mx = f * 2^ex with f in [0.5, 1): the biased exponent of a normal
+      // float minus 126, frexpf for the rest (zero and subnormals)
+      const uint32_t bits = __float_as_uint(mx[c]);
+      const int be = (int)((bits >> 23) & 0xFFu);
+      int ex = be - 126;
+      if (be == 0) {
+        ex = 0;
+        if (mx[c] > 0.0f) frexpf(mx[c], &ex);
+      }
       sh[c] = 62 - headroom - ex;  // |term| * 2^sh < 2^(62 - headroom)
+      const bool fast = sh[c] >= -126 && sh[c] <= 127;
+      up[c] = fast ? __uint_as_float((uint32_t)(sh[c] + 127) << 23) : 0.0f;
+      down[c] = fast ? __uint_as_float((uint32_t)(127 - sh[c]) << 23) : 0.0f;
       acc[c] = 0;
     }
   }
+  // term * 2^sh, exact (a power-of-two scale that neither overflows nor,
+  // for any term that rounds to a nonzero integer, underflows)
+  __device__ __forceinline__ float scaled(float t, int c) const { return up[c] != 0.0f ? t * up[c] : ldexpf(t, sh[c]); }
   __device__ __forceinline__ void add(const float* t) {
 #pragma unroll
-    for (int c = 0; c < 6; ++c) acc[c] += __float2ll_rn(ldexpf(t[c], sh[c]));
+    for (int c = 0; c < 6; ++c) acc[c] += __float2ll_rn(scaled(t[c], c));
   }
-  __device__ __forceinline__ float value(int c) const { return ldexpf(__ll2float_rn(acc[c]), -sh[c]); }
+  __device__ __forceinline__ float value(int c) const {
+    const float v = __ll2float_rn(acc[c]);
+    return down[c] != 0.0f ? v * down[c] : ldexpf(v, -sh[c]);
+  }
 };
 
 __device__ __forceinline__ void termsOf(const float4 c0, const float4 c1, float* t) {
