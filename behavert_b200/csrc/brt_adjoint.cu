@@ -86,10 +86,16 @@ __device__ __forceinline__ f3 limitedDeviation(f3 source, float cosineOfConeAngl
 
 }  // namespace
 
+// Resident blocks per SM the two reverse kernels are compiled for: 6 caps them
+// at 80 registers a thread (a few spills) and 24 resident warps; the
+// uncapped builds (about 105 registers, 16 warps) were latency-bound and
+// measured 5% slower on config 4's backward, 1.5% on config 3's.
+constexpr int kAdjointMinBlocks = 6;
+
 // Branch bits of the exported flag word (the oracle's frozen-branch layout).
 constexpr uint32_t kBrLow = 1u, kBrLimited = 2u, kBrClipF = 4u, kBrClipV = 8u;
 
-__global__ void __launch_bounds__(kAdjointThreads) adjointStepKernel(AdjointStepArgs A) {
+__global__ void __launch_bounds__(kAdjointThreads, kAdjointMinBlocks) adjointStepKernel(AdjointStepArgs A) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = i < A.n;
   uint32_t f = 0;
@@ -428,7 +434,7 @@ __device__ __forceinline__ void termsOf(const float4 c0, const float4 c1, float*
 constexpr uint32_t kGatherLanes = 8;
 constexpr uint32_t kGatherPerLane = 8;  // inbox entries a lane holds: inCap <= 64
 
-__global__ void __launch_bounds__(kAdjointThreads) adjointGatherKernel(AdjointStepArgs A) {
+__global__ void __launch_bounds__(kAdjointThreads, kAdjointMinBlocks) adjointGatherKernel(AdjointStepArgs A) {
   const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t j = gt / kGatherLanes, sub = gt % kGatherLanes;
   const bool valid = j < A.n;
