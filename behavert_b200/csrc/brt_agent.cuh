@@ -25,6 +25,8 @@ __device__ __forceinline__ uint32_t buildNeighborList(uint32_t self, f3 p, const
                                                       uint32_t ls, float* distList) {
   const int gx = gridCoord(p.x, fl.cell, fl.G), gy = gridCoord(p.y, fl.cell, fl.G), gz = gridCoord(p.z, fl.cell, fl.G);
   const uint32_t M = fl.M;
+  // kNN replacement is per flock: an engine may mix kNN and first-M flocks
+  const bool knn = KNN && fl.useKnn;
   uint32_t n = 0;
   float maxDistValue = 0.0f;
   for (int ox = -1; ox <= 1; ++ox) {
@@ -46,7 +48,7 @@ __device__ __forceinline__ uint32_t buildNeighborList(uint32_t self, f3 p, const
           const float4 q = __ldg(&posS[j]);
           const float dx = (q.x + sx) - p.x, dy = (q.y + sy) - p.y, dz = (q.z + sz) - p.z;
           const float d2 = dx * dx + dy * dy + dz * dz;
-          if (!KNN) {
+          if (!knn) {
             if (d2 > fl.r2thr) continue;
             list[(n++) * ls] = j;
             if (n == M) return n;
@@ -269,6 +271,16 @@ __device__ __forceinline__ uint32_t scanNeighborsPipelined(uint32_t self, f3 p, 
 // `self`, position p, home cell key `key`, flock `flock`).  Each agent's list
 // goes to column laneCol0 + lane of the shared array sList (stride ls).
 // Returns the lane's list length.
+// Position of the (w + 1)-th set bit of m (w < popc(m)): the largest q with
+// w or fewer set bits below it.
+__device__ __forceinline__ uint32_t nthSetBit(uint32_t m, uint32_t w) {
+  uint32_t q = 0;
+#pragma unroll
+  for (uint32_t step = 16; step > 0; step >>= 1)
+    if ((uint32_t)__popc(m & ((1u << (q + step)) - 1u)) <= w) q += step;
+  return q;
+}
+
 __device__ __forceinline__ uint32_t orderedBits(float x) {
   const uint32_t u = __float_as_uint(x);
   return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
@@ -277,14 +289,31 @@ __device__ __forceinline__ float fromOrderedBits(uint32_t u) {
   return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u);
 }
 
-template <int R, int WINT = 0, bool CULL = false>
+// With KNN, runs of a flock with useKnn build the reference's kNN list
+// instead (the first M accepted, then each closer candidate replacing the
+// entry found farthest, Proximity3D_resources.cu:71-104), still agent-major
+// over R register-held rounds: lane k holds entry k of the agent's list and
+// its distance (M <= 32), the farthest entry is a warp maximum, and the
+// agent's list and distances wait in sList / dList between windows.
+//
+// The reference's bound is stale: a replacement sets it to the largest
+// distance before the replacement, and the new entry may lie above that.  So
+// the bound s can rise, but never above the larger of its last two values:
+// after a replacement of candidate d (d < s_k) the new bound is
+// s_{k+1} = max(list) and the next one is at most max(s_{k+1}, d) <
+// max(s_{k+1}, s_k).  A candidate at or beyond B = max(s, previous s) can
+// never replace an entry and is skipped before the serial replacements.
+// The first M accepted go in with one ballot, as in the first-M scan.
+template <int R, int WINT = 0, bool CULL = false, bool KNN = false>
 __device__ __forceinline__ uint32_t scanNeighborsCooperative(bool active, uint32_t self, f3 p, uint32_t key,
                                                              const FlockDev* __restrict__ flocks, uint32_t flock,
                                                              const uint32_t* __restrict__ cellStart,
                                                              const uint32_t* __restrict__ cellEnd,
                                                              const float4* __restrict__ posS, uint32_t* sList,
-                                                             uint32_t ls, uint32_t laneCol0, float4* cbuf = nullptr) {
+                                                             uint32_t ls, uint32_t laneCol0, float4* cbuf = nullptr,
+                                                             float* dList = nullptr) {
   static_assert(!CULL || R > 0, "the culled scan votes on register-held rounds");
+  static_assert(!KNN || (R > 0 && !CULL), "the kNN scan votes on register-held rounds, unculled");
   const uint32_t full = 0xFFFFFFFFu;
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t myKey = active ? key : 0xFFFFFFFFu;
@@ -293,6 +322,7 @@ __device__ __forceinline__ uint32_t scanNeighborsCooperative(bool active, uint32
   uint32_t heads = __ballot_sync(full, head);
   const uint32_t activeMask = __ballot_sync(full, active);
   uint32_t n = 0;
+  float kmx = 0.0f, kmxPrev = 0.0f;  // kNN: the lane's agent's bound (maxDistValue) and its previous value
   // bounding box of the lane's run: lanes of equal key (a run, or with a
   // corrupted order a superset of it, which only culls less)
   float bLo[3] = {0.f, 0.f, 0.f}, bHi[3] = {0.f, 0.f, 0.f};
@@ -348,6 +378,121 @@ __device__ __forceinline__ uint32_t scanNeighborsCooperative(bool active, uint32
     const uint32_t total = __shfl_sync(full, incl, 31);
     uint32_t open = groupMask;  // group agents whose list is not full yet
     uint32_t base0 = 0;
+    if constexpr (KNN) {
+      if (fl.useKnn) {
+        constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
+        const float radius = fl.radius;
+        for (; base0 < total; base0 += (uint32_t)R * 32u) {
+          float cqx[R], cqy[R], cqz[R];
+          uint32_t cslot[R];
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            cqx[r] = cqy[r] = cqz[r] = 0.0f;
+            cslot[r] = kNoSlot;
+            if (base0 + (uint32_t)r * 32u < total) {
+              const uint32_t t = base0 + (uint32_t)r * 32u + lane;
+              uint32_t c = 0;
+#pragma unroll
+              for (int step = 16; step > 0; step >>= 1) {
+                const uint32_t cand = c + (uint32_t)step;
+                const uint32_t e = __shfl_sync(full, excl, cand & 31u);
+                if (cand < 27u && e <= t) c = cand;
+              }
+              const uint32_t cStart = __shfl_sync(full, segStart, c), cExcl = __shfl_sync(full, excl, c);
+              const float csx = __shfl_sync(full, sx, c), csy = __shfl_sync(full, sy, c), csz = __shfl_sync(full, sz, c);
+              if (t < total) {
+                cslot[r] = cStart + (t - cExcl);
+                const float4 q = __ldg(&posS[cslot[r]]);
+                cqx[r] = q.x + csx;
+                cqy[r] = q.y + csy;
+                cqz[r] = q.z + csz;
+              }
+            }
+          }
+          for (uint32_t todo = groupMask; todo; todo &= todo - 1u) {
+            const uint32_t a = __ffs(todo) - 1u;
+            const float ax = __shfl_sync(full, p.x, a), ay = __shfl_sync(full, p.y, a), az = __shfl_sync(full, p.z, a);
+            const uint32_t aSelf = __shfl_sync(full, self, a);
+            uint32_t an = __shfl_sync(full, n, a);
+            float amx = __shfl_sync(full, kmx, a), amxPrev = __shfl_sync(full, kmxPrev, a);
+            uint32_t* col = sList + laneCol0 + a;
+            float* dcol = dList + laneCol0 + a;
+            const uint32_t below = (1u << lane) - 1u;
+            // the agent's list so far: entry `lane` and its distance
+            uint32_t ks = 0u;
+            float kd = 0.0f;
+            if (lane < an) {
+              ks = col[lane * ls];
+              kd = dcol[lane * ls];
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+              if (base0 + (uint32_t)r * 32u >= total) break;
+              const float dx = cqx[r] - ax, dy = cqy[r] - ay, dz = cqz[r] - az;
+              const float dist = sqrtf(dx * dx + dy * dy + dz * dz);
+              const bool acc = cslot[r] != kNoSlot && cslot[r] != aSelf && !(dist > radius);
+              uint32_t bal = __ballot_sync(full, acc);
+              if (an < M) {
+                // the fill: accepted candidates in order into entries an, an + 1, ...
+                const uint32_t pos = an + (uint32_t)__popc(bal & below);
+                const bool fill = acc && pos < M;
+                const uint32_t fillers = __ballot_sync(full, fill);
+                {
+                  // entry lanes an, an + 1, ... pull their new entry from the
+                  // lane of the 1st, 2nd, ... candidate taken
+                  const uint32_t want = lane - an;  // wraps for lanes below an
+                  const bool mine = lane >= an && want < (uint32_t)__popc(fillers);
+                  const uint32_t srcLane = mine ? nthSetBit(fillers, want) : 0u;
+                  const float cd = __shfl_sync(full, dist, srcLane);
+                  const uint32_t cs = __shfl_sync(full, cslot[r], srcLane);
+                  if (mine) { ks = cs; kd = cd; }
+                }
+                // maxDistValue = max over the entries taken, in order (no NaN
+                // is ever kept as the bound by the reference's std::max)
+                const uint32_t fb = (fill && !isnan(dist)) ? __float_as_uint(dist) : 0u;
+                const uint32_t fm = __reduce_max_sync(full, fb);
+                if (fillers) amx = fmaxf(amx, __uint_as_float(fm));
+                an += (uint32_t)__popc(fillers);
+                bal &= ~fillers;
+                amxPrev = amx;
+              }
+              // the rest: candidates below the bound's ceiling, one at a time
+              const float ceilB = fmaxf(amx, amxPrev);
+              bal &= __ballot_sync(full, dist < ceilB);
+              for (; bal; bal &= bal - 1u) {
+                const uint32_t src = __ffs(bal) - 1u;
+                const float cd = __shfl_sync(full, dist, src);
+                const uint32_t cs = __shfl_sync(full, cslot[r], src);
+                if (cd < amx) {
+                  // the first entry holding the largest distance, as the
+                  // reference's scan from entry 0 with a strict < finds it
+                  // (a NaN entry 0 stays the pick; other NaN entries never are)
+                  const float d0 = __shfl_sync(full, kd, 0);
+                  uint32_t idx = 0;
+                  float mv = d0;
+                  if (!isnan(d0)) {
+                    const bool ok = lane < an && !isnan(kd);
+                    const uint32_t kb = ok ? __float_as_uint(kd) : 0u;  // distances are >= +0
+                    const uint32_t mb = __reduce_max_sync(full, kb);
+                    idx = __ffs(__ballot_sync(full, ok && kb == mb)) - 1u;
+                    mv = __uint_as_float(mb);
+                  }
+                  amxPrev = amx;
+                  amx = mv;
+                  if (lane == idx) { ks = cs; kd = cd; }
+                }
+              }
+            }
+            if (lane < an) {
+              col[lane * ls] = ks;
+              dcol[lane * ls] = kd;
+            }
+            if (lane == a) { n = an; kmx = amx; kmxPrev = amxPrev; }
+          }
+        }
+        continue;  // the next run
+      }
+    }
     if constexpr (CULL) {
       constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
       const uint32_t below = (1u << lane) - 1u;

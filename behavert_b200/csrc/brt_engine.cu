@@ -355,10 +355,12 @@ int enqueueStep(brt_engine* e, float dt, bool record) {
   F.scanVariant = e->scanVariant;
   F.tiles = e->tiles; F.numTiles = e->numTiles; F.tileCounter = e->tileCounter; F.tileBlocks = e->tileBlocks;
   F.stepCounter = e->stepCounter;
-  // The single-pass kernel covers every flock unless one needs kNN
-  // replacement or clustering steering (both need the whole list first).
-  bool twoPass = e->anyKnn || e->forceTwoPass;
+  // The single-pass kernel covers every flock unless one needs clustering
+  // steering (it needs the whole list first) or kNN lists longer than a warp.
+  // kNN flocks take its cooperative kNN scan (scan 8).
+  bool twoPass = e->forceTwoPass || (e->anyKnn && e->Mmax > 32);
   for (const FlockDev& d : e->flocksHost) twoPass = twoPass || (d.F > 0 && (d.clus != 0.0f || d.aclus != 0.0f));
+  if (e->anyKnn && !twoPass) F.scanVariant = 8;
   if (e->school) BRT_CUDA_TRY(launchSchool(F, e->stream));
   else if (twoPass) BRT_CUDA_TRY(launchFused(F, e->anyKnn, e->stream));
   else BRT_CUDA_TRY(launchFlock(F, e->phase2Variant, e->fusedBlock, e->regBudget, e->stream));

@@ -48,9 +48,12 @@ constexpr int kCoopWindowAgents = 8;
 // float4 per warp, from a 16-byte aligned word offset.
 constexpr uint32_t kCullBufPerWarp = (kCoopCachedRounds + 1) * 32;
 __host__ __device__ constexpr uint32_t cullBufOffsetWords(uint32_t ls, uint32_t Mmax) { return (ls * Mmax + 3u) & ~3u; }
+// Scan 8 (the cooperative scan with the kNN replacement, for engines with a
+// useKnn flock and maxNeighbors <= 32) keeps each list's distances beside it.
 __host__ __device__ constexpr size_t flockSmemBytes(uint32_t block, uint32_t Mmax, int scan) {
-  return scan == 7 ? (size_t)cullBufOffsetWords(block + 1, Mmax) * 4 + (size_t)(block / 32) * kCullBufPerWarp * 16
-                   : (size_t)(block + (scan >= 4 ? 1u : 0u)) * Mmax * 4;
+  return scan == 7   ? (size_t)cullBufOffsetWords(block + 1, Mmax) * 4 + (size_t)(block / 32) * kCullBufPerWarp * 16
+         : scan == 8 ? (size_t)2 * (block + 1) * Mmax * 4
+                     : (size_t)(block + (scan >= 4 ? 1u : 0u)) * Mmax * 4;
 }
 
 // Phase 2 of the flock kernels: steering and feature sums over agent i's
@@ -260,6 +263,10 @@ __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs 
       float4* cbuf = reinterpret_cast<float4*>(sList + cullBufOffsetWords(ls, A.Mmax)) + (threadIdx.x >> 5) * kCullBufPerWarp;
       n = scanNeighborsCooperative<kCoopCachedRounds, 0, true>(active, i, p, key, A.flocks, f, A.cellStart, A.cellEnd,
                                                                A.posS, sList, ls, threadIdx.x & ~31u, cbuf);
+    } else if constexpr (SCAN == 8) {
+      float* dList = reinterpret_cast<float*>(sList + ls * A.Mmax);
+      n = scanNeighborsCooperative<kCoopCachedRounds, kCoopWindowAgents, false, true>(
+          active, i, p, key, A.flocks, f, A.cellStart, A.cellEnd, A.posS, sList, ls, threadIdx.x & ~31u, nullptr, dList);
     } else {
       n = scanNeighborsCooperative<kCoopCachedRounds, SCAN == 5 ? kCoopWindowAgents : 0>(
           active, i, p, key, A.flocks, f, A.cellStart, A.cellEnd, A.posS, sList, ls, threadIdx.x & ~31u);
@@ -513,6 +520,7 @@ cudaError_t launchFlockFP(const FusedArgs& A, uint32_t blocks, uint32_t block, s
   if (A.scanVariant == 4) launchFlockScan<FP, 4>(A, blocks, block, smem, phase2, regs, st);
   else if (A.scanVariant == 5) launchFlockScan<FP, 5>(A, blocks, block, smem, phase2, regs, st);
   else if (A.scanVariant == 7) launchFlockScan<FP, 7>(A, blocks, block, smem, phase2, regs, st);
+  else if (A.scanVariant == 8) launchFlockScan<FP, 8>(A, blocks, block, smem, phase2, regs, st);
   else launchFlockScan<FP, 0>(A, blocks, block, smem, phase2, regs, st);
   return cudaGetLastError();
 }
@@ -534,7 +542,7 @@ cudaError_t configureCoopScan(int smem) {
   return cudaSuccess;
 }
 template <int FP>
-cudaError_t configureFlockFP(int smem, int smemCull) {
+cudaError_t configureFlockFP(int smem, int smemCull, int smemKnn) {
   const void* fns[4] = {(const void*)flockKernel<FP, 0, 4, 0>, (const void*)flockKernel<FP, 1, 4, 0>,
                         (const void*)flockKernel<FP, 0, 2, 0>, (const void*)flockKernel<FP, 1, 2, 0>};
   for (const void* fn : fns) {
@@ -543,6 +551,7 @@ cudaError_t configureFlockFP(int smem, int smemCull) {
   }
   cudaError_t e = configureCoopScan<FP, 4>(smem);
   if (e == cudaSuccess) e = configureCoopScan<FP, 5>(smem);
+  if (e == cudaSuccess) e = configureCoopScan<FP, 8>(smemKnn);
   return e == cudaSuccess ? configureCoopScan<FP, 7>(smemCull) : e;
 }
 }  // namespace
@@ -613,12 +622,13 @@ cudaError_t launchFlock(const FusedArgs& A, int phase2, uint32_t block, int regs
 cudaError_t configureFlockKernels(uint32_t Mmax) {
   const int smem = (int)flockSmemBytes(kFlockMaxThreads, Mmax, 5);
   const int smemCull = (int)flockSmemBytes(kFlockMaxThreads, Mmax, 7);
+  const int smemKnn = (int)flockSmemBytes(kFlockMaxThreads, std::min<uint32_t>(Mmax, 32), 8);
   cudaError_t e = cudaSuccess;
-  if ((e = configureFlockFP<0>(smem, smemCull))) return e;
-  if ((e = configureFlockFP<4>(smem, smemCull))) return e;
-  if ((e = configureFlockFP<8>(smem, smemCull))) return e;
-  if ((e = configureFlockFP<16>(smem, smemCull))) return e;
-  if ((e = configureFlockFP<32>(smem, smemCull))) return e;
+  if ((e = configureFlockFP<0>(smem, smemCull, smemKnn))) return e;
+  if ((e = configureFlockFP<4>(smem, smemCull, smemKnn))) return e;
+  if ((e = configureFlockFP<8>(smem, smemCull, smemKnn))) return e;
+  if ((e = configureFlockFP<16>(smem, smemCull, smemKnn))) return e;
+  if ((e = configureFlockFP<32>(smem, smemCull, smemKnn))) return e;
   const int tsmem = (int)((size_t)(kTileThreads + 1) * Mmax * 4);
   if ((e = configureTileFP<0>(tsmem))) return e;
   if ((e = configureTileFP<4>(tsmem))) return e;

@@ -18,6 +18,11 @@ feature relaxation.  Rank 0 prints one JSON line.
 * cpu_baseline (rank 0, N=1): the CPU oracle (multi-threaded C++ restatement of
   the reference's plugin logic) on a bounded sample of the same workload, plus
   the per-step error of the GPU state against the FP64 oracle.
+* batched / adjoint / fitting (N=1): configs 2, 3 and 4.
+* next_rows (rank 0, N=1): the components beside the flocking path (Schooling,
+  kNN lists, the crowd order with steerAndSlowToAvoidNeighbors, clustering
+  analytics, snapshots) on 1,048,576-agent states, each with the oracle's
+  host time for the same work and a parity check of its first step.
 
 Multi-GPU: the path does not shard (one flock on one GPU); N ranks run N
 independent replicas ("weak" scaling), one process per GPU.
@@ -365,6 +370,127 @@ def adjoint_leg(device: int, reps: int = 5):
             "loss": float(loss.item()), "grad_weights": gw.cpu().numpy()[0].tolist(), "tuned": tuned}
 
 
+def next_rows_leg(device: int, steps: int = 100, repeats: int = 3):
+    """The components beside the flocking path, each on a 1,048,576-agent
+    state: the Schooling law (animateSchool, and the split path with its
+    random stream), the kNN neighbour semantics (useKnn: the nearest
+    maxNeighbors kept), the crowd sample's order with
+    steerAndSlowToAvoidNeighbors (stage-wise launches), the clustering
+    analytics (10 label-propagation sweeps, then the hit rate) and a state
+    snapshot.  Device time by CUDA events on the engine stream (fused steps:
+    `steps`-step graphs from the seeded state, median of `repeats`).  Beside
+    each, the oracle's time for the same work on the host cores, and a live
+    parity check of the first step (or call) against it."""
+    import os
+    import tempfile
+    import torch
+    from behavert_b200 import Engine, workloads
+    from oracle import oracle
+    threads = min(oracle.hardware_threads(), 64)
+    out = {}
+
+    def fused(name, w, mode_kw):
+        eng = Engine(w.params, device=device)
+        stream = torch.cuda.ExternalStream(eng.stream_handle())
+        eng.set_state(w.pos, w.fwd, w.acc, w.feat)
+        eng.step(w.dt, 1)
+        g1 = eng.get_state()
+        eng.step_prepare(w.dt, steps)
+        ts = []
+        for _ in range(repeats + 1):
+            eng.set_state(w.pos, w.fwd, w.acc, w.feat)
+            eng.sync()
+            ts.append(_events_ms(stream, lambda: eng.step(w.dt, steps)))
+        eng.close()
+        t = float(np.median(ts[1:])) / 1e3
+        t0 = time.perf_counter()
+        r = oracle.step(w.params, w.pos, w.fwd, w.acc, w.feat, dt=w.dt, mode=0, threads=threads,
+                        want_intermediates=False, **mode_kw)
+        tc = time.perf_counter() - t0
+        exact = all(np.array_equal(np.asarray(a).view(np.uint32), np.ascontiguousarray(b, np.float32).view(np.uint32))
+                    for a, b in ((g1[0], r["pos"]), (g1[1], r["fwd"]), (g1[2], r["acc"])))
+        n = w.num_agents
+        out[name] = {"value": n * steps / t, "unit": UNIT, "ms_per_step": 1e3 * t / steps,
+                     "cpu_value": n / tc, "cpu_cores": threads, "cpu_sample": "1 oracle step of the same state",
+                     "step1_state_bit_exact_vs_oracle": bool(exact)}
+
+    for mode, name in ((1, "schooling_animate"), (2, "schooling_split")):
+        w = workloads.schooling(n=1 << 20, L=256.0, mode=mode)
+        fused(name, w, {"random_step": 1})
+        out[name]["workload"] = "Schooling law (mode %d), 1,048,576 agents, cube 256, maxNeighbors 16" % mode
+    w = workloads.large()
+    w.params[0].useKnn = 1
+    fused("knn", w, {})
+    out["knn"]["workload"] = "config 1 with useKnn (the nearest 32 kept)"
+
+    # the crowd order: stage-wise functionalities, one launch sequence a step
+    w = workloads.plain(n=1 << 20, L=256.0, M=32, seed=5)
+    eng = Engine(w.params, device=device)
+    stream = torch.cuda.ExternalStream(eng.stream_handle())
+    eng.set_state(w.pos, w.fwd, w.acc)
+    eng.update_crowd(w.dt)
+    g1 = eng.get_state(features=False)
+    ts = []
+    for _ in range(repeats + 1):
+        eng.set_state(w.pos, w.fwd, w.acc)
+        eng.sync()
+        ts.append(_events_ms(stream, lambda: [eng.update_crowd(w.dt) for _ in range(10)]))
+    t = float(np.median(ts[1:])) / 1e3 / 10
+    # the clustering analytics on config 1's lists after one step
+    wc = workloads.large()
+    ec = Engine(wc.params, device=device)
+    sc = torch.cuda.ExternalStream(ec.stream_handle())
+    ec.record_lists(True)
+    ec.set_state(wc.pos, wc.fwd, wc.acc, wc.feat)
+    ec.step(wc.dt, 1)
+    ec.computeClusterMembership(10)
+    labels = ec.getClusterMembership()[:, 0].copy()
+    tm, th = [], []
+    for _ in range(repeats + 1):
+        tm.append(_events_ms(sc, lambda: ec.computeClusterMembership(10)))
+        th.append(_events_ms(sc, lambda: ec.analyzeClusterHitRate(1.5)))
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "state.brt")
+        s0 = time.perf_counter()
+        ec.save_snapshot(path)
+        s1 = time.perf_counter()
+        ec.load_snapshot(path)
+        ec.sync()
+        s2 = time.perf_counter()
+        snap_bytes = os.path.getsize(path)
+    ec.close()
+    eng.close()
+    t0 = time.perf_counter()
+    r = oracle.step(w.params, w.pos, w.fwd, w.acc, dt=w.dt, mode=0, threads=threads, want_intermediates=False,
+                    avoid_neighbors=True)
+    tc = time.perf_counter() - t0
+    exact = all(np.array_equal(np.asarray(a).view(np.uint32), np.ascontiguousarray(b, np.float32).view(np.uint32))
+                for a, b in ((g1[0], r["pos"]), (g1[1], r["fwd"]), (g1[2], r["acc"])))
+    out["crowd_avoid"] = {"workload": "crowd order (steerAndSlowToAvoidNeighbors in place of separation), "
+                                      "1,048,576 agents, cube 256, maxNeighbors 32, stage-wise launches",
+                          "value": w.num_agents / t, "unit": UNIT, "ms_per_step": 1e3 * t,
+                          "cpu_value": w.num_agents / tc, "cpu_cores": threads,
+                          "cpu_sample": "1 oracle step of the same state",
+                          "step1_state_bit_exact_vs_oracle": bool(exact)}
+    o = oracle.step(wc.params, wc.pos, wc.fwd, wc.acc, wc.feat, dt=wc.dt, threads=threads)
+    t0 = time.perf_counter()
+    ref = oracle.cluster_membership(o, 10)
+    tcm = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    oracle.cluster_hit_rate(wc.params, wc.pos, o, ref, 1.5)
+    tch = time.perf_counter() - t0
+    out["cluster_analytics"] = {"workload": "config 1 after one step: computeClusterMembership(10), "
+                                            "analyzeClusterHitRate(1.5)",
+                                "membership_ms": float(np.median(tm[1:])), "hit_rate_ms": float(np.median(th[1:])),
+                                "cpu_membership_ms": 1e3 * tcm, "cpu_hit_rate_ms": 1e3 * tch,
+                                "cpu_kind": "numpy restatement, 1 thread",
+                                "labels_equal_vs_oracle": bool(np.array_equal(labels, ref))}
+    out["snapshot"] = {"workload": "config 1 state (positions, forwards, accelerations, features)",
+                       "bytes": snap_bytes, "save_ms": 1e3 * (s1 - s0), "load_ms": 1e3 * (s2 - s1),
+                       "note": "host file I/O to a temporary directory"}
+    return out
+
+
 def adjoint_accuracy(device: int):
     """Config 3 gradients against the FP64 frozen-neighbour oracle (the CPU
     checker): the FP64 reverse with the GPU's frozen lists and branches, and
@@ -517,6 +643,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-fit", action="store_true")
+    ap.add_argument("--no-next-rows", action="store_true",
+                    help="skip the schooling / kNN / crowd / clustering-analytics / snapshot leg")
     ap.add_argument("--fit-iters", type=int, default=200)
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--e2e-iters", type=int, default=3)
@@ -746,6 +874,8 @@ def main():
             line["adjoint"]["accuracy"] = adjoint_accuracy(local)
     if world == 1 and not args.no_fit:
         line["fitting"] = fitting_leg(local, args.fit_iters)
+    if rank == 0 and world == 1 and not args.no_next_rows:
+        line["next_rows"] = next_rows_leg(local)
     for leg in ("batched", "adjoint", "fitting"):
         if leg in line and isinstance(line[leg].get("tuned"), dict):
             line[leg]["tuned"] = compact_tuned(line[leg]["tuned"])
@@ -791,6 +921,15 @@ def summary_keys(line: dict) -> dict:
         out["fit_iters_per_s"] = f["fit_iters_per_s"]
         out["fit_speedup_vs_looped"] = f["speedup_vs_looped"]
         out["fit_recovered_weight_median_abs_err"] = f["recovered_weight_abs_err"]["median"]
+    nr = line.get("next_rows")
+    if nr:
+        for k in ("schooling_animate", "schooling_split", "knn", "crowd_avoid"):
+            out[k + "_agent_steps_per_s"] = nr[k]["value"]
+            out[k + "_vs_oracle_cpu"] = nr[k]["value"] / nr[k]["cpu_value"]
+        out["cluster_membership_ms"] = nr["cluster_analytics"]["membership_ms"]
+        out["next_rows_parity"] = all(nr[k]["step1_state_bit_exact_vs_oracle"]
+                                      for k in ("schooling_animate", "schooling_split", "knn", "crowd_avoid")) \
+            and nr["cluster_analytics"]["labels_equal_vs_oracle"]
     return out
 
 

@@ -315,6 +315,34 @@ def test_obstacles():
         check_step(eng, w.params)
 
 
+@pytest.mark.parametrize("M", [16, 40])
+def test_knn_and_first_m_flocks_in_one_engine(M):
+    """kNN replacement is per flock: an engine holding a useKnn flock and a
+    first-M flock gives each its own lists (M <= 32: the cooperative kNN scan
+    of the single-pass kernel; M > 32: the two-pass kernel), bit-exact."""
+    a = workloads.plain(n=3000, L=28.0, M=M, seed=51)
+    b = workloads.plain(n=2500, L=28.0, M=M, seed=52)
+    a.params[0].useKnn = 1
+    w = workloads.Workload("mixed", a.params + b.params, np.concatenate([a.pos, b.pos]),
+                           np.concatenate([a.fwd, b.fwd]), np.concatenate([a.acc, b.acc]), None, 2, a.dt, {})
+    with make_engine(w) as eng:
+        for _ in range(2):
+            check_step(eng, w.params)
+
+
+@pytest.mark.parametrize("block", [64, 256])
+def test_knn_dense_blobs_with_features(block):
+    """The cooperative kNN scan where lists fill and most accepted candidates
+    replace an entry (Gaussian blobs at config 1's density, 8 relaxed
+    features), three steps, bit-exact lists and state."""
+    w = workloads.large(n=1 << 16, steps=3)
+    w.params[0].useKnn = 1
+    with make_engine(w) as eng:
+        eng.set_option("block_size", block)
+        for _ in range(3):
+            check_step(eng, w.params)
+
+
 @pytest.mark.parametrize("variant", ["knn", "maxbodies", "2d", "minradius_cos"])
 def test_variants(variant):
     w = workloads.plain(n=4000, L=40.0, M=6, seed=41)
