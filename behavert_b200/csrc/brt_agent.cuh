@@ -271,6 +271,18 @@ __device__ __forceinline__ uint32_t scanNeighborsPipelined(uint32_t self, f3 p, 
 // `self`, position p, home cell key `key`, flock `flock`).  Each agent's list
 // goes to column laneCol0 + lane of the shared array sList (stride ls).
 // Returns the lane's list length.
+// Rounds of 32 candidates the cooperative scan holds in registers: 96
+// candidates cover most home cells' 27-cell neighbourhoods at densities of 3
+// to 4 agents a cell (72 to 108 candidates).  Holding 4 measured the same on
+// the batched workload and 3% slower on config 1; 2 was slower on both.
+constexpr int kCoopCachedRounds = 3;
+// The windowed scan (flock kernel scan 5, the Schooling kernel) takes
+// further windows while at least this many of a run's agents still need
+// candidates (dense cells, e.g. config 1's Gaussian blobs): 4% faster on
+// config 1, 1% slower on the uniform batched workload, where runs are short.
+// 16 measured between the two.
+constexpr int kCoopWindowAgents = 8;
+
 // Position of the (w + 1)-th set bit of m (w < popc(m)): the largest q with
 // w or fewer set bits below it.
 __device__ __forceinline__ uint32_t nthSetBit(uint32_t m, uint32_t w) {

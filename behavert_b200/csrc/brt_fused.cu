@@ -33,16 +33,6 @@ namespace brt {
 // in windows of register-held rounds while a run has many open agents; each
 // its own instantiation so that it gets its own register allocation.
 //
-// Rounds of 32 candidates the cooperative scan holds in registers: 96
-// candidates cover most home cells' 27-cell neighbourhoods at densities of 3
-// to 4 agents a cell (72 to 108 candidates).  Holding 4 measured the same on
-// the batched workload and 3% slower on config 1; 2 was slower on both.
-constexpr int kCoopCachedRounds = 3;
-// Scan 5 takes further windows while at least this many of a run's agents
-// still need candidates (dense cells, e.g. config 1's Gaussian blobs): 4%
-// faster on config 1, 1% slower on the uniform batched workload, where runs
-// are short.  16 measured between the two.
-constexpr int kCoopWindowAgents = 8;
 // Scan 7 (the cooperative scan with bounding-box culling) stages each run's
 // surviving candidates in shared memory after the lists: (R + 1) rounds of
 // float4 per warp, from a 16-byte aligned word offset.

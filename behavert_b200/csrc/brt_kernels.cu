@@ -127,21 +127,37 @@ __device__ __forceinline__ void loadFeatures(const float* __restrict__ featS, ui
 
 // Fused neighbour search + flocking steering + clustering + obstacles +
 // feature relaxation + integration.  Lists stay in shared memory
-// ([k][thread] layout, conflict-free) unless recording is on.
+// ([k][thread] layout, odd stride) unless recording is on.  First-M lists
+// come from the warp-cooperative windowed scan (every lane of a warp takes
+// part; inactive lanes mirror the last agent read-only and leave after it),
+// kNN lists (maxNeighbors above a warp) from the per-agent scan.
 template <bool KNN>
 __global__ void __launch_bounds__(kFusedThreads) fusedKernel(FusedArgs A) {
   extern __shared__ uint32_t sList[];
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= A.n) return;
+  const uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = i0 < A.n;
+  if (KNN && !active) return;
+  const uint32_t i = active ? i0 : A.n - 1;
   const uint32_t f = A.nflocks == 1 ? 0u : flockOfSlot(A.agentBase, A.nflocks, i);
   const FlockDev& fl = A.flocks[f];
   const float4 p4 = __ldg(&A.posS[i]);
+  uint32_t* list = sList + threadIdx.x;
+  const uint32_t ls = blockDim.x + 1;
+  uint32_t n;
+  if constexpr (KNN) {
+    float distL[BRT_MAX_NEIGHBORS];
+    n = buildNeighborList<true>(i, xyz(p4), fl, A.cellStart, A.cellEnd, A.posS, list, ls, distL);
+  } else {
+    const f3 p = xyz(p4);
+    const uint32_t G = fl.G;
+    const uint32_t key = fl.cellBase + ((uint32_t)gridCoord(p.z, fl.cell, G) * G + (uint32_t)gridCoord(p.y, fl.cell, G)) * G +
+                         (uint32_t)gridCoord(p.x, fl.cell, G);
+    n = scanNeighborsCooperative<kCoopCachedRounds, kCoopWindowAgents>(active, i, p, key, A.flocks, f, A.cellStart,
+                                                                      A.cellEnd, A.posS, sList, ls, threadIdx.x & ~31u);
+    if (!active) return;
+  }
   const float4 w4 = __ldg(&A.fwdS[i]);
   const float4 a4 = __ldg(&A.accS[i]);
-  uint32_t* list = sList + threadIdx.x;
-  const uint32_t ls = blockDim.x;
-  float distL[KNN ? BRT_MAX_NEIGHBORS : 1];
-  const uint32_t n = buildNeighborList<KNN>(i, xyz(p4), fl, A.cellStart, A.cellEnd, A.posS, list, ls, distL);
   if (A.lists) {
     uint32_t* out = A.lists + (size_t)i * A.listStride;
     out[0] = n;
@@ -181,18 +197,35 @@ __global__ void __launch_bounds__(kFusedThreads) fusedKernel(FusedArgs A) {
 // ---------------------------------------------------------------------------
 // Stage-wise kernels (the reference's separate functionalities).
 
+// computeNeighborhoods: every agent's list into the list array.  First-M
+// lists come from the warp-cooperative windowed scan through shared memory
+// (inactive lanes take part read-only), kNN lists from the per-agent scan.
 template <bool KNN>
 __global__ void __launch_bounds__(128) listsKernel(StageArgs A) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= A.n) return;
+  extern __shared__ uint32_t sList[];
+  const uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = i0 < A.n;
+  if (KNN && !active) return;
+  const uint32_t i = active ? i0 : A.n - 1;
   const uint32_t f = A.nflocks == 1 ? 0u : flockOfSlot(A.agentBase, A.nflocks, i);
   const FlockDev& fl = A.flocks[f];
   uint32_t* out = A.lists + (size_t)i * A.listStride;
-  float distL[KNN ? BRT_MAX_NEIGHBORS : 1];
   const f3 p = xyz(__ldg(&A.posS[i]));
-  const uint32_t n = KNN ? buildNeighborList<KNN>(i, p, fl, A.cellStart, A.cellEnd, A.posS, out + 1, 1, distL)
-                         : scanNeighborsPipelined<4, true>(i, p, fl, A.cellStart, A.cellEnd, A.posS, out + 1, 1);
-  out[0] = n;
+  if constexpr (KNN) {
+    float distL[BRT_MAX_NEIGHBORS];
+    out[0] = buildNeighborList<true>(i, p, fl, A.cellStart, A.cellEnd, A.posS, out + 1, 1, distL);
+  } else {
+    const uint32_t G = fl.G;
+    const uint32_t key = fl.cellBase + ((uint32_t)gridCoord(p.z, fl.cell, G) * G + (uint32_t)gridCoord(p.y, fl.cell, G)) * G +
+                         (uint32_t)gridCoord(p.x, fl.cell, G);
+    const uint32_t ls = blockDim.x + 1;
+    const uint32_t n = scanNeighborsCooperative<kCoopCachedRounds, kCoopWindowAgents>(
+        active, i, p, key, A.flocks, f, A.cellStart, A.cellEnd, A.posS, sList, ls, threadIdx.x & ~31u);
+    if (!active) return;
+    const uint32_t* list = sList + threadIdx.x;
+    for (uint32_t k = 0; k < n; ++k) out[1 + k] = list[k * ls];
+    out[0] = n;
+  }
 }
 
 // which: 0 separation, 1 alignment, 2 cohesion, 3 clustering, 4 obstacles
@@ -323,14 +356,16 @@ cudaError_t launchReorder(const ReorderArgs& A, cudaStream_t st) {
   return cudaGetLastError();
 }
 cudaError_t configureFusedKernels(uint32_t Mmax) {
-  const int smem = (int)((size_t)kFusedThreads * Mmax * 4);
+  const int smem = (int)((size_t)(kFusedThreads + 1) * Mmax * 4);
   cudaError_t e = cudaFuncSetAttribute(fusedKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(fusedKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  e = cudaFuncSetAttribute(fusedKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(listsKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(129 * Mmax * 4));
 }
 cudaError_t launchFused(const FusedArgs& A, bool knn, cudaStream_t st) {
   if (A.n == 0) return cudaSuccess;
-  const size_t smem = (size_t)kFusedThreads * A.Mmax * 4;
+  const size_t smem = (size_t)(kFusedThreads + 1) * A.Mmax * 4;
   if (knn) fusedKernel<true><<<blocksFor(A.n, kFusedThreads), kFusedThreads, smem, st>>>(A);
   else fusedKernel<false><<<blocksFor(A.n, kFusedThreads), kFusedThreads, smem, st>>>(A);
   return cudaGetLastError();
@@ -338,7 +373,7 @@ cudaError_t launchFused(const FusedArgs& A, bool knn, cudaStream_t st) {
 cudaError_t launchLists(const StageArgs& A, bool knn, cudaStream_t st) {
   if (A.n == 0) return cudaSuccess;
   if (knn) listsKernel<true><<<blocksFor(A.n, 128), 128, 0, st>>>(A);
-  else listsKernel<false><<<blocksFor(A.n, 128), 128, 0, st>>>(A);
+  else listsKernel<false><<<blocksFor(A.n, 128), 128, (size_t)129 * (A.listStride - 1) * 4, st>>>(A);
   return cudaGetLastError();
 }
 // Registered per-agent arrays of `words` 32-bit words: slot i of dst takes

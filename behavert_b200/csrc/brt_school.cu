@@ -148,16 +148,27 @@ __device__ __forceinline__ void copyFeatures(const float* featS, float* featA, u
   for (uint32_t q = 0; q < Fs / 4; ++q) dst[q] = __ldg(&src[q]);
 }
 
+// The lists come from the warp-cooperative windowed scan (the flock
+// kernel's scan 5): every lane of a warp takes part, inactive lanes mirror
+// the last agent read-only and leave after the scan.
 __global__ void __launch_bounds__(128) schoolKernel(FusedArgs A) {
   extern __shared__ uint32_t sList[];
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= A.n) return;
+  const uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = i0 < A.n;
+  const uint32_t i = active ? i0 : A.n - 1;
   const uint32_t f = A.nflocks == 1 ? 0u : flockOfSlot(A.agentBase, A.nflocks, i);
   const FlockDev& fl = A.flocks[f];
-  const float4 p4 = __ldg(&A.posS[i]), w4 = __ldg(&A.fwdS[i]), a4 = __ldg(&A.accS[i]);
+  const float4 p4 = __ldg(&A.posS[i]);
+  const f3 p = xyz(p4);
+  const uint32_t G = fl.G;
+  const uint32_t key = fl.cellBase + ((uint32_t)gridCoord(p.z, fl.cell, G) * G + (uint32_t)gridCoord(p.y, fl.cell, G)) * G +
+                       (uint32_t)gridCoord(p.x, fl.cell, G);
+  const uint32_t ls = blockDim.x + 1;  // odd: one vote's rows fall in distinct banks
+  const uint32_t n = scanNeighborsCooperative<kCoopCachedRounds, kCoopWindowAgents>(
+      active, i, p, key, A.flocks, f, A.cellStart, A.cellEnd, A.posS, sList, ls, threadIdx.x & ~31u);
+  if (!active) return;
   uint32_t* list = sList + threadIdx.x;
-  const uint32_t ls = blockDim.x;
-  const uint32_t n = scanNeighborsPipelined<4, true>(i, xyz(p4), fl, A.cellStart, A.cellEnd, A.posS, list, ls);
+  const float4 w4 = __ldg(&A.fwdS[i]), a4 = __ldg(&A.accS[i]);
   if (A.lists) {
     uint32_t* out = A.lists + (size_t)i * A.listStride;
     out[0] = n;
@@ -216,7 +227,7 @@ __global__ void __launch_bounds__(128) schoolStageKernel(StageArgs A, int which)
 cudaError_t launchSchool(const FusedArgs& A, cudaStream_t st) {
   if (A.n == 0) return cudaSuccess;
   const uint32_t block = 128;
-  schoolKernel<<<(A.n + block - 1) / block, block, (size_t)block * A.Mmax * 4, st>>>(A);
+  schoolKernel<<<(A.n + block - 1) / block, block, (size_t)(block + 1) * A.Mmax * 4, st>>>(A);
   return cudaGetLastError();
 }
 
@@ -227,7 +238,7 @@ cudaError_t launchSchoolStage(const StageArgs& A, int which, cudaStream_t st) {
 }
 
 cudaError_t configureSchoolKernels(uint32_t Mmax) {
-  return cudaFuncSetAttribute(schoolKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(128 * Mmax * 4));
+  return cudaFuncSetAttribute(schoolKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(129 * Mmax * 4));
 }
 
 }  // namespace brt
