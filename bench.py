@@ -656,6 +656,9 @@ def main():
                     help="run this many config-4 adjoint iterations (taped forward + backward) and exit (for ncu)")
     ap.add_argument("--profile-flocks", type=int, default=0,
                     help="with --profile-steps: step the config-2 batched workload cut to this many flocks")
+    ap.add_argument("--profile-workload", default="large", choices=["large", "school1", "school2", "knn", "crowd"],
+                    help="with --profile-steps: config 1 (large), the Schooling law (mode 1 or 2), config 1 with "
+                         "kNN lists, or the crowd order's stage-wise step, each on 1,048,576 agents")
     ap.add_argument("--options", default="",
                     help="engine options key=value,... applied before stepping (replaces the autotuner)")
     args = ap.parse_args()
@@ -698,7 +701,18 @@ def main():
                 eng.adjoint_backward()
         return 0
 
-    w = workloads.batched(num_flocks=args.profile_flocks) if args.profile_steps and args.profile_flocks else workloads.large()
+    crowd = False
+    if args.profile_steps and args.profile_flocks:
+        w = workloads.batched(num_flocks=args.profile_flocks)
+    elif args.profile_steps and args.profile_workload in ("school1", "school2"):
+        w = workloads.schooling(n=1 << 20, L=256.0, mode=int(args.profile_workload[-1]))
+    elif args.profile_steps and args.profile_workload == "crowd":
+        w = workloads.plain(n=1 << 20, L=256.0, M=32, seed=5)
+        crowd = True
+    else:
+        w = workloads.large()
+        if args.profile_steps and args.profile_workload == "knn":
+            w.params[0].useKnn = 1
     eng = Engine(w.params, device=local)
     options = [kv.split("=") for kv in args.options.split(",") if kv]
     for key, val in options:
@@ -711,7 +725,10 @@ def main():
 
     if args.profile_steps:
         for _ in range(args.warmup + args.profile_steps):
-            eng.step(dt, 1)
+            if crowd:
+                eng.update_crowd(dt)
+            else:
+                eng.step(dt, 1)
         eng.sync()
         eng.close()
         return 0
