@@ -491,7 +491,9 @@ int brt_radix_sort_pairs(const uint32_t* pairs_in, uint32_t* pairs_out, uint32_t
      - it allocates nothing: no cudaMalloc, cudaFree or allocating library call.
    Results are identical to brt_radix_sort_pairs.  Before it returns, the call
    copies the device error word to the host and synchronises `stream`, so the
-   host waits for the sort to finish. */
+   host waits for the sort to finish; for the same reason it cannot be called
+   while `stream` is being captured into a CUDA graph (the capture would be
+   invalidated): use brt_radix_sort_pairs with caller-owned scratch there. */
 size_t brt_radix_sort_noalloc_max_pairs(void);
 int brt_radix_sort_pairs_noalloc(const uint32_t* pairs_in, uint32_t* pairs_out, uint32_t n,
                                  uint32_t bits, void* stream);
