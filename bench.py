@@ -128,6 +128,23 @@ def dist_setup(args):
     return world, rank, local
 
 
+def max_over_ranks(pg, ms: float, device) -> float:
+    """The largest of the ranks' device times (one all-reduce; every rank
+    calls it at the same point, and a single process returns its own)."""
+    if pg is None:
+        return ms
+    import torch
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(world: int, agents: int, steps: int, ms: float) -> float:
+    """Whole-job agent-steps/s of `world` replicas of `agents` agents each,
+    every one stepping `steps` steps, the job taking the slowest rank's `ms`."""
+    return world * agents * steps / (ms / 1e3)
+
+
 def _horizons(steps: int, horizon: int = E2E_HORIZON):
     """Split `steps` into runs of at most `horizon` steps, each restarting from
     the seeded state (config 1 is a 100-step run from its seeded state)."""
@@ -782,12 +799,9 @@ def main():
     elapsed_ms = e0.elapsed_time(e1)
     time.sleep(0.2)
     clocks.stop()
-    if pg:
-        t = torch.tensor([elapsed_ms], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+    elapsed_ms = max_over_ranks(pg, elapsed_ms, "cuda")
     ms_per_step = elapsed_ms / args.steps
-    value = world * n * args.steps / (elapsed_ms / 1e3)
+    value = replica_value(world, n, args.steps, elapsed_ms)
 
     # second timed pass: per-stage CUDA events (single-step launches from the seeded state)
     stage_steps = min(args.steps, E2E_HORIZON)
@@ -819,11 +833,8 @@ def main():
     e3.record(stream)
     e3.synchronize()
     e2e_ms = e2.elapsed_time(e3)
-    if pg:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * n * E2E_HORIZON * args.e2e_iters / (e2e_ms / 1e3)
+    e2e_ms = max_over_ranks(pg, e2e_ms, "cuda")
+    e2e_value = replica_value(world, n, E2E_HORIZON * args.e2e_iters, e2e_ms)
 
     # the same timed runs with the full onesweep sort on every step (the
     # incremental re-sort off), so the radix path stays measured
