@@ -1519,10 +1519,19 @@ int brt_engine_launch(brt_engine* e, brt_launch_fn fn, void* user_data) {
 }  // extern "C"
 
 namespace {
+// The kernels' dynamic shared-memory limits are per device and per function,
+// shared by every engine of the process: they follow the largest
+// maxNeighbors any engine on the device has asked for, so an engine created
+// later with shorter lists never lowers the limit another engine needs.
 int configureKernels(brt_engine* e) {
-  BRT_CUDA_TRY(configureFusedKernels(e->Mmax));
-  BRT_CUDA_TRY(configureFlockKernels(e->Mmax));
-  BRT_CUDA_TRY(configureSchoolKernels(e->Mmax));
+  static std::mutex mu;
+  static std::map<int, uint32_t> highWater;
+  std::lock_guard<std::mutex> lock(mu);
+  uint32_t& mx = highWater[e->device];
+  mx = std::max(mx, e->Mmax);
+  BRT_CUDA_TRY(configureFusedKernels(mx));
+  BRT_CUDA_TRY(configureFlockKernels(mx));
+  BRT_CUDA_TRY(configureSchoolKernels(mx));
   return BRT_OK;
 }
 }  // namespace

@@ -137,3 +137,24 @@ def test_autotune_keeps_state_and_results():
         out = eng.get_state()
     for a, b in zip(ref, out):
         assert np.array_equal(a, b)
+
+
+def test_engines_with_different_list_lengths_coexist():
+    """Kernel shared-memory limits are per device: an engine created later
+    with short lists must not lower the limit an earlier engine with long
+    lists needs (here 257 x 100 list words a block, above the default 48 KB)."""
+    big = workloads.plain(n=4096, L=32.0, M=100, steps=1)
+    small = workloads.plain(n=2048, L=32.0, M=8, steps=1)
+    ref = _run(big, 2, [("block_size", 256)])
+    with Engine(big.params) as a:
+        a.set_option("block_size", 256)
+        a.set_state(big.pos, big.fwd, big.acc, big.feat)
+        a.step(DT, 1)
+        with Engine(small.params) as b:
+            b.set_state(small.pos, small.fwd, small.acc, small.feat)
+            b.step(DT, 1)
+            a.step(DT, 1)
+            out = a.get_state()
+    for x, y in zip(ref, out):
+        if x is not None:
+            assert np.array_equal(x, y)
