@@ -251,8 +251,40 @@ class DeviceArrayWrapper {
   }
   // Double buffering is internal to the engine; kept for source compatibility.
   void swapPosReadWrite() {}
+  // The device arrays (DeviceArrayWrapper.h:87-90), for a plugin's own
+  // kernels.  A step reads the sorted copy of the state and writes the
+  // canonical one, so "read" is the sorted array of the current step (valid
+  // after reorderSimData) and "write" the canonical array in the engine's slot
+  // order; the engine's own buffers (borrowed, not owned by the wrapper).
+  // Features the engine computes (hash, cell starts, lists, steering force)
+  // have no separate write array: both calls give the same pointer.
+  Type* getReadDeviceArray() { return deviceArray(true); }
+  Type* getWriteDeviceArray() { return deviceArray(false); }
+  // DeviceArrayWrapper.h:165 stores the repository index a kernel's FETCH
+  // uses; kernels here take pointers, so the field receives the user array
+  // id (Feature::User) or the feature's number, for source compatibility.
+  void bindToField(int& field) { field = m_Feature == Feature::User ? (int)m_ArrayId : (int)m_Feature; }
 
  private:
+  Type* deviceArray(bool read) {
+    brt_arrays a;
+    check(brt_engine_get_arrays(m_CommonRes.engine(), &a), "brt_engine_get_arrays");
+    void* p = nullptr;
+    switch (m_Feature) {
+      case Feature::Position: p = read ? a.sorted_pos4 : a.pos4; break;
+      case Feature::Forward: p = read ? a.sorted_forward4 : a.forward4; break;
+      case Feature::SmoothAccel: p = read ? a.sorted_smooth_accel4 : a.smooth_accel4; break;
+      case Feature::Features: p = read ? a.sorted_features : a.features; break;
+      case Feature::CellStart: p = (void*)a.cell_start; break;
+      case Feature::NeighList: p = (void*)a.neighbor_lists; break;
+      case Feature::SteerForce: p = a.steer4; break;
+      case Feature::User: p = m_ArrayId < a.num_user ? a.user[m_ArrayId] : nullptr; break;
+      default: break;
+    }
+    if (!p) throw std::runtime_error("this feature has no device array in the engine's view");
+    return static_cast<Type*>(p);
+  }
+
   Feature m_Feature;
   int m_Size, m_Dimension;
   std::vector<Type> m_Host;

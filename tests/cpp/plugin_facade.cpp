@@ -58,7 +58,17 @@ int main(int argc, char** argv) {
 
   tag.copyArrayFromDevice();
   snapshot.copyArrayFromDevice();
-  bool ok = before && after;
+  // the wrappers' device arrays are the engine view's
+  brt_arrays view;
+  check(brt_engine_get_arrays(m_CommonRes.engine(), &view), "brt_engine_get_arrays");
+  int field = -1;
+  snapshot.bindToField(field);
+  const bool arraysOk = snapshot.getReadDeviceArray() == (float4v*)view.user[snapshot.getUserArrayId()] &&
+                        engine.getPos()->getWriteDeviceArray() == (float4v*)view.pos4 &&
+                        engine.getPos()->getReadDeviceArray() == (float4v*)view.sorted_pos4 &&
+                        field == (int)snapshot.getUserArrayId();
+  std::printf("device arrays: %s\n", arraysOk ? "yes" : "no");
+  bool ok = before && after && arraysOk;
   for (uint32_t i = 0; i < n && ok; ++i) ok = tag.getHostArray()[i] == 3u * i + 1u;
   const bool tagsOk = ok;
   ok = ok && std::memcmp(snapshot.getHostArray(), pos3.data(), n * sizeof(float4v)) == 0;
