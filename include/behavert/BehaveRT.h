@@ -200,6 +200,14 @@ class DeviceArrayWrapper {
       check(brt_engine_add_array(m_CommonRes.engine(), (uint32_t)(sizeof(Type) * dimension), &m_ArrayId),
             "brt_engine_add_array");
   }
+  // The reference's constructor for a plugin's own array
+  // (DeviceArrayWrapper.h:74-77): a per-agent array registered with the
+  // engine (Feature::User).  Double buffering is internal to the engine and
+  // there is no VBO (headless buffers), so the last two flags are accepted
+  // and ignored; size must be the engine's agent count.
+  DeviceArrayWrapper(DeviceInterface* /*deviceInterface*/, int size, int dimension = 1,
+                     bool /*useDoubleBufferingOnDevice*/ = true, bool /*useVbo*/ = false)
+      : DeviceArrayWrapper(Feature::User, size, dimension) {}
   uint32_t getUserArrayId() const { return m_ArrayId; }
   Type* getHostArray() { return m_Host.data(); }
   int getSize() const { return m_Size; }

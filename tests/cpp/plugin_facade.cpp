@@ -22,7 +22,8 @@ int main(int argc, char** argv) {
   const float dt = 0.1f;
   engine.reset();
 
-  DeviceArrayWrapper<uint32_t> tag(Feature::User, (int)n);
+  // the reference's constructor form: a plugin array on the device interface
+  DeviceArrayWrapper<uint32_t> tag(m_CommonRes.getDeviceInterface(), (int)n, 1, true, false);
   DeviceArrayWrapper<float4v> snapshot(Feature::User, (int)n);
   for (uint32_t i = 0; i < n; ++i) {
     const uint32_t v = 3u * i + 1u;
