@@ -401,6 +401,14 @@ class EnvGrid3DPlugIn : public Super {
   }
   // Agent id of the agent at sorted slot `index`.
   uint getSortedIndex(uint index, bool copyFromDevice = true) { return getHash()->getHostArrayElement((int)index, copyFromDevice).y; }
+  // addToFeaturesToReorder (EnvGrid3DPlugIn.h:101): every engine feature
+  // and every plugin array (Feature::User, registered when it is built) is
+  // already reordered with the agents at each step, so this only checks the
+  // wrapper is one of those.
+  template <class T>
+  void addToFeaturesToReorder(DeviceArrayWrapper<T>* feature, const void* /*type*/ = nullptr) {
+    if (!feature) throw std::runtime_error("addToFeaturesToReorder: no feature");
+  }
 
  protected:
   std::unique_ptr<DeviceArrayWrapper<float4v>> m_Pos;
@@ -524,9 +532,22 @@ class OpenSteerWrapperPlugIn : public Super {
   // The whole per-frame update of BehaveRT_Flocking.cpp:177-199 as one call
   // (fused kernel; nsteps > 1 runs a captured CUDA graph).
   void step(float elapsedTime, uint32_t nsteps = 1) { check(brt_step(m_CommonRes.engine(), elapsedTime, nsteps), "brt_step"); }
+  // calcInverseHash (OpenSteerWrapperPlugIn.h:278-284, calcInverseHashD,
+  // envgrid3d_kernel.cu:70-78), the reference's host-debugging map from agent
+  // id to the agent's sorted slot, built on the host from the sorted hash.
+  void calcInverseHash() {
+    const uint32_t n = m_CommonRes.params().numBodies;
+    std::vector<uint32_t> keys(n), ids(n);
+    check(brt_get_hash(m_CommonRes.engine(), keys.data(), ids.data(), BRT_MEM_HOST), "calcInverseHash");
+    m_InverseHash.assign(n, 0u);
+    for (uint32_t i = 0; i < n; ++i)
+      if (ids[i] < n) m_InverseHash[ids[i]] = i;
+  }
+  const std::vector<uint32_t>& getInverseHash() const { return m_InverseHash; }
 
  protected:
   std::unique_ptr<DeviceArrayWrapper<float4v>> m_Forward, m_Accel, m_Steer;
+  std::vector<uint32_t> m_InverseHash;
 };
 
 // BehaviorClusteringPlugIn (PlugIns/BehaviorClustering/include/BehaviorClusteringPlugIn.h:60-230)
@@ -582,6 +603,45 @@ class BehaviorClusteringPlugIn : public Super {
     check(brt_get_cluster_membership(m_CommonRes.engine(), (float*)out.data(), BRT_MEM_HOST), "getClusterMembership");
     return out;
   }
+  // mergeClusters (BehaviorClusteringPlugIn.h:930-952, kernel
+  // BehaviorClustering_MergeClusters_kernel, BehaviorClustering_kernel.cu:
+  // 697-742): the agents whose leader is one of the two leaders head for the
+  // other leader at the maximum speed, forward = normalize(other leader's
+  // position - own leader's position); the rest keep their forward.  Leaders
+  // are labels of the last computeClusterMembership (sorted slots of that
+  // step), as the reference's mergeClusterLeaders; equal leaders do nothing.
+  // Runs on the host over the engine's state (an interactive operation of
+  // the demo, not part of a step).
+  void mergeClusters(int leaderA, int leaderB) {
+    if (leaderA == leaderB) return;
+    brt_engine* e = m_CommonRes.engine();
+    const uint32_t n = m_CommonRes.params().numBodies;
+    const std::vector<float4v> member = getClusterMembership();
+    std::vector<uint32_t> keys(n), ids(n);
+    check(brt_get_hash(e, keys.data(), ids.data(), BRT_MEM_HOST), "mergeClusters");
+    std::vector<float4v> pos(n), fwd(n);
+    check(brt_get_state(e, (float*)pos.data(), (float*)fwd.data(), nullptr, nullptr, BRT_MEM_HOST), "mergeClusters");
+    auto leaderPos = [&](int leader) -> float4v {
+      if (leader < 0 || (uint32_t)leader >= n) throw std::runtime_error("mergeClusters: leader out of range");
+      return pos[ids[(uint32_t)leader]];
+    };
+    const float4v pa = leaderPos(leaderA), pb = leaderPos(leaderB);
+    const float speed = m_CommonRes.params().commonMaxSpeed;
+    for (uint32_t id = 0; id < n; ++id) {
+      const int mine = (int)member[id].x;
+      if (mine != leaderA && mine != leaderB) continue;
+      const float4v& from = mine == leaderA ? pa : pb;
+      const float4v& to = mine == leaderA ? pb : pa;
+      const float dx = to.x - from.x, dy = to.y - from.y, dz = to.z - from.z;
+      const float inv = 1.0f / std::sqrt(dx * dx + dy * dy + dz * dz);
+      fwd[id] = float4v{dx * inv, dy * inv, dz * inv, speed};
+    }
+    check(brt_set_state(e, nullptr, (const float*)fwd.data(), nullptr, nullptr, BRT_MEM_HOST), "mergeClusters");
+  }
+  // freezeClusters (BehaviorClusteringPlugIn.h:958-967): the reference's
+  // freeze kernel (BehaviorClustering_kernel.cu:749-757) has an empty body,
+  // so the operation changes nothing.
+  void freezeClusters(int /*leader*/) {}
   DeviceArrayWrapper<float>* getFeaturesVector() {
     if (!m_Features)
       m_Features.reset(new DeviceArrayWrapper<float>(Feature::Features, (int)m_CommonRes.params().numBodies,

@@ -72,3 +72,19 @@ def test_configuration_mapping(tmp_path, cfg, cap):
     got = dict(zip(fields[0::2], fields[1::2]))
     assert int(got["maxBodiesPerCell"]) == cap
     assert int(got["numBodies"]) == (1 << 10 if cfg == "automatic_cap.cfg" else 1 << 12)
+
+
+def test_cluster_application_builds(tmp_path):
+    _build("cluster_facade", tmp_path / "cluster_facade")
+
+
+@pytest.mark.gpu
+def test_cluster_inverse_hash_and_merge(tmp_path):
+    """calcInverseHash against getSortedIndex, mergeClusters against a host
+    restatement of the reference's merge kernel, freezeClusters a no-op."""
+    exe = tmp_path / "cluster_facade"
+    _build("cluster_facade", exe)
+    res = subprocess.run([str(exe), str(ROOT / "tests" / "cpp" / "flocking.cfg")], capture_output=True, text=True)
+    print(res.stdout, res.stderr)
+    assert res.returncode == 0, res.stdout + res.stderr
+    assert "inverse hash: yes" in res.stdout and ": yes" in res.stdout.split("merged")[1]
