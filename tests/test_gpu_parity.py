@@ -12,7 +12,8 @@ maximum per agent and the normwise error are reported).
 Horizons: config 0 is compared at every one of its 200 steps and over the
 whole 200-step trajectory; config 1 at full size (1,048,576 agents) at each of
 its first 10 steps (the incremental re-sort from step 2 on) and at the end of
-its 100-step horizon.
+its 100-step horizon; configs 2 and 4 at full size (10.9 M and 2.7 M agents)
+at their first two steps.
 """
 import numpy as np
 import pytest
@@ -288,6 +289,26 @@ def test_graph_equals_single_steps():
 
 def test_batched_small():
     w = workloads.batched(num_flocks=24, lo=50, hi=3000, seed=7)
+    with make_engine(w) as eng:
+        for _ in range(2):
+            check_step(eng, w.params)
+
+
+def test_batched_full_size_first_two_steps():
+    """Config 2 at full size (1,024 flocks, 10.9 M agents): step 1 (full radix
+    sort on the (flock, cell) key) and step 2 (incremental re-sort), lists,
+    order and FP32 state bit-exact against the oracle, and within the FP64
+    tolerances."""
+    w = workloads.batched()
+    with make_engine(w) as eng:
+        for _ in range(2):
+            check_step(eng, w.params)
+
+
+def test_fitting_full_size_first_two_steps():
+    """Config 4 at full size (256 flocks, 2.7 M agents, 32 sphere obstacles
+    each): two steps against the FP32 and FP64 oracle."""
+    w = workloads.fitting()
     with make_engine(w) as eng:
         for _ in range(2):
             check_step(eng, w.params)
