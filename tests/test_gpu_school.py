@@ -47,6 +47,31 @@ def test_one_step_bit_exact(mode):
 
 
 @pytest.mark.parametrize("mode", [1, 2])
+def test_full_size_two_steps_bit_exact(mode):
+    """1,048,576 agents in the cube of side 256 (the size the benchmark
+    measures): two steps, lists, order and state bit-exact."""
+    o = _oracle()
+    w = workloads.schooling(n=1 << 20, L=256.0, mode=mode)
+    with Engine(w.params) as eng:
+        eng.set_state(w.pos, w.fwd, w.acc)
+        p, f, a = w.pos, w.fwd, w.acc
+        for s in range(2):
+            eng.record_lists(True)
+            eng.step(w.dt, 1)
+            keys, ids = eng.getHash()
+            lists = eng.getNeighborLists()
+            pos, fwd, acc, _ = eng.get_state(features=False)
+            r = o.step(w.params, p, f, a, dt=w.dt, mode=0, random_step=s + 1)
+            assert np.array_equal(keys, r["keys"]) and np.array_equal(ids, r["ids"])
+            cnt = lists[:, 0]
+            assert np.array_equal(cnt, r["lists"][:, 0])
+            mask = np.arange(lists.shape[1] - 1)[None, :] < cnt[:, None]
+            assert np.array_equal(np.where(mask, lists[:, 1:], 0), np.where(mask, r["lists"][:, 1:], 0))
+            assert np.array_equal(pos, r["pos"]) and np.array_equal(fwd, r["fwd"]) and np.array_equal(acc, r["acc"])
+            p, f, a = pos, fwd, acc
+
+
+@pytest.mark.parametrize("mode", [1, 2])
 def test_ten_steps_bit_exact(mode):
     o = _oracle()
     w = workloads.schooling(n=4096, L=64.0, mode=mode)
