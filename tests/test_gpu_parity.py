@@ -364,6 +364,16 @@ def test_knn_dense_blobs_with_features(block):
             check_step(eng, w.params)
 
 
+def test_knn_full_size_first_two_steps():
+    """Config 1 at full size with kNN lists (the nearest 32 kept; the
+    cooperative kNN scan): two steps against the FP32 and FP64 oracle."""
+    w = workloads.large()
+    w.params[0].useKnn = 1
+    with make_engine(w) as eng:
+        for _ in range(2):
+            check_step(eng, w.params)
+
+
 @pytest.mark.parametrize("variant", ["knn", "maxbodies", "2d", "minradius_cos"])
 def test_variants(variant):
     w = workloads.plain(n=4000, L=40.0, M=6, seed=41)
