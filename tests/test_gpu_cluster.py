@@ -35,6 +35,26 @@ def test_membership_and_hit_rate_match_restatement(iterations):
         assert np.all(labels[:, 0] <= ref_labels.max())
 
 
+def test_membership_and_hit_rate_full_size():
+    """Config 1 at full size after one step: 10 label-propagation sweeps and
+    the hit rate, equal to the restatement."""
+    from oracle import oracle
+    w = workloads.large(steps=1)
+    with Engine(w.params) as eng:
+        eng.record_lists(True)
+        eng.set_state(w.pos, w.fwd, w.acc, w.feat)
+        eng.step(w.dt, 1)
+        eng.computeClusterMembership(10)
+        labels = eng.getClusterMembership()[:, 0].copy()
+        eng.analyzeClusterHitRate(1.5)
+        hr = eng.getClusterMembership()
+    o = oracle.step(w.params, w.pos, w.fwd, w.acc, w.feat, dt=w.dt)
+    ref_labels = oracle.cluster_membership(o, 10)
+    assert np.array_equal(labels, ref_labels)
+    ref = oracle.cluster_hit_rate(w.params, w.pos, o, ref_labels, 1.5)
+    assert np.array_equal(hr[:, :3], ref[:, :3])
+
+
 def test_stagewise_lists_and_errors():
     w = workloads.plain(n=2048, L=32.0, steps=1)
     with Engine(w.params) as eng:

@@ -222,6 +222,23 @@ def test_crowd_order_steer_and_slow_to_avoid_neighbors():
     assert e["vel_over"] <= MAX_FRAC_OVER, e
 
 
+def test_crowd_order_full_size_one_step():
+    """The crowd order, stage by stage, on 1,048,576 agents (the size the
+    benchmark measures): lists and FP32 state bit-exact."""
+    w = workloads.plain(n=1 << 20, L=256.0, M=32, seed=5, steps=1)
+    with make_engine(w) as eng:
+        pos, fwd, acc, _ = eng.get_state()
+        eng.update_crowd(w.dt)
+        lists = eng.getNeighborLists()
+        gpos, gfwd, gacc, _ = eng.get_state()
+    o = oracle.step(w.params, pos, fwd, acc, dt=w.dt, mode=0, avoid_neighbors=True)
+    cnt = lists[:, 0]
+    assert np.array_equal(cnt, o["lists"][:, 0])
+    mask = np.arange(lists.shape[1] - 1)[None, :] < cnt[:, None]
+    assert np.array_equal(np.where(mask, lists[:, 1:], 0), np.where(mask, o["lists"][:, 1:], 0))
+    assert _same_bits(gpos, o["pos"]) and _same_bits(gfwd, o["fwd"]) and _same_bits(gacc, o["acc"])
+
+
 def test_crowd_order_with_move_away_from_base():
     """The crowd order with steerForMoveAwayBaseTarget after cohesion, stage
     by stage through the C-ABI, against the oracle."""
