@@ -125,29 +125,44 @@ __global__ void __launch_bounds__(kAdjointThreads, kAdjointMinBlocks) adjointSte
     f3 sSep = mk3(0.f, 0.f, 0.f), sAli = mk3(0.f, 0.f, 0.f), sCoh = mk3(0.f, 0.f, 0.f);
     Comp3 cpSep, cpAli, cpCoh;
     uint32_t cSep = 0, cAli = 0, cCoh = 0, mS = 0, mA = 0, mC = 0;
+    // Memberships as the flock kernel decides them: with the angle test
+    // inactive (cosFree), exact squared-distance thresholds; otherwise the
+    // distance and the cosine (both forms decide the same, bit for bit).
+    const bool cosFree = dot3(a.fwd, a.fwd) * 1.002f < fl.cosBound2;
     for (uint32_t k = 0; k < n; ++k) {
       const uint32_t j = lst[1 + k];
       const f3 other = neighborImage(a, __ldg(&A.posS[j]), fl);
       const f3 offset = sub3(other, a.pos);
       const float d2 = dot3(offset, offset);
-      const float dist = sqrtf(d2);
-      const f3 nrm = mul3(offset, 1.0f / dist);
-      const float cosAngle = dot3(a.fwd, nrm);
-      if (inBoid(dist, cosAngle, fl.minR, fl.sep[1], fl.sep[2])) {
+      bool inS, inA, inC;
+      if (cosFree && d2 >= 1e-30f) {
+        const bool lo = d2 < fl.minT;
+        inS = lo || !(d2 > fl.sepT);
+        inA = lo || !(d2 > fl.aliT);
+        inC = lo || !(d2 > fl.cohT);
+      } else {
+        const float dist = sqrtf(d2);
+        const f3 nrm = mul3(offset, 1.0f / dist);
+        const float cosAngle = dot3(a.fwd, nrm);
+        inS = inBoid(dist, cosAngle, fl.minR, fl.sep[1], fl.sep[2]);
+        inA = inBoid(dist, cosAngle, fl.minR, fl.ali[1], fl.ali[2]);
+        inC = inBoid(dist, cosAngle, fl.minR, fl.coh[1], fl.coh[2]);
+      }
+      if (inS) {
         const f3 t = div3(offset, -d2);
         sSep = add3(sSep, t);
         cpSep.add(t);
         ++cSep;
         mS |= 1u << k;
       }
-      if (inBoid(dist, cosAngle, fl.minR, fl.ali[1], fl.ali[2])) {
+      if (inA) {
         const f3 fj = xyz(__ldg(&A.fwdS[j]));
         sAli = add3(sAli, fj);
         cpAli.add(sub3(fj, a.fwd));
         ++cAli;
         mA |= 1u << k;
       }
-      if (inBoid(dist, cosAngle, fl.minR, fl.coh[1], fl.coh[2])) {
+      if (inC) {
         sCoh = add3(sCoh, other);
         cpCoh.add(offset);
         ++cCoh;
