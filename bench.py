@@ -855,11 +855,29 @@ def main():
     achieved = fused_bytes / (fused_ms / 1e3) / 1e9 if fused_ms > 0 else None
     traffic_file = ROOT / "profiles" / "flockKernel_config1_traffic.json"
     traffic = None
+    warp_insts = None
     if traffic_file.exists():
         try:
-            traffic = json.loads(traffic_file.read_text()).get("bytes_per_launch")
+            tj = json.loads(traffic_file.read_text())
+            traffic = tj.get("bytes_per_launch")
+            warp_insts = tj.get("warp_instructions_per_launch")
         except Exception:
             traffic = None
+    # The flock kernel is bound by instruction issue, not by HBM: its ncu
+    # warp-instruction count (committed beside the traffic) against the SM
+    # issue peak (SMs x 4 schedulers x 1 instruction a cycle at the clock
+    # sampled during the timed region), over the measured launch time.
+    clock_summary = clocks.summary(t_wall0, t_wall1)
+    sm_mhz = clock_summary.get("sm_mhz") or clock_summary.get("sm_max_mhz")
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    issue = None
+    if warp_insts and sm_mhz and fused_ms > 0:
+        peak_issue = sms * 4 * sm_mhz * 1e6
+        issue = {"warp_instructions_per_launch": warp_insts, "peak_warp_instructions_per_s": peak_issue,
+                 "achieved_warp_instructions_per_s": warp_insts / (fused_ms / 1e3),
+                 "frac": warp_insts / (fused_ms / 1e3) / peak_issue, "sm_mhz": sm_mhz, "sms": sms,
+                 "source": "warp instructions from one ncu capture (profiles/flockKernel_config1_traffic.json), "
+                           "time from this run's stage events"}
     step_gbs = ab["per_agent_step"] * n / (ms_per_step / 1e3) / 1e9
 
     line = {
@@ -879,7 +897,8 @@ def main():
                      "peak_source": peak_kind,
                      "alg_bytes_per_launch": fused_bytes,
                      "step_alg_bytes_per_agent": ab["per_agent_step"],
-                     "step_achieved_gbs": step_gbs, "step_frac": step_gbs / hbm},
+                     "step_achieved_gbs": step_gbs, "step_frac": step_gbs / hbm,
+                     "issue": issue},
         "stages_ms": {"hash": stage_avg[0], "sort": stage_avg[1], "reorder": stage_avg[2], "fused": stage_avg[3],
                       "timed_steps": timed},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes / E2E_HORIZON,
@@ -887,7 +906,7 @@ def main():
                 "note": "each call: upload state, %d-step horizon, read state back" % E2E_HORIZON},
         "gpu_launches": args.steps * launches_per_step + 4 * len(horizons),
         "full_sort_ms_per_step": full_sort_ms,
-        "clocks": clocks.summary(t_wall0, t_wall1),
+        "clocks": clock_summary,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base, accuracy = cpu_baseline_leg(w, state_before, state_after)
@@ -922,6 +941,9 @@ def summary_keys(line: dict) -> dict:
     """Flat scalar copies of the legs' headline figures, so that a reader of
     the top level sees them without the nested objects."""
     out = {}
+    iss = (line.get("roofline") or {}).get("issue")
+    if iss:
+        out["flock_kernel_issue_frac"] = iss["frac"]
     acc = line.get("accuracy")
     if acc:
         out["fp64_max_rel_err"] = max(acc[k]["max"] for k in ("pos_vs_fp64", "vel_vs_fp64", "feat_vs_fp64"))
