@@ -255,8 +255,7 @@ int stageMark(brt_engine* e, int k) {
 
 // hash -> sort -> reorder + cell ranges
 ResortArgs resortArgs(brt_engine* e) {
-  ResortArgs A;
-  std::memset(&A, 0, sizeof(A));
+  ResortArgs A{};
   A.pos = e->posA; A.id = e->idA; A.prevPairs = e->pairs[e->plan.passes & 1];
   A.cellStart = e->cellStart; A.cellEnd = e->cellEnd;
   A.flocks = e->flocks; A.agentBase = e->agentBase;
