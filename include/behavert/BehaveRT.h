@@ -196,6 +196,10 @@ class DeviceArrayWrapper {
  public:
   DeviceArrayWrapper(Feature feature, int size, int dimension = 1)
       : m_Feature(feature), m_Size(size), m_Dimension(dimension), m_Host((size_t)size * dimension) {
+    // every feature but the cell starts holds one row per agent, and the
+    // engine copies all of them to and from the host image
+    if (feature != Feature::CellStart && (uint32_t)size != m_CommonRes.params().numBodies)
+      throw std::runtime_error("DeviceArrayWrapper: this feature holds one element per agent (size = numBodies)");
     if (feature == Feature::User)
       check(brt_engine_add_array(m_CommonRes.engine(), (uint32_t)(sizeof(Type) * dimension), &m_ArrayId),
             "brt_engine_add_array");

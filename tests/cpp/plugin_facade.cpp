@@ -69,7 +69,15 @@ int main(int argc, char** argv) {
                         engine.getPos()->getReadDeviceArray() == (float4v*)view.sorted_pos4 &&
                         field == (int)snapshot.getUserArrayId();
   std::printf("device arrays: %s\n", arraysOk ? "yes" : "no");
-  bool ok = before && after && arraysOk;
+  // a plugin array holds one element per agent: other sizes are refused
+  bool refused = false;
+  try {
+    DeviceArrayWrapper<uint32_t> bad(Feature::User, (int)n - 1);
+  } catch (const std::runtime_error&) {
+    refused = true;
+  }
+  std::printf("wrong size refused: %s\n", refused ? "yes" : "no");
+  bool ok = before && after && arraysOk && refused;
   for (uint32_t i = 0; i < n && ok; ++i) ok = tag.getHostArray()[i] == 3u * i + 1u;
   const bool tagsOk = ok;
   ok = ok && std::memcmp(snapshot.getHostArray(), pos3.data(), n * sizeof(float4v)) == 0;
