@@ -391,7 +391,7 @@ extern "C" {
 int brt_adjoint_forward(brt_engine* e, float elapsedTime, uint32_t nsteps, uint32_t checkpoint_every,
                         const float* target_pos4, int where, double* loss_per_flock) {
   if (!e || !target_pos4 || nsteps == 0 || checkpoint_every == 0) { setLastError("brt_adjoint_forward: bad arguments"); return BRT_ERR_ARG; }
-  if (where != BRT_MEM_HOST && where != BRT_MEM_DEVICE) return BRT_ERR_ARG;
+  if (where != BRT_MEM_HOST && where != BRT_MEM_DEVICE) return brt::argError(__func__);
   if (e->N == 0) return BRT_OK;
   int rc = checkSupported(e);
   if (rc) return rc;
@@ -420,9 +420,9 @@ int brt_adjoint_forward(brt_engine* e, float elapsedTime, uint32_t nsteps, uint3
 int brt_adjoint_backward(brt_engine* e, const double* loss_scale, const float* gpos4_T, const float* gfwd4_T,
                          const float* gacc4_T, int where_in, float* grad_pos4, float* grad_fwd4, float* grad_vel4,
                          float* grad_acc4, double* grad_weights, int where_out) {
-  if (!e) return BRT_ERR_ARG;
+  if (!e) return brt::argError(__func__);
   if ((where_in != BRT_MEM_HOST && where_in != BRT_MEM_DEVICE) || (where_out != BRT_MEM_HOST && where_out != BRT_MEM_DEVICE))
-    return BRT_ERR_ARG;
+    return brt::argError(__func__);
   AdjointState* a = e->adj;
   if (!a || !a->taped) { setLastError("brt_adjoint_backward: no taped forward (call brt_adjoint_forward first)"); return BRT_ERR_STATE; }
   if (a->version != e->paramsVersion || a->weightsVersion != e->weightsVersion) {
@@ -463,7 +463,7 @@ int brt_adjoint_backward(brt_engine* e, const double* loss_scale, const float* g
 }
 
 int brt_adjoint_get_tape(brt_engine* e, uint32_t* lists_by_id, uint32_t* flags_by_id, int where) {
-  if (!e) return BRT_ERR_ARG;
+  if (!e) return brt::argError(__func__);
   AdjointState* a = e->adj;
   if (!e->adjointExport || !a || !a->expLists || a->capExport < a->T) {
     setLastError("brt_adjoint_get_tape: enable option adjoint_export before brt_adjoint_forward");
@@ -479,13 +479,13 @@ int brt_adjoint_get_tape(brt_engine* e, uint32_t* lists_by_id, uint32_t* flags_b
 }
 
 int brt_adjoint_get_tape_states(brt_engine* e, float* pos4, float* fwd4, float* acc4, int where) {
-  if (!e) return BRT_ERR_ARG;
+  if (!e) return brt::argError(__func__);
   AdjointState* a = e->adj;
   if (!e->adjointExport || !a || !a->expState || a->capExport < a->T) {
     setLastError("brt_adjoint_get_tape_states: enable option adjoint_export before brt_adjoint_forward");
     return BRT_ERR_STATE;
   }
-  if (where != BRT_MEM_HOST && where != BRT_MEM_DEVICE) return BRT_ERR_ARG;
+  if (where != BRT_MEM_HOST && where != BRT_MEM_DEVICE) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   const size_t n = e->N;
   float* dst[3] = {pos4, fwd4, acc4};
@@ -500,8 +500,8 @@ int brt_adjoint_get_tape_states(brt_engine* e, float* pos4, float* fwd4, float* 
 }
 
 int brt_set_steering_weights(brt_engine* e, const float* weights3, int where) {
-  if (!e || !weights3) return BRT_ERR_ARG;
-  if (where != BRT_MEM_HOST && where != BRT_MEM_DEVICE) return BRT_ERR_ARG;
+  if (!e || !weights3) return brt::argError(__func__);
+  if (where != BRT_MEM_HOST && where != BRT_MEM_DEVICE) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   e->weightsVersion++;
   if (where == BRT_MEM_HOST) {
@@ -536,8 +536,8 @@ int brt_set_steering_weights(brt_engine* e, const float* weights3, int where) {
 }
 
 int brt_get_steering_weights(brt_engine* e, float* weights3, int where) {
-  if (!e || !weights3) return BRT_ERR_ARG;
-  if (where != BRT_MEM_HOST && where != BRT_MEM_DEVICE) return BRT_ERR_ARG;
+  if (!e || !weights3) return brt::argError(__func__);
+  if (where != BRT_MEM_HOST && where != BRT_MEM_DEVICE) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   if (where == BRT_MEM_HOST) {
     for (uint32_t f = 0; f < e->nflocks; ++f) {

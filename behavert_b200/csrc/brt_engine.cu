@@ -468,7 +468,7 @@ const char* brt_error_string(int status) {
 const char* brt_last_error(void) { return tlsLastError.c_str(); }
 
 int brt_device_count(int* count) {
-  if (!count) return BRT_ERR_ARG;
+  if (!count) return brt::argError(__func__);
   *count = 0;
   cudaError_t err = cudaGetDeviceCount(count);
   if (err != cudaSuccess) { *count = 0; cudaGetLastError(); }
@@ -476,7 +476,7 @@ int brt_device_count(int* count) {
 }
 
 int brt_params_default(brt_params* p) {
-  if (!p) return BRT_ERR_ARG;
+  if (!p) return brt::argError(__func__);
   std::memset(p, 0, sizeof(*p));
   p->numBodies = 4096;
   p->commonRadius = 1.0f;
@@ -647,7 +647,7 @@ int brt_engine_create(const brt_params* flocks, uint32_t num_flocks, int device,
 }
 
 int brt_engine_destroy(brt_engine* e) {
-  if (!e) return BRT_ERR_ARG;
+  if (!e) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   cudaStreamSynchronize(e->stream);
   freeAll(e);
@@ -656,17 +656,17 @@ int brt_engine_destroy(brt_engine* e) {
 }
 
 int brt_engine_num_agents(const brt_engine* e, uint32_t* n) {
-  if (!e || !n) return BRT_ERR_ARG;
+  if (!e || !n) return brt::argError(__func__);
   *n = e->N;
   return BRT_OK;
 }
 int brt_engine_num_cells(const brt_engine* e, uint32_t* c) {
-  if (!e || !c) return BRT_ERR_ARG;
+  if (!e || !c) return brt::argError(__func__);
   *c = e->C;
   return BRT_OK;
 }
 int brt_neighbor_list_stride(const brt_engine* e, uint32_t* stride) {
-  if (!e || !stride) return BRT_ERR_ARG;
+  if (!e || !stride) return brt::argError(__func__);
   *stride = e->listStride;
   return BRT_OK;
 }
@@ -713,7 +713,7 @@ int brt_engine_set_params(brt_engine* e, uint32_t flock, const brt_params* p) {
 }
 
 int brt_engine_set_option(brt_engine* e, const char* key, int64_t value) {
-  if (!e || !key) return BRT_ERR_ARG;
+  if (!e || !key) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   const std::string k(key);
   if (k == "two_pass") {
@@ -786,25 +786,25 @@ int brt_engine_set_option(brt_engine* e, const char* key, int64_t value) {
 }
 
 int brt_engine_stream(brt_engine* e, void** stream) {
-  if (!e || !stream) return BRT_ERR_ARG;
+  if (!e || !stream) return brt::argError(__func__);
   *stream = (void*)e->stream;
   return BRT_OK;
 }
 
 int brt_sync(brt_engine* e) {
-  if (!e) return BRT_ERR_ARG;
+  if (!e) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   return syncAndCheck(e);
 }
 
 int brt_engine_record_lists(brt_engine* e, int enable) {
-  if (!e) return BRT_ERR_ARG;
+  if (!e) return brt::argError(__func__);
   e->recordLists = enable != 0;
   return BRT_OK;
 }
 
 int brt_engine_check_device_error(brt_engine* e, uint32_t* word) {
-  if (!e || !word) return BRT_ERR_ARG;
+  if (!e || !word) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   BRT_CUDA_TRY(cudaMemcpyAsync(word, e->errWord, 4, cudaMemcpyDeviceToHost, e->stream));
   BRT_CUDA_TRY(cudaStreamSynchronize(e->stream));
@@ -817,8 +817,8 @@ int brt_engine_check_device_error(brt_engine* e, uint32_t* word) {
 // ---- feature I/O ------------------------------------------------------------
 
 int brt_set_state(brt_engine* e, const float* pos4, const float* fwd4, const float* acc4, const float* features, int where) {
-  if (!e) return BRT_ERR_ARG;
-  if (where != BRT_MEM_HOST && where != BRT_MEM_DEVICE) return BRT_ERR_ARG;
+  if (!e) return brt::argError(__func__);
+  if (where != BRT_MEM_HOST && where != BRT_MEM_DEVICE) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   cudaStream_t st = e->stream;
   const size_t n = e->N;
@@ -858,8 +858,8 @@ int brt_set_state(brt_engine* e, const float* pos4, const float* fwd4, const flo
 }
 
 int brt_get_state(brt_engine* e, float* pos4, float* fwd4, float* acc4, float* features, int where) {
-  if (!e) return BRT_ERR_ARG;
-  if (where != BRT_MEM_HOST && where != BRT_MEM_DEVICE) return BRT_ERR_ARG;
+  if (!e) return brt::argError(__func__);
+  if (where != BRT_MEM_HOST && where != BRT_MEM_DEVICE) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   cudaStream_t st = e->stream;
   const size_t n = e->N;
@@ -888,7 +888,7 @@ int brt_get_state(brt_engine* e, float* pos4, float* fwd4, float* acc4, float* f
 }
 
 int brt_set_similarity_stats(brt_engine* e, const float* stats4, int where) {
-  if (!e || !stats4) return BRT_ERR_ARG;
+  if (!e || !stats4) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   BRT_CUDA_TRY(cudaMemcpyAsync(e->statsById, stats4, (size_t)e->N * 16,
                                where == BRT_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, e->stream));
@@ -897,7 +897,7 @@ int brt_set_similarity_stats(brt_engine* e, const float* stats4, int where) {
 }
 
 int brt_get_similarity_stats(brt_engine* e, float* stats4, int where) {
-  if (!e || !stats4) return BRT_ERR_ARG;
+  if (!e || !stats4) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   BRT_CUDA_TRY(cudaMemcpyAsync(stats4, e->statsById, (size_t)e->N * 16,
                                where == BRT_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, e->stream));
@@ -908,7 +908,7 @@ int brt_get_similarity_stats(brt_engine* e, float* stats4, int where) {
 // ---- fused step --------------------------------------------------------------
 
 int brt_step(brt_engine* e, float elapsedTime, uint32_t nsteps) {
-  if (!e) return BRT_ERR_ARG;
+  if (!e) return brt::argError(__func__);
   if (nsteps == 0 || e->N == 0) return BRT_OK;
   DeviceGuard guard(e->device);
   const bool record = e->recordLists;
@@ -927,7 +927,7 @@ int brt_step(brt_engine* e, float elapsedTime, uint32_t nsteps) {
 }
 
 int brt_step_prepare(brt_engine* e, float elapsedTime, uint32_t nsteps) {
-  if (!e) return BRT_ERR_ARG;
+  if (!e) return brt::argError(__func__);
   if (nsteps < 2 || e->N == 0) return BRT_OK;
   DeviceGuard guard(e->device);
   cudaGraphExec_t ge = nullptr;
@@ -935,7 +935,7 @@ int brt_step_prepare(brt_engine* e, float elapsedTime, uint32_t nsteps) {
 }
 
 int brt_engine_stage_timing(brt_engine* e, int enable) {
-  if (!e) return BRT_ERR_ARG;
+  if (!e) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   if (enable && !e->ev[0][0]) {
     for (int r = 0; r < brt_engine::kRing; ++r)
@@ -952,7 +952,7 @@ int brt_engine_stage_timing(brt_engine* e, int enable) {
 }
 
 int brt_engine_stage_times(brt_engine* e, double* ms4, uint64_t* steps, uint32_t* launches_per_step) {
-  if (!e) return BRT_ERR_ARG;
+  if (!e) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   for (int r = 0; r < brt_engine::kRing; ++r) {
     int rc = drainSlot(e, (e->ringPos + r) % brt_engine::kRing);
@@ -970,7 +970,7 @@ int brt_engine_stage_times(brt_engine* e, double* ms4, uint64_t* steps, uint32_t
 }
 
 int brt_engine_autotune(brt_engine* e, float elapsedTime, uint32_t steps, char* report, size_t report_len) {
-  if (!e || steps == 0) return BRT_ERR_ARG;
+  if (!e || steps == 0) return brt::argError(__func__);
   if (e->N == 0) return BRT_OK;
   DeviceGuard guard(e->device);
   cudaStream_t st = e->stream;
@@ -1154,7 +1154,7 @@ int brt_engine_autotune(brt_engine* e, float elapsedTime, uint32_t steps, char* 
 // ---- stage-wise functionalities ------------------------------------------------
 
 int brt_reorder_sim_data(brt_engine* e) {
-  if (!e) return BRT_ERR_ARG;
+  if (!e) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   if (e->N == 0) return BRT_OK;
   int rc = enqueueReorder(e);
@@ -1165,7 +1165,7 @@ int brt_reorder_sim_data(brt_engine* e) {
 }
 
 int brt_compute_neighborhoods(brt_engine* e) {
-  if (!e) return BRT_ERR_ARG;
+  if (!e) return brt::argError(__func__);
   if (!e->reordered) { setLastError("computeNeighborhoods before reorderSimData"); return BRT_ERR_STATE; }
   DeviceGuard guard(e->device);
   BRT_CUDA_TRY(launchLists(stageArgs(e), e->anyKnn, e->stream));
@@ -1174,14 +1174,14 @@ int brt_compute_neighborhoods(brt_engine* e) {
 }
 
 int brt_reset_steer_force(brt_engine* e) {
-  if (!e) return BRT_ERR_ARG;
+  if (!e) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   if (e->N) BRT_CUDA_TRY(cudaMemsetAsync(e->steer, 0, (size_t)e->N * 16, e->stream));
   return BRT_OK;
 }
 
 static int steerStage(brt_engine* e, int which) {
-  if (!e) return BRT_ERR_ARG;
+  if (!e) return brt::argError(__func__);
   if (!e->reordered || !e->listsValid) { setLastError("steering stage before computeNeighborhoods"); return BRT_ERR_STATE; }
   DeviceGuard guard(e->device);
   BRT_CUDA_TRY(launchSteerStage(stageArgs(e), which, e->stream));
@@ -1198,7 +1198,7 @@ int brt_steer_for_clustering(brt_engine* e) { return steerStage(e, 3); }
 int brt_compute_seekings_world_center(brt_engine* e) { return steerStage(e, 4); }
 int brt_steer_and_slow_to_avoid_neighbors(brt_engine* e) { return steerStage(e, 5); }
 int brt_steer_for_move_away_base_target(brt_engine* e, const float* base3, const float* params3) {
-  if (!e || !base3) return BRT_ERR_ARG;
+  if (!e || !base3) return brt::argError(__func__);
   if (!e->reordered || !e->listsValid) { setLastError("steering stage before computeNeighborhoods"); return BRT_ERR_STATE; }
   DeviceGuard guard(e->device);
   StageArgs A = stageArgs(e);
@@ -1224,7 +1224,7 @@ struct SnapHeader {
 }  // namespace
 
 int brt_save_snapshot(brt_engine* e, const char* path) {
-  if (!e || !path) return BRT_ERR_ARG;
+  if (!e || !path) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   const size_t n = e->N, F = e->Fmax;
   std::vector<float> pos(4 * n), fwd(4 * n), acc(4 * n), stats(4 * n), feat(n * F);
@@ -1248,7 +1248,7 @@ int brt_save_snapshot(brt_engine* e, const char* path) {
 }
 
 int brt_load_snapshot(brt_engine* e, const char* path) {
-  if (!e || !path) return BRT_ERR_ARG;
+  if (!e || !path) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   FILE* f = std::fopen(path, "rb");
   if (!f) { setLastError(std::string("cannot open ") + path); return BRT_ERR_ARG; }
@@ -1300,7 +1300,7 @@ static int clusterReady(brt_engine* e) {
 }
 
 int brt_compute_cluster_membership(brt_engine* e, uint32_t iterations) {
-  if (!e) return BRT_ERR_ARG;
+  if (!e) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   int rc = clusterReady(e);
   if (rc || e->N == 0) return rc;
@@ -1312,7 +1312,7 @@ int brt_compute_cluster_membership(brt_engine* e, uint32_t iterations) {
 }
 
 int brt_analyze_cluster_hit_rate(brt_engine* e, float same_cluster_max_radius) {
-  if (!e) return BRT_ERR_ARG;
+  if (!e) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   int rc = clusterReady(e);
   if (rc || e->N == 0) return rc;
@@ -1322,7 +1322,7 @@ int brt_analyze_cluster_hit_rate(brt_engine* e, float same_cluster_max_radius) {
 }
 
 int brt_get_cluster_membership(brt_engine* e, float* membership4, int where) {
-  if (!e || !membership4) return BRT_ERR_ARG;
+  if (!e || !membership4) return brt::argError(__func__);
   if (!e->membership[0]) { setLastError("no cluster membership computed yet"); return BRT_ERR_STATE; }
   DeviceGuard guard(e->device);
   BRT_CUDA_TRY(cudaMemcpyAsync(membership4, e->membership[e->membershipCur], (size_t)e->N * 16,
@@ -1332,7 +1332,7 @@ int brt_get_cluster_membership(brt_engine* e, float* membership4, int where) {
 }
 
 static int schoolStage(brt_engine* e, int which) {
-  if (!e) return BRT_ERR_ARG;
+  if (!e) return brt::argError(__func__);
   if (!e->school) { setLastError("Schooling functionality on a flocking engine (schooling.mode 0)"); return BRT_ERR_STATE; }
   if (!e->reordered || !e->listsValid) { setLastError("Schooling functionality before computeNeighborhoods"); return BRT_ERR_STATE; }
   DeviceGuard guard(e->device);
@@ -1346,7 +1346,7 @@ int brt_school_movement(brt_engine* e) { return schoolStage(e, 2); }
 int brt_school_animate(brt_engine* e) { return schoolStage(e, 3); }
 
 int brt_apply_steering_forces(brt_engine* e, float elapsedTime) {
-  if (!e) return BRT_ERR_ARG;
+  if (!e) return brt::argError(__func__);
   if (!e->reordered || !e->listsValid) { setLastError("applySteeringForces before computeNeighborhoods"); return BRT_ERR_STATE; }
   DeviceGuard guard(e->device);
   BRT_CUDA_TRY(launchIntegrateStage(stageArgs(e), elapsedTime, e->stream));
@@ -1358,7 +1358,7 @@ int brt_apply_steering_forces(brt_engine* e, float elapsedTime) {
 static cudaMemcpyKind kindOut(int where) { return where == BRT_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice; }
 
 int brt_get_hash(brt_engine* e, uint32_t* keys, uint32_t* ids, int where) {
-  if (!e) return BRT_ERR_ARG;
+  if (!e) return brt::argError(__func__);
   if (!e->reordered) { setLastError("getHash before reorderSimData"); return BRT_ERR_STATE; }
   DeviceGuard guard(e->device);
   const size_t n = e->N;
@@ -1376,7 +1376,7 @@ int brt_get_hash(brt_engine* e, uint32_t* keys, uint32_t* ids, int where) {
 }
 
 int brt_get_cell_ranges(brt_engine* e, uint32_t* cell_start, uint32_t* cell_end, int where) {
-  if (!e) return BRT_ERR_ARG;
+  if (!e) return brt::argError(__func__);
   if (!e->reordered) { setLastError("getCellStart before reorderSimData"); return BRT_ERR_STATE; }
   DeviceGuard guard(e->device);
   if (cell_start) BRT_CUDA_TRY(cudaMemcpyAsync(cell_start, e->cellStart, (size_t)e->C * 4, kindOut(where), e->stream));
@@ -1386,7 +1386,7 @@ int brt_get_cell_ranges(brt_engine* e, uint32_t* cell_start, uint32_t* cell_end,
 }
 
 int brt_get_neighbor_lists(brt_engine* e, uint32_t* lists, int where) {
-  if (!e || !lists) return BRT_ERR_ARG;
+  if (!e || !lists) return brt::argError(__func__);
   if (!e->listsValid) { setLastError("neighbour lists not computed (computeNeighborhoods or record_lists)"); return BRT_ERR_STATE; }
   DeviceGuard guard(e->device);
   BRT_CUDA_TRY(cudaMemcpyAsync(lists, e->lists, (size_t)e->N * e->listStride * 4, kindOut(where), e->stream));
@@ -1395,7 +1395,7 @@ int brt_get_neighbor_lists(brt_engine* e, uint32_t* lists, int where) {
 }
 
 int brt_get_steer_force(brt_engine* e, float* steer4, int where) {
-  if (!e || !steer4) return BRT_ERR_ARG;
+  if (!e || !steer4) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   BRT_CUDA_TRY(cudaMemcpyAsync(steer4, e->steer, (size_t)e->N * 16, kindOut(where), e->stream));
   if (where == BRT_MEM_HOST) return syncAndCheck(e);
@@ -1405,7 +1405,7 @@ int brt_get_steer_force(brt_engine* e, float* steer4, int where) {
 // ---- plugin extension: registered arrays, the array view, user launches ----------
 
 int brt_engine_add_array(brt_engine* e, uint32_t bytes_per_agent, uint32_t* array_id) {
-  if (!e || !array_id) return BRT_ERR_ARG;
+  if (!e || !array_id) return brt::argError(__func__);
   if (bytes_per_agent == 0 || bytes_per_agent % 4 || bytes_per_agent > 1024) {
     setLastError("bytes_per_agent must be a multiple of 4 in [4, 1024]");
     return BRT_ERR_ARG;
@@ -1446,8 +1446,8 @@ int brt_engine_add_array(brt_engine* e, uint32_t bytes_per_agent, uint32_t* arra
 }
 
 int brt_engine_array_set(brt_engine* e, uint32_t array_id, const void* src, int where) {
-  if (!e || !src || array_id >= e->user.size()) return BRT_ERR_ARG;
-  if (where != BRT_MEM_HOST && where != BRT_MEM_DEVICE) return BRT_ERR_ARG;
+  if (!e || !src || array_id >= e->user.size()) return brt::argError(__func__);
+  if (where != BRT_MEM_HOST && where != BRT_MEM_DEVICE) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   const brt_engine::UserArray& u = e->user[array_id];
   const size_t bytes = (size_t)e->N * u.words * 4;
@@ -1464,8 +1464,8 @@ int brt_engine_array_set(brt_engine* e, uint32_t array_id, const void* src, int 
 }
 
 int brt_engine_array_get(brt_engine* e, uint32_t array_id, void* dst, int where) {
-  if (!e || !dst || array_id >= e->user.size()) return BRT_ERR_ARG;
-  if (where != BRT_MEM_HOST && where != BRT_MEM_DEVICE) return BRT_ERR_ARG;
+  if (!e || !dst || array_id >= e->user.size()) return brt::argError(__func__);
+  if (where != BRT_MEM_HOST && where != BRT_MEM_DEVICE) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   const brt_engine::UserArray& u = e->user[array_id];
   const size_t bytes = (size_t)e->N * u.words * 4;
@@ -1480,7 +1480,7 @@ int brt_engine_array_get(brt_engine* e, uint32_t array_id, void* dst, int where)
 }
 
 int brt_engine_get_arrays(brt_engine* e, brt_arrays* out) {
-  if (!e || !out) return BRT_ERR_ARG;
+  if (!e || !out) return brt::argError(__func__);
   std::memset(out, 0, sizeof(*out));
   out->num_agents = e->N;
   out->num_cells = e->C;
@@ -1505,7 +1505,7 @@ int brt_engine_get_arrays(brt_engine* e, brt_arrays* out) {
 }
 
 int brt_engine_launch(brt_engine* e, brt_launch_fn fn, void* user_data) {
-  if (!e || !fn) return BRT_ERR_ARG;
+  if (!e || !fn) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   brt_arrays view;
   int rc = brt_engine_get_arrays(e, &view);

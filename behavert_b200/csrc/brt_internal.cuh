@@ -194,6 +194,12 @@ cudaError_t launchSortHistogram(const SortPlan& p, const uint2* in, const SortSc
 
 // Thread-local error message.
 void setLastError(const std::string& msg);
+// A bad argument to entry point `fn`: records "fn: bad arguments" for
+// brt_last_error and returns BRT_ERR_ARG.
+inline int argError(const char* fn) {
+  setLastError(std::string(fn) + ": bad arguments");
+  return BRT_ERR_ARG;
+}
 
 }  // namespace brt
 

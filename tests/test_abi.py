@@ -80,6 +80,18 @@ def test_bad_configuration_is_rejected_before_any_gpu_work():
         brt.Engine(p)
 
 
+def test_bad_arguments_name_the_entry_point():
+    """A null engine or a bad memory kind is refused before any GPU work, and
+    brt_last_error names the entry point that refused it."""
+    L = _abi.lib()
+    cases = [("brt_step", lambda: L.brt_step(None, 0.1, 1)),
+             ("brt_set_state", lambda: L.brt_set_state(None, None, None, None, None, _abi.BRT_MEM_HOST)),
+             ("brt_engine_add_array", lambda: L.brt_engine_add_array(None, 4, None))]
+    for name, call in cases:
+        assert call() == _abi.BRT_ERR_ARG
+        assert L.brt_last_error().decode() == name + ": bad arguments"
+
+
 def test_facade_header_compiles():
     src = ROOT / "include" / "behavert" / "BehaveRT.h"
     if not src.exists():
