@@ -390,6 +390,7 @@ extern "C" {
 
 int brt_adjoint_forward(brt_engine* e, float elapsedTime, uint32_t nsteps, uint32_t checkpoint_every,
                         const float* target_pos4, int where, double* loss_per_flock) {
+  brt::TraceRange trace(__func__);
   if (!e || !target_pos4 || nsteps == 0 || checkpoint_every == 0) { setLastError("brt_adjoint_forward: bad arguments"); return BRT_ERR_ARG; }
   if (where != BRT_MEM_HOST && where != BRT_MEM_DEVICE) return brt::argError(__func__);
   if (e->N == 0) return BRT_OK;
@@ -420,6 +421,7 @@ int brt_adjoint_forward(brt_engine* e, float elapsedTime, uint32_t nsteps, uint3
 int brt_adjoint_backward(brt_engine* e, const double* loss_scale, const float* gpos4_T, const float* gfwd4_T,
                          const float* gacc4_T, int where_in, float* grad_pos4, float* grad_fwd4, float* grad_vel4,
                          float* grad_acc4, double* grad_weights, int where_out) {
+  brt::TraceRange trace(__func__);
   if (!e) return brt::argError(__func__);
   if ((where_in != BRT_MEM_HOST && where_in != BRT_MEM_DEVICE) || (where_out != BRT_MEM_HOST && where_out != BRT_MEM_DEVICE))
     return brt::argError(__func__);

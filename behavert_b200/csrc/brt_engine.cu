@@ -513,6 +513,7 @@ int brt_params_default(brt_params* p) {
 }
 
 int brt_engine_create(const brt_params* flocks, uint32_t num_flocks, int device, brt_engine** out) {
+  brt::TraceRange trace(__func__);
   if (!flocks || !out || num_flocks == 0) { setLastError("brt_engine_create: bad arguments"); return BRT_ERR_ARG; }
   *out = nullptr;
   int ndev = 0;
@@ -647,6 +648,7 @@ int brt_engine_create(const brt_params* flocks, uint32_t num_flocks, int device,
 }
 
 int brt_engine_destroy(brt_engine* e) {
+  brt::TraceRange trace(__func__);
   if (!e) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   cudaStreamSynchronize(e->stream);
@@ -817,6 +819,7 @@ int brt_engine_check_device_error(brt_engine* e, uint32_t* word) {
 // ---- feature I/O ------------------------------------------------------------
 
 int brt_set_state(brt_engine* e, const float* pos4, const float* fwd4, const float* acc4, const float* features, int where) {
+  brt::TraceRange trace(__func__);
   if (!e) return brt::argError(__func__);
   if (where != BRT_MEM_HOST && where != BRT_MEM_DEVICE) return brt::argError(__func__);
   DeviceGuard guard(e->device);
@@ -858,6 +861,7 @@ int brt_set_state(brt_engine* e, const float* pos4, const float* fwd4, const flo
 }
 
 int brt_get_state(brt_engine* e, float* pos4, float* fwd4, float* acc4, float* features, int where) {
+  brt::TraceRange trace(__func__);
   if (!e) return brt::argError(__func__);
   if (where != BRT_MEM_HOST && where != BRT_MEM_DEVICE) return brt::argError(__func__);
   DeviceGuard guard(e->device);
@@ -908,6 +912,7 @@ int brt_get_similarity_stats(brt_engine* e, float* stats4, int where) {
 // ---- fused step --------------------------------------------------------------
 
 int brt_step(brt_engine* e, float elapsedTime, uint32_t nsteps) {
+  brt::TraceRange trace(__func__);
   if (!e) return brt::argError(__func__);
   if (nsteps == 0 || e->N == 0) return BRT_OK;
   DeviceGuard guard(e->device);
@@ -927,6 +932,7 @@ int brt_step(brt_engine* e, float elapsedTime, uint32_t nsteps) {
 }
 
 int brt_step_prepare(brt_engine* e, float elapsedTime, uint32_t nsteps) {
+  brt::TraceRange trace(__func__);
   if (!e) return brt::argError(__func__);
   if (nsteps < 2 || e->N == 0) return BRT_OK;
   DeviceGuard guard(e->device);
@@ -970,6 +976,7 @@ int brt_engine_stage_times(brt_engine* e, double* ms4, uint64_t* steps, uint32_t
 }
 
 int brt_engine_autotune(brt_engine* e, float elapsedTime, uint32_t steps, char* report, size_t report_len) {
+  brt::TraceRange trace(__func__);
   if (!e || steps == 0) return brt::argError(__func__);
   if (e->N == 0) return BRT_OK;
   DeviceGuard guard(e->device);
@@ -1154,6 +1161,7 @@ int brt_engine_autotune(brt_engine* e, float elapsedTime, uint32_t steps, char* 
 // ---- stage-wise functionalities ------------------------------------------------
 
 int brt_reorder_sim_data(brt_engine* e) {
+  brt::TraceRange trace(__func__);
   if (!e) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   if (e->N == 0) return BRT_OK;
@@ -1165,6 +1173,7 @@ int brt_reorder_sim_data(brt_engine* e) {
 }
 
 int brt_compute_neighborhoods(brt_engine* e) {
+  brt::TraceRange trace(__func__);
   if (!e) return brt::argError(__func__);
   if (!e->reordered) { setLastError("computeNeighborhoods before reorderSimData"); return BRT_ERR_STATE; }
   DeviceGuard guard(e->device);
@@ -1174,6 +1183,7 @@ int brt_compute_neighborhoods(brt_engine* e) {
 }
 
 int brt_reset_steer_force(brt_engine* e) {
+  brt::TraceRange trace(__func__);
   if (!e) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   if (e->N) BRT_CUDA_TRY(cudaMemsetAsync(e->steer, 0, (size_t)e->N * 16, e->stream));
@@ -1188,16 +1198,35 @@ static int steerStage(brt_engine* e, int which) {
   return BRT_OK;
 }
 
-int brt_compute_separations(brt_engine* e) { return steerStage(e, 0); }
-int brt_compute_alignments(brt_engine* e) { return steerStage(e, 1); }
-int brt_compute_cohesions(brt_engine* e) { return steerStage(e, 2); }
-int brt_steer_for_clustering(brt_engine* e) { return steerStage(e, 3); }
+int brt_compute_separations(brt_engine* e) {
+  brt::TraceRange trace(__func__);
+  return steerStage(e, 0);
+}
+int brt_compute_alignments(brt_engine* e) {
+  brt::TraceRange trace(__func__);
+  return steerStage(e, 1);
+}
+int brt_compute_cohesions(brt_engine* e) {
+  brt::TraceRange trace(__func__);
+  return steerStage(e, 2);
+}
+int brt_steer_for_clustering(brt_engine* e) {
+  brt::TraceRange trace(__func__);
+  return steerStage(e, 3);
+}
 // In the periodic world every position is inside the world box, so the
 // reference's seek-to-centre force is zero (OpenSteerWrapper_kernel.cu:236-246);
 // this stage applies the static obstacle field of the EnvGrid3D grid instead.
-int brt_compute_seekings_world_center(brt_engine* e) { return steerStage(e, 4); }
-int brt_steer_and_slow_to_avoid_neighbors(brt_engine* e) { return steerStage(e, 5); }
+int brt_compute_seekings_world_center(brt_engine* e) {
+  brt::TraceRange trace(__func__);
+  return steerStage(e, 4);
+}
+int brt_steer_and_slow_to_avoid_neighbors(brt_engine* e) {
+  brt::TraceRange trace(__func__);
+  return steerStage(e, 5);
+}
 int brt_steer_for_move_away_base_target(brt_engine* e, const float* base3, const float* params3) {
+  brt::TraceRange trace(__func__);
   if (!e || !base3) return brt::argError(__func__);
   if (!e->reordered || !e->listsValid) { setLastError("steering stage before computeNeighborhoods"); return BRT_ERR_STATE; }
   DeviceGuard guard(e->device);
@@ -1224,6 +1253,7 @@ struct SnapHeader {
 }  // namespace
 
 int brt_save_snapshot(brt_engine* e, const char* path) {
+  brt::TraceRange trace(__func__);
   if (!e || !path) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   const size_t n = e->N, F = e->Fmax;
@@ -1248,6 +1278,7 @@ int brt_save_snapshot(brt_engine* e, const char* path) {
 }
 
 int brt_load_snapshot(brt_engine* e, const char* path) {
+  brt::TraceRange trace(__func__);
   if (!e || !path) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   FILE* f = std::fopen(path, "rb");
@@ -1300,6 +1331,7 @@ static int clusterReady(brt_engine* e) {
 }
 
 int brt_compute_cluster_membership(brt_engine* e, uint32_t iterations) {
+  brt::TraceRange trace(__func__);
   if (!e) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   int rc = clusterReady(e);
@@ -1312,6 +1344,7 @@ int brt_compute_cluster_membership(brt_engine* e, uint32_t iterations) {
 }
 
 int brt_analyze_cluster_hit_rate(brt_engine* e, float same_cluster_max_radius) {
+  brt::TraceRange trace(__func__);
   if (!e) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   int rc = clusterReady(e);
@@ -1340,12 +1373,25 @@ static int schoolStage(brt_engine* e, int which) {
   return BRT_OK;
 }
 
-int brt_school_repulsion(brt_engine* e) { return schoolStage(e, 0); }
-int brt_school_attraction_orientation(brt_engine* e) { return schoolStage(e, 1); }
-int brt_school_movement(brt_engine* e) { return schoolStage(e, 2); }
-int brt_school_animate(brt_engine* e) { return schoolStage(e, 3); }
+int brt_school_repulsion(brt_engine* e) {
+  brt::TraceRange trace(__func__);
+  return schoolStage(e, 0);
+}
+int brt_school_attraction_orientation(brt_engine* e) {
+  brt::TraceRange trace(__func__);
+  return schoolStage(e, 1);
+}
+int brt_school_movement(brt_engine* e) {
+  brt::TraceRange trace(__func__);
+  return schoolStage(e, 2);
+}
+int brt_school_animate(brt_engine* e) {
+  brt::TraceRange trace(__func__);
+  return schoolStage(e, 3);
+}
 
 int brt_apply_steering_forces(brt_engine* e, float elapsedTime) {
+  brt::TraceRange trace(__func__);
   if (!e) return brt::argError(__func__);
   if (!e->reordered || !e->listsValid) { setLastError("applySteeringForces before computeNeighborhoods"); return BRT_ERR_STATE; }
   DeviceGuard guard(e->device);
@@ -1505,6 +1551,7 @@ int brt_engine_get_arrays(brt_engine* e, brt_arrays* out) {
 }
 
 int brt_engine_launch(brt_engine* e, brt_launch_fn fn, void* user_data) {
+  brt::TraceRange trace(__func__);
   if (!e || !fn) return brt::argError(__func__);
   DeviceGuard guard(e->device);
   brt_arrays view;

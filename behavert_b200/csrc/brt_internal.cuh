@@ -15,6 +15,8 @@
 
 #include "../../include/behavert_b200.h"
 
+#include <nvtx3/nvToolsExt.h>
+
 namespace brt {
 
 constexpr uint32_t kEmpty = 0xFFFFFFFFu;
@@ -194,6 +196,17 @@ cudaError_t launchSortHistogram(const SortPlan& p, const uint2* in, const SortSc
 
 // Thread-local error message.
 void setLastError(const std::string& msg);
+// A named range on a profiler's timeline (NVTX) for the duration of an entry
+// point, as the reference timed its kernel calls (Core/DeviceInterface.cu:
+// 389-456): the host-side span of the call, nested ranges included.  With no
+// tool attached the push and pop cost a few nanoseconds.
+struct TraceRange {
+  explicit TraceRange(const char* name) { nvtxRangePushA(name); }
+  ~TraceRange() { nvtxRangePop(); }
+  TraceRange(const TraceRange&) = delete;
+  TraceRange& operator=(const TraceRange&) = delete;
+};
+
 // A bad argument to entry point `fn`: records "fn: bad arguments" for
 // brt_last_error and returns BRT_ERR_ARG.
 inline int argError(const char* fn) {

@@ -326,6 +326,7 @@ extern "C" size_t brt_radix_sort_scratch_bytes(uint32_t n, uint32_t bits) {
 
 extern "C" int brt_radix_sort_pairs(const uint32_t* pairs_in, uint32_t* pairs_out, uint32_t n, uint32_t bits,
                                     void* scratch, size_t scratch_bytes, void* stream) {
+  brt::TraceRange trace(__func__);
   if (n == 0) return BRT_OK;
   if (!pairs_in || !pairs_out || !scratch) { brt::setLastError("brt_radix_sort_pairs: null pointer"); return BRT_ERR_ARG; }
   if ((const void*)pairs_in == (const void*)pairs_out) { brt::setLastError("brt_radix_sort_pairs: in and out must differ"); return BRT_ERR_ARG; }
@@ -404,6 +405,7 @@ extern "C" size_t brt_radix_sort_noalloc_max_pairs(void) { return kNoAllocMaxPai
 
 extern "C" int brt_radix_sort_pairs_noalloc(const uint32_t* pairs_in, uint32_t* pairs_out, uint32_t n, uint32_t bits,
                                             void* stream) {
+  brt::TraceRange trace(__func__);
   if (n == 0) return BRT_OK;
   if (!pairs_in || !pairs_out) { brt::setLastError("brt_radix_sort_pairs_noalloc: null pointer"); return BRT_ERR_ARG; }
   if ((const void*)pairs_in == (const void*)pairs_out) {
