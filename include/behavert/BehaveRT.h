@@ -19,12 +19,14 @@
 #pragma once
 
 #include <algorithm>
+#include <cstdarg>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <fstream>
 #include <functional>
 #include <map>
+#include <list>
 #include <memory>
 #include <random>
 #include <sstream>
@@ -143,6 +145,61 @@ class DeviceInterface {
 };
 
 // ---------------------------------------------------------------------------
+// UtilityLogger (Core/include/UtilityLogger.h:50-133): the last maxSize
+// messages of (sender, text, level), each also written to standard output as
+// "sender>> text"; a sender filter and a level (debug or info) select what a
+// display shows.  quickLog formats printf-style.
+class UtilityLogger {
+ public:
+  enum mLogLevels { LOG_DEBUG, LOG_INFO };
+  typedef std::string msgSenderType;
+  typedef std::string msgTextType;
+  typedef std::pair<msgSenderType, msgTextType> logMsg;
+  typedef std::pair<logMsg, mLogLevels> logItem;
+  typedef std::list<logItem> msgListType;
+
+  explicit UtilityLogger(unsigned int maxSize) : mMaxSize(maxSize) {}
+  void log(msgSenderType msgSender, msgTextType msgText, mLogLevels level = LOG_INFO) {
+    std::printf("%s>> %s\n", msgSender.c_str(), msgText.c_str());
+    mMsgList.push_back(logItem(logMsg(msgSender, msgText), level));
+    while (mMsgList.size() > mMaxSize) mMsgList.pop_front();
+    mModified = true;
+  }
+  void quickLog(msgSenderType msgSender, const char* fmt, ...) {
+    char msg[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(msg, sizeof(msg), fmt, ap);
+    va_end(ap);
+    log(msgSender, msg);
+  }
+  bool checkSender(const logItem& item) const { return item.first.first == mSenderFilter; }
+  bool checkLevel(const logItem& item) const { return item.second == mLevel || item.second == LOG_INFO; }
+  std::string getMsgString(const logItem& item) const { return item.first.second; }
+  void setLevelString(const std::string& level) { mLevel = level == "debug" ? LOG_DEBUG : LOG_INFO; }
+  // the messages the level admits, oldest first, joined by `separator`
+  std::string getMsgListString(const std::string& separator) const {
+    std::string out;
+    for (const logItem& item : mMsgList)
+      if (checkLevel(item)) out += getMsgString(item) + separator;
+    return out;
+  }
+  msgListType getMsgList() const { return mMsgList; }
+  bool isModified() const { return mModified; }
+  void setModified(bool modified) { mModified = modified; }
+  void setSenderFilter(const std::string& senderFilter) { mSenderFilter = senderFilter; }
+  std::string getSenderFilter() const { return mSenderFilter; }
+
+  msgListType mMsgList;
+
+ protected:
+  unsigned int mMaxSize;
+  mLogLevels mLevel = LOG_INFO;
+  bool mModified = false;
+  std::string mSenderFilter;
+};
+
+// ---------------------------------------------------------------------------
 // CommonResources: configuration, device interface and the parameters the
 // installed plugins fill in (the reference's hXParams globals).
 class CommonResources {
@@ -155,6 +212,8 @@ class CommonResources {
   bool isInitialized() const { return m_Initialized; }
   DeviceInterface* getDeviceInterface() { return &m_DeviceInterface; }
   UtilityConfigFile* getConfig() { return &m_Config; }
+  // the reference keeps the last 50 messages (Core/src/CommonResources.cpp:58)
+  UtilityLogger* getLogger() { return &m_Logger; }
   brt_params& params() { return m_Params; }
   // The engine is created the first time a functionality needs it, once
   // every plugin has installed its parameters.
@@ -169,6 +228,7 @@ class CommonResources {
  private:
   bool m_Initialized = false;
   UtilityConfigFile m_Config;
+  UtilityLogger m_Logger{50};
   DeviceInterface m_DeviceInterface;
   brt_params m_Params;
   std::vector<std::string> m_Installed;

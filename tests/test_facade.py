@@ -88,3 +88,13 @@ def test_cluster_inverse_hash_and_merge(tmp_path):
     print(res.stdout, res.stderr)
     assert res.returncode == 0, res.stdout + res.stderr
     assert "inverse hash: yes" in res.stdout and ": yes" in res.stdout.split("merged")[1]
+
+
+def test_logger(tmp_path):
+    """UtilityLogger through m_CommonRes.getLogger(): bounded list, printf-style
+    quickLog, level and sender filters (host only)."""
+    exe = tmp_path / "logger_facade"
+    _build("logger_facade", exe)
+    res = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert res.returncode == 0, res.stdout + res.stderr
+    assert "Flocking>> frame 59 of demo" in res.stdout and "logger: yes" in res.stdout
