@@ -218,12 +218,23 @@ class CommonResources {
   // The engine is created the first time a functionality needs it, once
   // every plugin has installed its parameters.
   brt_engine* engine() {
-    if (!m_DeviceInterface.hasEngine()) m_DeviceInterface.createEngine(m_Params);
+    if (!m_DeviceInterface.hasEngine()) {
+      m_DeviceInterface.createEngine(m_Params);
+      // a configured block size that the flock kernel accepts (a multiple of
+      // 32 up to 256); others leave the engine's default, with a message
+      if (blockSize > 0) {
+        if (blockSize % 32 == 0 && blockSize <= 256)
+          check(brt_engine_set_option(m_DeviceInterface.engine(), "block_size", blockSize), "block_size");
+        else
+          m_Logger.quickLog("CommonResources", "block size %d not used: a multiple of 32 up to 256 is", blockSize);
+      }
+    }
     return m_DeviceInterface.engine();
   }
   void installPlugIn(const std::string& name) { m_Installed.push_back(name); }
   const std::vector<std::string>& installedPlugIns() const { return m_Installed; }
   uint32_t seed = 1;
+  int blockSize = 0;  // from customBlockSize / BlockDim; 0: the engine's default
 
  private:
   bool m_Initialized = false;
@@ -425,6 +436,27 @@ class EnvGrid3DPlugIn : public Super {
     const std::string cs = m_CommonRes.getConfig()->getSetting("cellSize", s);
     if (!cs.empty()) { parseFloat3(cs, cell); p.cellSize = cell[0]; }
     BRT_READ_PARAM(s, "worldSize", p.worldSize, parseFloat);
+    // setupWorldRadius (EnvGrid3DPlugIn.h:421-470).  The reference's box spans
+    // center -/+ worldRadius; with keepDensity its radius is
+    // (numBodies / density)^(1/3) / 2 (the square root in 2D, bodiesDensity2D).
+    // Here the periodic cube's side is twice that radius, rounded up to whole
+    // cells (the periodic grid needs an integer number of cells, at least 3).
+    // An explicit worldSize wins.  worldCenter and lockWorldProportions have
+    // no meaning for the periodic cube and are not read.
+    UtilityConfigFile* c = m_CommonRes.getConfig();
+    if (!c->has("worldSize", s)) {
+      float side = 0.0f;
+      if (parseBool(c->getSetting("keepDensity", s))) {
+        const char* key = p.use2DProjection ? "bodiesDensity2D" : "bodiesDensity3D";
+        const float d = c->has(key, s) ? parseFloat(c->getSetting(key, s)) : 0.0f;
+        if (d > 0.0f) side = std::pow((float)p.numBodies / d, p.use2DProjection ? 0.5f : 0.33333f);
+      } else if (c->has("worldRadius", s)) {
+        float r[3] = {0.0f, 0.0f, 0.0f};
+        parseFloat3(c->getSetting("worldRadius", s), r);
+        side = 2.0f * std::max(r[0], std::max(r[1], r[2]));
+      }
+      if (side > 0.0f) p.worldSize = std::max(3.0f, std::ceil(side / p.cellSize)) * p.cellSize;
+    }
     // setupMaxBodiesPerCell (EnvGrid3DPlugIn.h:537-562): the configured cap,
     // or with useAutomaticMaxBodiesPerCell the upper bound
     // 1 + cellVolume / bodyVolume, bodyVolume = 4.1866 r^3 of the body radius
@@ -490,6 +522,23 @@ class Proximity3DPlugIn : public Super {
     BRT_READ_PARAM(s, "maxNeighbors", p.maxNeighbors, parseInt);
     BRT_READ_PARAM(s, "commonSearchRadius", p.commonSearchRadius, parseFloat);
     if (parseBool(m_CommonRes.getConfig()->getSetting("useCellSizeAsSearchRadius", s))) p.commonSearchRadius = p.cellSize;
+    // searchDepth (Proximity3DPlugIn.h:120-125): the cells scanned on each
+    // side of the home cell.  The engine scans the 27 cells of depth 1 1 1
+    // (cellSize >= radius); other depths are refused.
+    UtilityConfigFile* c = m_CommonRes.getConfig();
+    if (c->has("searchDepth", s)) {
+      std::istringstream in(c->getSetting("searchDepth", s));
+      int d[3] = {1, 1, 1};
+      in >> d[0] >> d[1] >> d[2];
+      if (d[0] != 1 || d[1] != 1 || d[2] != 1)
+        throw std::runtime_error("Proximity3DPlugIn: searchDepth must be 1 1 1 (the 27-cell neighbourhood)");
+    }
+    // customBlockSize (Proximity3DPlugIn.h:131-134), or DeviceInterface's
+    // BlockDim: the flock kernel's threads per block.  useSplittedNeigCalc and
+    // useForwardVBO choose reference code paths (a split list kernel, GL
+    // buffers) that have no counterpart; they are not read.
+    if (c->has("customBlockSize", s)) m_CommonRes.blockSize = parseInt(c->getSetting("customBlockSize", s));
+    else if (c->has("BlockDim", "DeviceInterface")) m_CommonRes.blockSize = parseInt(c->getSetting("BlockDim", "DeviceInterface"));
     SimEnginePlugIn::installPlugIn();
   }
   const std::string name() override { return "Proximity3DPlugIn"; }

@@ -12,7 +12,8 @@ int main(int argc, char** argv) {
   m_CommonRes.initialize(argc > 1 ? argv[1] : "");
   CrowdEngine engine;
   const brt_params& p = m_CommonRes.params();
-  std::printf("numBodies %u worldSize %g cellSize %g maxBodiesPerCell %u maxNeighbors %u radius %g\n", p.numBodies,
-              p.worldSize, p.cellSize, p.maxBodiesPerCell, p.maxNeighbors, p.commonSearchRadius);
+  std::printf("numBodies %u worldSize %g cellSize %g maxBodiesPerCell %u maxNeighbors %u radius %g blockSize %d\n",
+              p.numBodies, p.worldSize, p.cellSize, p.maxBodiesPerCell, p.maxNeighbors, p.commonSearchRadius,
+              m_CommonRes.blockSize);
   return 0;
 }

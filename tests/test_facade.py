@@ -8,7 +8,7 @@ import pytest
 
 ROOT = Path(__file__).resolve().parent.parent
 LIB_DIR = ROOT / "behavert_b200"
-APPS = [("flocking_facade", "flocking.cfg"), ("schooling_facade", "schooling.cfg")]
+APPS = [("flocking_facade", "flocking.cfg"), ("flocking_facade", "world_radius.cfg"), ("schooling_facade", "schooling.cfg")]
 
 
 CUDA = Path("/usr/local/cuda")
@@ -58,12 +58,15 @@ def test_plugin_arrays_and_kernel_call(tmp_path):
     assert "snapshot follows its agents: yes" in res.stdout
 
 
-@pytest.mark.parametrize("cfg,cap", [("automatic_cap.cfg", 16), ("flocking.cfg", 0)])
-def test_configuration_mapping(tmp_path, cfg, cap):
+@pytest.mark.parametrize("cfg,cap,world,block", [("automatic_cap.cfg", 16, 64, 0), ("flocking.cfg", 0, 64, 0),
+                                                  ("world_radius.cfg", 0, 64, 128), ("keep_density.cfg", 0, 44, 256)])
+def test_configuration_mapping(tmp_path, cfg, cap, world, block):
     """The reference's key names reach the engine parameters; with
     useAutomaticMaxBodiesPerCell the per-cell cap is the reference's upper
-    bound 1 + cellVolume / bodyVolume (EnvGrid3DPlugIn.h:537-562).  CPU only:
-    the engine is created lazily and no functionality is called."""
+    bound 1 + cellVolume / bodyVolume (EnvGrid3DPlugIn.h:537-562); worldRadius
+    and keepDensity size the cube (EnvGrid3DPlugIn.h:421-470) in whole cells;
+    customBlockSize / BlockDim set the block size.  CPU only: the engine is
+    created lazily and no functionality is called."""
     exe = tmp_path / "config_facade"
     _build("config_facade", exe)
     res = subprocess.run([str(exe), str(ROOT / "tests" / "cpp" / cfg)], capture_output=True, text=True)
@@ -72,6 +75,15 @@ def test_configuration_mapping(tmp_path, cfg, cap):
     got = dict(zip(fields[0::2], fields[1::2]))
     assert int(got["maxBodiesPerCell"]) == cap
     assert int(got["numBodies"]) == (1 << 10 if cfg == "automatic_cap.cfg" else 1 << 12)
+    assert float(got["worldSize"]) == world and int(got["blockSize"]) == block
+
+
+def test_search_depth_other_than_one_is_refused(tmp_path):
+    exe = tmp_path / "config_facade"
+    _build("config_facade", exe)
+    res = subprocess.run([str(exe), str(ROOT / "tests" / "cpp" / "search_depth.cfg")], capture_output=True, text=True)
+    assert res.returncode != 0
+    assert "searchDepth must be 1 1 1" in res.stderr
 
 
 def test_cluster_application_builds(tmp_path):
