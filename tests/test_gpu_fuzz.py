@@ -6,12 +6,15 @@ bit-exact).  The draws mix what the hand-written cases cover one at a time:
 maxNeighbors from 1 to 40, kNN and first-M flocks side by side, a per-cell
 cap, the 2D projection, features with and without relaxation, sphere
 obstacles, a sensing minimum radius and angle cuts, dense clumps, coincident
-agents and speeds down into the low-speed branch."""
+agents and speeds down into the low-speed branch.  The same for the
+Schooling law (random zones, limits, weights, speed and random deviation)
+and for the crowd order run stage by stage."""
 import numpy as np
 import pytest
 
 from behavert_b200.workloads import Workload, _agents, _below, _flock_params
-from tests.test_gpu_parity import check_step, make_engine
+from oracle import oracle
+from tests.test_gpu_parity import _same_bits, check_step, make_engine
 
 pytestmark = pytest.mark.gpu
 
@@ -73,3 +76,83 @@ def test_random_configuration_two_steps(seed):
     with make_engine(w) as eng:
         for _ in range(2):
             check_step(eng, w.params, dt=DT, fp64=False)
+
+
+def _random_school(seed: int) -> Workload:
+    """1 to 3 schools of one mode (an engine's flocks share the steering
+    family), random zone radii, turning and blind-angle limits, weights,
+    speed and random deviation."""
+    rng = np.random.default_rng(7000 + seed)
+    mode = int(rng.choice([1, 2]))
+    params, pos, fwd = [], [], []
+    for _ in range(int(rng.choice([1, 1, 2, 3]))):
+        L = 4.0 * int(rng.integers(3, 10))
+        n = int(rng.integers(2, 2500))
+        p = _flock_params(n, L, int(rng.choice([4, 16, 32])))
+        sp = p.schooling
+        sp.mode = mode
+        sp.r_r = float(rng.uniform(0.3, 2.0))
+        sp.r_p = float(rng.uniform(sp.r_r, 4.0))
+        sp.theta = float(rng.uniform(-0.5, 0.99))
+        sp.eta = float(rng.uniform(-1.0, 0.5))
+        sp.w_a = float(rng.uniform(0.2, 2.0))
+        sp.w_o = float(rng.uniform(1.0, 20.0))
+        sp.s = float(rng.uniform(0.5, 4.0))
+        sp.randomDeviationWeight = float(rng.choice([0.0, float(rng.uniform(0.0, 0.3))]))
+        sp.seed = int(rng.integers(1 << 31))
+        P, W = _agents(rng, n, L)
+        W[:, 3] = sp.s
+        if n > 10 and rng.random() < 0.4:
+            m = n // 3
+            P[:m, :3] = _below(rng.uniform(0, L, 3) + rng.normal(0.0, 1.0, (m, 3)), L)
+        params.append(p)
+        pos.append(P)
+        fwd.append(W)
+    P = np.concatenate(pos)
+    return Workload("fuzz_school", params, P, np.concatenate(fwd), np.zeros_like(P), None, 2, DT, {"seed": seed})
+
+
+@pytest.mark.parametrize("seed", range(30))
+def test_random_school_two_steps(seed):
+    w = _random_school(seed)
+    with make_engine(w) as eng:
+        p, f, a = w.pos, w.fwd, w.acc
+        for step in range(2):
+            eng.record_lists(True)
+            eng.step(DT, 1)
+            lists = eng.getNeighborLists()
+            pos, fwd, acc, _ = eng.get_state(features=False)
+            r = oracle.step(w.params, p, f, a, dt=DT, mode=0, random_step=step + 1)
+            cnt = lists[:, 0]
+            assert np.array_equal(cnt, r["lists"][:, 0])
+            mask = np.arange(lists.shape[1] - 1)[None, :] < cnt[:, None]
+            assert np.array_equal(np.where(mask, lists[:, 1:], 0), np.where(mask, r["lists"][:, 1:], 0))
+            assert _same_bits(pos, r["pos"]) and _same_bits(fwd, r["fwd"]) and _same_bits(acc, r["acc"])
+            p, f, a = pos, fwd, acc
+
+
+@pytest.mark.parametrize("seed", range(20))
+def test_random_crowd_order_one_step(seed):
+    """The crowd order, stage by stage (steerAndSlowToAvoidNeighbors, and in
+    half the draws the move-away-from-base stage), on random flocks."""
+    w = _random_workload(100 + seed)
+    for p in w.params:
+        p.useKnn = 0
+        p.featuresCount = 0
+    w = Workload(w.name, w.params, w.pos, w.fwd, w.acc, None, 1, DT, w.meta)
+    rng = np.random.default_rng(9000 + seed)
+    move = None
+    if rng.random() < 0.5:
+        move = (tuple(float(x) for x in rng.uniform(0, 16, 3)),
+                (float(rng.uniform(0.5, 3.0)), float(rng.uniform(1.0, 600.0)), float(rng.uniform(2.0, 10.0))))
+    with make_engine(w) as eng:
+        pos, fwd, acc, _ = eng.get_state()
+        if move:
+            eng.update_crowd(DT, avoid_base=move[0], avoid_base_params=move[1])
+        else:
+            eng.update_crowd(DT)
+        lists = eng.getNeighborLists()
+        gpos, gfwd, gacc, _ = eng.get_state()
+    o = oracle.step(w.params, pos, fwd, acc, dt=DT, mode=0, avoid_neighbors=True, move_away=move)
+    assert np.array_equal(lists[:, 0], o["lists"][:, 0])
+    assert _same_bits(gpos, o["pos"]) and _same_bits(gfwd, o["fwd"]) and _same_bits(gacc, o["acc"])
