@@ -156,3 +156,73 @@ def test_random_crowd_order_one_step(seed):
     o = oracle.step(w.params, pos, fwd, acc, dt=DT, mode=0, avoid_neighbors=True, move_away=move)
     assert np.array_equal(lists[:, 0], o["lists"][:, 0])
     assert _same_bits(gpos, o["pos"]) and _same_bits(gfwd, o["fwd"]) and _same_bits(gacc, o["acc"])
+
+
+def _random_adjoint(seed: int):
+    """1 to 3 flocks of 200 to 3,000 agents, random weights, sometimes
+    obstacles, a sensing minimum radius and angle cuts, low speeds (the
+    deviation-limited branch), horizons of 4 to 12 steps with a random
+    checkpoint interval, and targets near the start."""
+    rng = np.random.default_rng(11000 + seed)
+    params, pos, fwd = [], [], []
+    for _ in range(int(rng.choice([1, 1, 2, 3]))):
+        n = int(rng.integers(200, 3000))
+        L = 4.0 * int(rng.integers(4, 10))
+        p = _flock_params(n, L, int(rng.choice([4, 16, 32])), weights=tuple(float(w) for w in rng.uniform(0.3, 2.0, 3)))
+        if rng.random() < 0.3:
+            p.commonSensingMinRadius = float(rng.uniform(0.0, 1.0))
+            for arr in (p.separationParams, p.alignmentParams, p.cohesionParams):
+                arr[1] = float(rng.uniform(2.0, 4.0))
+                arr[2] = float(rng.choice([-2.0, float(rng.uniform(-0.8, 0.3))]))
+        if rng.random() < 0.4:
+            k = int(rng.integers(1, 6))
+            p.numObstacles = k
+            p.obstacleAvoidanceWeight = float(rng.uniform(0.5, 2.5))
+            for o in range(k):
+                c = rng.uniform(0.0, L, 3)
+                p.obstacles[o][0], p.obstacles[o][1], p.obstacles[o][2] = (float(x) for x in c)
+                p.obstacles[o][3] = float(rng.uniform(1.0, 4.0))
+        P, W = _agents(rng, n, L)
+        W[:, 3] = rng.uniform(0.05 if rng.random() < 0.5 else 0.5, 1.0, n).astype(np.float32)
+        params.append(p)
+        pos.append(P)
+        fwd.append(W)
+    P = np.concatenate(pos)
+    w = Workload("fuzz_adjoint", params, P, np.concatenate(fwd), np.zeros_like(P), None, 0, DT, {})
+    T = int(rng.integers(4, 13))
+    k = int(rng.integers(1, T + 1))
+    target = P.copy()
+    target[:, :3] += rng.normal(0.0, 1.0, (len(P), 3)).astype(np.float32)
+    return w, target, T, k
+
+
+@pytest.mark.parametrize("seed", range(15))
+def test_random_adjoint_against_fp64_reverse_at_the_gpu_trajectory(seed):
+    """The GPU gradients (weights per flock, positions, velocities) against
+    the FP64 frozen-neighbour reverse linearised at the GPU's own FP32
+    trajectory (the adjoint's arithmetic alone), within 1e-4."""
+    from tests.test_gpu_adjoint import _counts_per_agent, _L_per_agent, _min_image, _vel_grad
+    w, target, T, k = _random_adjoint(seed)
+    with make_engine(w) as eng:
+        eng.set_option("adjoint_export", 1)
+        eng.set_state(w.pos, w.fwd, w.acc)
+        eng.adjoint_forward(target, T, k, DT)
+        g = eng.adjoint_backward()
+        lists, flags = eng.adjoint_tape(T)
+        states = eng.adjoint_tape_states(T)
+        final = eng.get_state(features=False)[0].astype(np.float64)
+    wts = np.array([[p.separationParams[0], p.alignmentParams[0], p.cohesionParams[0]] for p in w.params], np.float64)
+    d = _min_image(final[:, :3] - target[:, :3].astype(np.float64), _L_per_agent(w.params)[:, None])
+    gT = np.zeros((len(final), 4))
+    gT[:, :3] = 2.0 * d / _counts_per_agent(w.params)[:, None]
+    at = oracle.frozen_reverse_at(w.params, states, lists, gT, weights=wts, flags=flags, dt=DT)
+    at["vel"] = _vel_grad(at, w.fwd.astype(np.float64))
+
+    def nrel(a, b):
+        b = np.asarray(b, np.float64)
+        return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-300))
+
+    for f in range(len(w.params)):
+        assert nrel(g["weights"][f], at["weights"][f]) <= 1e-4, (f, g["weights"][f], at["weights"][f])
+    assert nrel(g["pos"][:, :3], at["pos"][:, :3]) <= 1e-4
+    assert nrel(g["vel"][:, :3], at["vel"][:, :3]) <= 1e-4
