@@ -132,19 +132,23 @@ __device__ __forceinline__ uint32_t scanNeighborsFlat(uint32_t self, f3 p, const
 // cells' ranges are fetched together, and candidate positions are loaded
 // UNROLL at a time before they are tested in order.
 //
-// With CULL, a neighbour cell is skipped when its box is provably farther
-// than the search radius: the distance from p to the shared face is exact
-// (p - g*cell and (g+1)*cell - p are Sterbenz-exact for g >= 1, within an ulp
-// of 4 otherwise) and any candidate of that cell lies beyond the face up to
-// the rounding of its own coordinate, so a margin of 0.01 on d^2 cannot drop a
-// candidate that would pass the exact test.  Skipping such a cell therefore
-// leaves the list unchanged.
+// With CULL and `cull` set, a neighbour cell is skipped when its box is
+// provably farther than the search radius: the distance from p to the shared
+// face is exact (p - g*cell and (g+1)*cell - p are Sterbenz-exact for g >= 1,
+// within an ulp of 4 otherwise) and any candidate of that cell lies beyond
+// the face up to the rounding of its own coordinate, so a margin of 0.01 on
+// d^2 cannot drop a candidate that would pass the exact test.  Skipping such
+// a cell therefore leaves the list unchanged.  That holds only while every
+// position lies in its hashed cell: a NaN position is hashed to cell 0 and
+// accepted by every agent that reads it (!(NaN > r2thr)), and a position
+// outside the world is clamped into an edge cell.  The caller clears `cull`
+// when the step's sorted state holds such a position.
 template <int UNROLL, bool CULL>
 __device__ __forceinline__ uint32_t scanNeighborsPipelined(uint32_t self, f3 p, const FlockDev& fl,
                                                            const uint32_t* __restrict__ cellStart,
                                                            const uint32_t* __restrict__ cellEnd,
                                                            const float4* __restrict__ posS, uint32_t* list,
-                                                           uint32_t ls) {
+                                                           uint32_t ls, bool cull) {
   const int gx = gridCoord(p.x, fl.cell, fl.G), gy = gridCoord(p.y, fl.cell, fl.G), gz = gridCoord(p.z, fl.cell, fl.G);
   const uint32_t M = fl.M;
   const float thr = fl.r2thr;
@@ -168,7 +172,7 @@ __device__ __forceinline__ uint32_t scanNeighborsPipelined(uint32_t self, f3 p, 
       const int cy = wrapCoord(gy + oy, fl.G);
       const float sy = imageShift(gy, oy, fl.G, fl.L);
       const float bxy = CULL ? bx + (oy < 0 ? lo2[1] : (oy > 0 ? hi2[1] : 0.0f)) : 0.0f;
-      if (CULL && bxy > cullThr) continue;
+      if (CULL && cull && bxy > cullThr) continue;
       uint32_t st[3], en[3];
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
@@ -182,7 +186,7 @@ __device__ __forceinline__ uint32_t scanNeighborsPipelined(uint32_t self, f3 p, 
         const uint32_t start = st[k];
         uint32_t stop = en[k];
         if (!usableRange(fl, start, stop)) continue;
-        if (CULL && bxy + (k == 0 ? lo2[2] : (k == 2 ? hi2[2] : 0.0f)) > cullThr) continue;
+        if (CULL && cull && bxy + (k == 0 ? lo2[2] : (k == 2 ? hi2[2] : 0.0f)) > cullThr) continue;
         if (fl.maxPerCell && stop - start > fl.maxPerCell) stop = start + fl.maxPerCell;
         const float sz = imageShift(gz, k - 1, fl.G, fl.L);
         // Without an image shift (every cell away from the periodic seam)
@@ -262,7 +266,9 @@ __device__ __forceinline__ uint32_t scanNeighborsPipelined(uint32_t self, f3 p, 
 // dropped before the votes.  The squared box distance is built like an
 // agent's d2, (ex * ex + ey * ey) + ez * ez with ex = max(lo - q, q - hi, 0),
 // and rounding is monotone, so it is never above any agent's d2: no
-// candidate an agent accepts is dropped.  The survivors keep their order in
+// candidate an agent accepts is dropped.  A NaN d2 passes the test, so runs
+// holding a non-finite agent coordinate take an unbounded box, and candidates
+// with a non-finite coordinate are always kept.  The survivors keep their order in
 // a per-warp staging buffer cbuf ((R + 1) * 32 entries: x, y, z with the
 // image shift, slot in w) and are voted on R rounds at a time, agent-major.
 // The lists are the same as without culling.
@@ -347,6 +353,13 @@ __device__ __forceinline__ uint32_t scanNeighborsCooperative(bool active, uint32
     bHi[0] = fromOrderedBits(__reduce_max_sync(grp, ox));
     bHi[1] = fromOrderedBits(__reduce_max_sync(grp, oy));
     bHi[2] = fromOrderedBits(__reduce_max_sync(grp, oz));
+    // A non-finite coordinate can make an agent's d2 NaN (NaN - q, or
+    // inf - inf), and a NaN d2 passes the test: such a run is not culled.
+    const bool finite = isfinite(p.x) && isfinite(p.y) && isfinite(p.z);
+    if (__reduce_or_sync(grp, finite ? 0u : 1u)) {
+      bLo[0] = bLo[1] = bLo[2] = -INFINITY;
+      bHi[0] = bHi[1] = bHi[2] = INFINITY;
+    }
   }
   while (heads) {
     const uint32_t g0 = __ffs(heads) - 1;
@@ -536,7 +549,9 @@ __device__ __forceinline__ uint32_t scanNeighborsCooperative(bool active, uint32
             const float ey = fmaxf(fmaxf(ly - v.y, v.y - hy), 0.0f);
             const float ez = fmaxf(fmaxf(lz - v.z, v.z - hz), 0.0f);
             const float b2 = ex * ex + ey * ey + ez * ez;
-            keep = !(b2 > thr);
+            // a candidate with a non-finite coordinate can give a NaN d2,
+            // which passes: it is always kept
+            keep = !(b2 > thr) || !isfinite(v.x + v.y + v.z);
           }
           const uint32_t bal = __ballot_sync(full, keep);
           if (keep) cbuf[buffered + (uint32_t)__popc(bal & below)] = v;

@@ -186,7 +186,7 @@ void freeAll(brt_engine* e) {
       if (e->ev[r][k]) cudaEventDestroy(e->ev[r][k]);
   void* ptrs[] = {e->flocks, e->agentBase, e->obstacles, e->obsMask, e->posA, e->fwdA, e->accA, e->posS, e->fwdS, e->accS,
                   e->featA, e->featS, e->idA, e->idS, e->statsById, e->steer, e->lists, e->pairs[0], e->pairs[1],
-                  e->cellStart, e->cellEnd, e->sortMem, e->errWord, e->stage4, e->stageF, e->stepCounter,
+                  e->cellStart, e->cellEnd, e->sortMem, e->errWord, e->stage4, e->stageF, e->stepCounter, e->cullWords,
                   e->membership[0], e->membership[1], e->resortMem};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -312,6 +312,10 @@ int enqueueReorder(brt_engine* e, bool incremental = false) {
   R.cellStart = e->cellStart; R.cellEnd = e->cellEnd;
   R.hist = e->ss.hist; R.histWords = e->plan.passes * e->plan.bins;
   R.n = e->N; R.numCells = e->C; R.errWord = e->errWord;
+  if (e->scanVariant == 0 || e->scanVariant == 1) {
+    R.cullWords = e->cullWords;
+    R.flocks = e->flocks; R.agentBase = e->agentBase; R.nflocks = e->nflocks;
+  }
   if (rs) {
     R.resortMode = e->rsWords + kResortWordMode;
     R.newStart = e->rsNewStart;
@@ -354,6 +358,7 @@ int enqueueStep(brt_engine* e, float dt, bool record) {
   F.scanVariant = e->scanVariant;
   F.tiles = e->tiles; F.numTiles = e->numTiles; F.tileCounter = e->tileCounter; F.tileBlocks = e->tileBlocks;
   F.stepCounter = e->stepCounter;
+  F.cullGate = (e->scanVariant == 0 || e->scanVariant == 1) ? e->cullWords + 2 : nullptr;
   // The single-pass kernel covers every flock unless one needs clustering
   // steering (it needs the whole list first) or kNN lists longer than a warp.
   // kNN flocks take its cooperative kNN scan (scan 8).
@@ -587,6 +592,7 @@ int brt_engine_create(const brt_params* flocks, uint32_t num_flocks, int device,
   chk(devAlloc(&e->cellStart, e->Cpad)); chk(devAlloc(&e->cellEnd, e->Cpad));
   chk(devAlloc(&e->errWord, 1));
   chk(devAlloc(&e->stepCounter, 1));
+  chk(devAlloc(&e->cullWords, 4));
   chk(devAlloc(&e->stage4, n));
   chk(devAlloc(&e->stageF, std::max<size_t>(1, n * e->Fmax)));
   const size_t sortBytes = sortScratchBytes(e->plan, false);
@@ -625,6 +631,7 @@ int brt_engine_create(const brt_params* flocks, uint32_t num_flocks, int device,
   }
   BRT_CUDA_TRY(cudaMemsetAsync(e->errWord, 0, 4, st));
   BRT_CUDA_TRY(cudaMemsetAsync(e->stepCounter, 0, 4, st));
+  BRT_CUDA_TRY(cudaMemsetAsync(e->cullWords, 0, 16, st));
   if (n) {
     BRT_CUDA_TRY(cudaMemsetAsync(e->posA, 0, n * 16, st));
     BRT_CUDA_TRY(cudaMemsetAsync(e->fwdA, 0, n * 16, st));

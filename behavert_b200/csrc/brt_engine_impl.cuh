@@ -28,6 +28,10 @@ struct brt_engine {
   bool anyKnn = false;
   bool school = false;        // the flocks use the Schooling law (schooling.mode 1 or 2)
   uint32_t* stepCounter = nullptr;  // device word: steps taken (keys the Schooling random stream)
+  // device words of the cell-cull gate of scan variants 0 and 1: accumulator,
+  // block ticket, and the result the flock kernel reads (nonzero: a sorted
+  // position is NaN or outside the world, so cells are not culled)
+  uint32_t* cullWords = nullptr;
   float4* membership[2] = {nullptr, nullptr};  // clusterMembership by agent id (ping-pong)
   int membershipCur = 0;
   bool forceTwoPass = false;  // option "two_pass": run the list-first kernel even when not needed

@@ -263,9 +263,10 @@ __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs 
     }
     if (!active) return;
   } else {
-    n = A.scanVariant == 0 ? scanNeighborsPipelined<4, true>(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls)
-      : A.scanVariant == 1 ? scanNeighborsPipelined<2, true>(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls)
-      : A.scanVariant == 2 ? scanNeighborsPipelined<4, false>(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls)
+    const bool cull = A.cullGate && __ldg(A.cullGate) == 0u;
+    n = A.scanVariant == 0 ? scanNeighborsPipelined<4, true>(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls, cull)
+      : A.scanVariant == 1 ? scanNeighborsPipelined<2, true>(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls, cull)
+      : A.scanVariant == 2 ? scanNeighborsPipelined<4, false>(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls, false)
                            : scanNeighborsFlat(i, p, fl, A.cellStart, A.cellEnd, A.posS, list, ls);
   }
   if (A.lists) {

@@ -74,6 +74,7 @@ __global__ void __launch_bounds__(256) reorderKernel(ReorderArgs A) {
     }
   }
   if (gtid == 0 && A.resortValid) *A.resortValid = 1u;
+  bool outside = false;  // cell-cull gate: a position of this thread's slots lies outside its cell
   for (uint32_t i = gtid; i < A.n; i += gstride) {
     const uint2 kv = A.pairs[i];
     const uint32_t key = kv.x, ps = kv.y;
@@ -105,12 +106,33 @@ __global__ void __launch_bounds__(256) reorderKernel(ReorderArgs A) {
       }
       pos.w = sqrtf(nn);
     }
+    if (A.cullWords && !outside) {
+      const FlockDev& fl = A.flocks[A.nflocks == 1 ? 0u : flockOfSlot(A.agentBase, A.nflocks, i)];
+      outside = !(pos.x >= 0.0f && pos.x <= fl.L && pos.y >= 0.0f && pos.y <= fl.L && pos.z >= 0.0f && pos.z <= fl.L);
+    }
     A.posS[i] = pos;
     if (key != prev) {
       A.cellStart[key] = i;
       if (A.moverHead) { A.moverHead[key] = kNoMover; A.moverCount[key] = 0u; }
     }
     if (key != next) A.cellEnd[key] = i + 1;
+  }
+  if (A.cullWords) {
+    // Scan variants 0 and 1 skip a neighbour cell by the distance from the
+    // agent to the cell's face.  That bounds a candidate's distance only when
+    // both lie in their hashed cells, which every finite position inside the
+    // world does (L is a whole number of cells); a NaN position (clamped into
+    // cell 0) or one outside the world (clamped into an edge cell) does not.
+    // The last block to finish publishes the OR of all blocks' flags and
+    // leaves the accumulator and the ticket at zero for the next launch.
+    if (__syncthreads_or(outside) && threadIdx.x == 0) atomicOr(&A.cullWords[0], 1u);
+    if (threadIdx.x == 0) {
+      __threadfence();
+      if (atomicAdd(&A.cullWords[1], 1u) == gridDim.x - 1) {
+        A.cullWords[2] = atomicExch(&A.cullWords[0], 0u);
+        A.cullWords[1] = 0u;
+      }
+    }
   }
 }
 

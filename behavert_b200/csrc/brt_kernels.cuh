@@ -45,6 +45,12 @@ struct ReorderArgs {
   const uint32_t* newStart;    // per cell, from the re-sort's cell scan
   uint32_t* moverCount; uint32_t* moverHead;  // reset for every cell seen
   uint32_t* resortValid;       // set: the next step may re-sort from this order
+  // cell-cull gate of scan variants 0 and 1 (null: not computed).  Words
+  // [0] and [1] are the launch's accumulator and block ticket, both back at
+  // zero when the launch ends; [2] is set to nonzero when a sorted position
+  // is NaN or outside [0, L] on some axis of its flock's world.
+  uint32_t* cullWords;
+  const FlockDev* flocks; const uint32_t* agentBase; uint32_t nflocks;
 };
 
 struct FusedArgs {
@@ -65,6 +71,8 @@ struct FusedArgs {
                                // 6: staged tiles (tileFlockKernel), 7: warp-cooperative with
                                // bounding-box culling
   const uint32_t* stepCounter; // random-stream step of the Schooling move
+  const uint32_t* cullGate;    // scan variants 0 and 1: cells are culled only when
+                               // this word is zero (null: never culled)
   // scan variant 6: the (flock, row segment) tiles and the work-queue counter
   const uint4* tiles;          // x flock, y row y | z << 16, z first x | cells << 16
   uint32_t numTiles;

@@ -197,8 +197,18 @@ struct Flock {
 };
 
 // envgrid3d_resources.cu:60-84 (calcGridPos + clamping calcGridHash), origin 0.
+// calcGridPos assigns floor(...) to an int in device code, a conversion that
+// saturates at the int range and takes NaN to 0 (PTX cvt.rzi.s32.f32); a
+// plain C++ cast of +inf or of a value past the int range is undefined (x86
+// gives INT_MIN, which would clamp to cell 0 instead of G - 1).
+inline int deviceFloatToInt(float v) {
+  if (std::isnan(v)) return 0;
+  if (v >= 2147483648.0f) return INT32_MAX;
+  if (v < -2147483648.0f) return INT32_MIN;
+  return (int)v;
+}
 inline int gridCoord(float x, float cell, uint32_t G) {
-  int g = (int)std::floor(x / cell);
+  int g = deviceFloatToInt(std::floor(x / cell));
   return std::max(0, std::min(g, (int)G - 1));
 }
 inline uint32_t cellHash(int gx, int gy, int gz, uint32_t G) {

@@ -289,7 +289,8 @@ def cluster_hit_rate(params: Sequence, pos_in, step_out: dict, labels, radius: f
     ps = np.ascontiguousarray(pos_in, np.float32)[ids, :3]
 
     def grid(x):
-        return np.clip(np.floor(x / cell), 0, G - 1).astype(np.int64)
+        # the device's float-to-int conversion takes NaN to 0 and saturates
+        return np.nan_to_num(np.clip(np.floor(x / cell), 0, G - 1), nan=0.0).astype(np.int64)
 
     gi = grid(ps)
     my = labels[ids]

@@ -226,3 +226,28 @@ def test_random_adjoint_against_fp64_reverse_at_the_gpu_trajectory(seed):
         assert nrel(g["weights"][f], at["weights"][f]) <= 1e-4, (f, g["weights"][f], at["weights"][f])
     assert nrel(g["pos"][:, :3], at["pos"][:, :3]) <= 1e-4
     assert nrel(g["vel"][:, :3], at["vel"][:, :3]) <= 1e-4
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_random_configuration_every_scan_variant(seed):
+    """The random forward draws under every scan loop and list walk of the
+    flock kernel: lists and state bit-identical to the default options."""
+    w = _random_workload(200 + seed)
+
+    def run(options):
+        with make_engine(w) as eng:
+            for k, v in options:
+                eng.set_option(k, v)
+            eng.record_lists(True)
+            eng.step(DT, 2)
+            return eng.getNeighborLists(), eng.get_state()
+
+    ref_lists, ref = run([])
+    for scan, walk in ((0, 0), (0, 1), (1, 0), (2, 1), (3, 0), (4, 0), (4, 2), (5, 0), (6, 2), (7, 2)):
+        lists, out = run([("scan_variant", scan), ("phase2_variant", walk)])
+        assert np.array_equal(lists[:, 0], ref_lists[:, 0]), (scan, walk)
+        mask = np.arange(lists.shape[1] - 1)[None, :] < lists[:, :1]
+        assert np.array_equal(np.where(mask, lists[:, 1:], 0), np.where(mask, ref_lists[:, 1:], 0)), (scan, walk)
+        for a, b in zip(ref, out):
+            if a is not None:
+                assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (scan, walk)

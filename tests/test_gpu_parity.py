@@ -31,7 +31,8 @@ def _rel(a, b):
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
     scale = max(np.abs(b).max(), 1e-30)
-    return float(np.abs(a - b).max() / scale)
+    with np.errstate(invalid="ignore"):  # states holding inf report NaN here
+        return float(np.abs(a - b).max() / scale)
 
 
 def _vel(fwd):
@@ -428,6 +429,38 @@ def test_edge_cases_dense_boundary_frozen():
     w.fwd[:5, 3] = -1.0  # frozen agents (speed < 0)
     with make_engine(w) as eng:
         check_step(eng, w.params, fp64=False)
+
+
+def _non_finite_workload(seed):
+    """Positions a neighbour-cell cull must not trust: NaN agents (every axis,
+    and one axis only) hashed into cell 0 beside finite agents there, infinite
+    coordinates, and agents outside the world clamped into edge cells.  A NaN
+    candidate passes the radius test (!(NaN > r)) of every agent that reads
+    its cell; a NaN agent accepts every candidate it reads."""
+    n = 600
+    w = workloads.plain(n=n, L=16.0, M=40, seed=seed)
+    rng = np.random.default_rng(seed)
+    w.pos[:40, :3] = (rng.random((40, 3)) * 3.0).astype(np.float32)
+    w.pos[40:43, :3] = np.nan
+    w.pos[43, 0] = np.nan
+    w.pos[44, 1] = np.inf
+    w.pos[45, 2] = -np.inf
+    w.pos[46, 0] = -3.0
+    w.pos[47, 0] = 21.0
+    w.pos[48, 1] = 17.5
+    return w
+
+
+@pytest.mark.parametrize("scan,walk", [(0, 0), (1, 0), (2, 1), (3, 0), (4, 0), (5, 2), (6, 2), (7, 2)])
+def test_non_finite_and_outside_positions_every_scan(scan, walk):
+    """Every scan loop against the oracle on such a state, two steps (the
+    NaN spreads to the neighbours in the first)."""
+    w = _non_finite_workload(7)
+    with make_engine(w) as eng:
+        eng.set_option("scan_variant", scan)
+        eng.set_option("phase2_variant", walk)
+        for _ in range(2):
+            check_step(eng, w.params, fp64=False)
 
 
 def test_single_agent_and_tiny_flock():

@@ -164,3 +164,20 @@ def test_golden_fixtures(name):
     out = run_case(CASES[name])
     for k in data.files:
         assert np.array_equal(out[k], data[k]), (name, k)
+
+
+def test_hash_of_non_finite_and_outside_positions():
+    """calcGridPos (envgrid3d_resources.cu:60-67) assigns floor(x / cell) to
+    an int in device code: the conversion saturates and takes NaN to 0, and
+    calcGridHash clamps into the grid.  So +inf and values past the int range
+    hash into the last cell, NaN, -inf and negative values into cell 0."""
+    w = _small(n=8, L=16.0, M=4, seed=2)
+    w.pos[:, :3] = 6.0
+    xs = [np.nan, np.inf, -np.inf, 1e30, -5.0, 19.0, -1e30, 15.999]
+    want = [0, 3, 0, 3, 0, 3, 0, 3]
+    w.pos[:, 0] = np.array(xs, np.float32)
+    o = oracle.step(w.params, w.pos, w.fwd, w.acc, dt=0.1)
+    key_of_id = np.empty(8, np.int64)
+    key_of_id[o["ids"]] = o["keys"]
+    home = (1 * 4 + 1) * 4  # y and z in cell 1
+    assert key_of_id.tolist() == [home + g for g in want]
