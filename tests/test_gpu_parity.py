@@ -463,6 +463,35 @@ def test_non_finite_and_outside_positions_every_scan(scan, walk):
             check_step(eng, w.params, fp64=False)
 
 
+@pytest.mark.parametrize("M", [16, 40])
+def test_non_finite_and_outside_positions_knn(M):
+    """kNN lists on the same state: the cooperative kNN scan (maxNeighbors up
+    to a warp) and the two-pass kernel above it.  A NaN distance fills a free
+    list entry but never displaces a kept one (dist < maxDistValue fails)."""
+    w = _non_finite_workload(7)
+    w.params[0].useKnn = 1
+    w.params[0].maxNeighbors = M
+    with make_engine(w) as eng:
+        for _ in range(2):
+            check_step(eng, w.params, fp64=False)
+
+
+def test_non_finite_and_outside_positions_crowd_order():
+    """The stage-wise crowd order on the same state."""
+    w = _non_finite_workload(7)
+    with make_engine(w) as eng:
+        pos, fwd, acc, _ = eng.get_state()
+        eng.update_crowd(w.dt)
+        lists = eng.getNeighborLists()
+        gpos, gfwd, gacc, _ = eng.get_state()
+    o = oracle.step(w.params, pos, fwd, acc, dt=w.dt, mode=0, avoid_neighbors=True)
+    cnt = lists[:, 0]
+    assert np.array_equal(cnt, o["lists"][:, 0])
+    mask = np.arange(lists.shape[1] - 1)[None, :] < cnt[:, None]
+    assert np.array_equal(np.where(mask, lists[:, 1:], 0), np.where(mask, o["lists"][:, 1:], 0))
+    assert _same_bits(gpos, o["pos"]) and _same_bits(gfwd, o["fwd"]) and _same_bits(gacc, o["acc"])
+
+
 def test_single_agent_and_tiny_flock():
     w = workloads.plain(n=1, L=12.0, M=4, seed=2)
     with make_engine(w) as eng:

@@ -47,6 +47,32 @@ def test_one_step_bit_exact(mode):
 
 
 @pytest.mark.parametrize("mode", [1, 2])
+def test_non_finite_and_outside_positions(mode):
+    """NaN agents (every axis, one axis) beside finite agents in cell 0,
+    infinite coordinates and agents outside the world: lists, order and state
+    as the oracle's, NaN for NaN."""
+    from tests.test_gpu_parity import _same_bits
+    o = _oracle()
+    w = workloads.schooling(n=600, L=16.0, mode=mode)
+    rng = np.random.default_rng(7)
+    w.pos[:40, :3] = (rng.random((40, 3)) * 3.0).astype(np.float32)
+    w.pos[40:43, :3] = np.nan
+    w.pos[43, 0] = np.nan
+    w.pos[44, 1] = np.inf
+    w.pos[45, 2] = -np.inf
+    w.pos[46, 0] = -3.0
+    w.pos[47, 0] = 21.0
+    (pos, fwd, acc, _), ((keys, ids), lists) = _gpu_steps(w, 1, record=True)
+    r = o.step(w.params, w.pos, w.fwd, w.acc, dt=w.dt, mode=0, random_step=1)
+    assert np.array_equal(keys, r["keys"]) and np.array_equal(ids, r["ids"])
+    cnt = lists[:, 0]
+    assert np.array_equal(cnt, r["lists"][:, 0])
+    mask = np.arange(lists.shape[1] - 1)[None, :] < cnt[:, None]
+    assert np.array_equal(np.where(mask, lists[:, 1:], 0), np.where(mask, r["lists"][:, 1:], 0))
+    assert _same_bits(pos, r["pos"]) and _same_bits(fwd, r["fwd"]) and _same_bits(acc, r["acc"])
+
+
+@pytest.mark.parametrize("mode", [1, 2])
 def test_full_size_two_steps_bit_exact(mode):
     """1,048,576 agents in the cube of side 256 (the size the benchmark
     measures): two steps, lists, order and state bit-exact."""
