@@ -434,9 +434,10 @@ def test_edge_cases_dense_boundary_frozen():
 def _non_finite_workload(seed):
     """Positions a neighbour-cell cull must not trust: NaN agents (every axis,
     and one axis only) hashed into cell 0 beside finite agents there, infinite
-    coordinates, and agents outside the world clamped into edge cells.  A NaN
-    candidate passes the radius test (!(NaN > r)) of every agent that reads
-    its cell; a NaN agent accepts every candidate it reads."""
+    coordinates, agents outside the world clamped into edge cells (some past
+    the int range of the cell conversion).  A NaN candidate passes the radius
+    test (!(NaN > r)) of every agent that reads its cell; a NaN agent accepts
+    every candidate it reads."""
     n = 600
     w = workloads.plain(n=n, L=16.0, M=40, seed=seed)
     rng = np.random.default_rng(seed)
@@ -448,6 +449,8 @@ def _non_finite_workload(seed):
     w.pos[46, 0] = -3.0
     w.pos[47, 0] = 21.0
     w.pos[48, 1] = 17.5
+    w.pos[49, 2] = 1e30   # past the int range: the device conversion saturates (last cell)
+    w.pos[50, 0] = -1e30
     return w
 
 
