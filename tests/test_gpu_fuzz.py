@@ -8,7 +8,9 @@ cap, the 2D projection, features with and without relaxation, sphere
 obstacles, a sensing minimum radius and angle cuts, dense clumps, coincident
 agents and speeds down into the low-speed branch.  The same for the
 Schooling law (random zones, limits, weights, speed and random deviation)
-and for the crowd order run stage by stage."""
+and for the crowd order run stage by stage.  Further draws run every scan
+loop, and random draws of every launch option, against the default options
+(bit-identical lists and state)."""
 import numpy as np
 import pytest
 
@@ -21,15 +23,17 @@ pytestmark = pytest.mark.gpu
 DT = float(np.float32(0.1))
 
 
-def _random_workload(seed: int) -> Workload:
+def _random_workload(seed: int, flocks=None, max_agents: int = 3000) -> Workload:
+    """`flocks`: (low, high) bounds of the flock count, drawn uniformly;
+    1 to 3 (1 twice as likely) otherwise."""
     rng = np.random.default_rng(5000 + seed)
-    nflocks = int(rng.choice([1, 1, 2, 3]))
+    nflocks = int(rng.choice([1, 1, 2, 3])) if flocks is None else int(rng.integers(flocks[0], flocks[1] + 1))
     F = int(rng.choice([0, 0, 4, 8]))
     relax = float(rng.choice([0.0, 0.05]))
     params, pos, fwd, feat = [], [], [], []
     for _ in range(nflocks):
         L = 4.0 * int(rng.integers(3, 12))
-        n = int(rng.integers(1, 3000))
+        n = int(rng.integers(1, max_agents))
         M = int(rng.choice([1, 4, 16, 32, 40]))
         p = _flock_params(n, L, M, weights=tuple(float(w) for w in rng.uniform(0.2, 2.0, 3)), F=F, relax=relax)
         p.useKnn = int(rng.random() < 0.3)
@@ -73,6 +77,16 @@ def _random_workload(seed: int) -> Workload:
 @pytest.mark.parametrize("seed", range(80))
 def test_random_configuration_two_steps(seed):
     w = _random_workload(seed)
+    with make_engine(w) as eng:
+        for _ in range(2):
+            check_step(eng, w.params, dt=DT, fp64=False)
+
+
+@pytest.mark.parametrize("seed", range(24))
+def test_random_batch_of_many_flocks_two_steps(seed):
+    """4 to 48 flocks of 1 to 800 agents in one engine (the batched path:
+    per-flock cell bases, parameters and list modes side by side)."""
+    w = _random_workload(600 + seed, flocks=(4, 48), max_agents=800)
     with make_engine(w) as eng:
         for _ in range(2):
             check_step(eng, w.params, dt=DT, fp64=False)
@@ -251,3 +265,40 @@ def test_random_configuration_every_scan_variant(seed):
         for a, b in zip(ref, out):
             if a is not None:
                 assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (scan, walk)
+
+
+@pytest.mark.parametrize("seed", range(64))
+def test_random_configuration_random_options(seed):
+    """Random forward draws under a random draw of every launch option the
+    autotuner and the user can set (block size, sort digit width, scan loop,
+    list walk, register budget, incremental re-sort, forced two-pass kernel):
+    lists and state after three steps bit-identical to the default options.
+    Odd draws hold 4 to 48 flocks."""
+    w = _random_workload(400 + seed, **({"flocks": (4, 48), "max_agents": 800} if seed % 2 else {}))
+    rng = np.random.default_rng(12000 + seed)
+    options = [
+        ("block_size", int(rng.choice([32, 64, 96, 128, 160, 192, 256]))),
+        ("sort_digit_bits", int(rng.integers(4, 10))),
+        ("scan_variant", int(rng.integers(0, 8))),
+        ("phase2_variant", int(rng.integers(0, 3))),
+        ("registers", int(rng.choice([40, 48, 64, 128]))),
+        ("incremental_sort", int(rng.integers(0, 2))),
+        ("two_pass", int(rng.random() < 0.25)),
+    ]
+
+    def run(opts):
+        with make_engine(w) as eng:
+            for k, v in opts:
+                eng.set_option(k, v)
+            eng.record_lists(True)
+            eng.step(DT, 3)
+            return eng.getNeighborLists(), eng.get_state()
+
+    ref_lists, ref = run([])
+    lists, out = run(options)
+    assert np.array_equal(lists[:, 0], ref_lists[:, 0]), options
+    mask = np.arange(lists.shape[1] - 1)[None, :] < lists[:, :1]
+    assert np.array_equal(np.where(mask, lists[:, 1:], 0), np.where(mask, ref_lists[:, 1:], 0)), options
+    for a, b in zip(ref, out):
+        if a is not None:
+            assert _same_bits(a, b), options
