@@ -250,7 +250,8 @@ __device__ __forceinline__ uint32_t scanNeighborsPipelined(uint32_t self, f3 p, 
 // each lane give the position of each accepted candidate in that agent's
 // list.  Lists are identical to the per-agent scan: same candidates, same
 // order, same predicate !(d2 > r2thr) on ((q + s) - p)^2 sums, self excluded,
-// first M kept.  Cells are not culled (culling never changes a list).
+// first M kept.  Cells are not culled: every candidate of the 27 cells is
+// tested, so a NaN candidate (which passes every agent's test) is never lost.
 //
 // With R > 0 the run's first R rounds of candidates are loaded into registers
 // up front and each agent then goes through them alone (agent-major): its
