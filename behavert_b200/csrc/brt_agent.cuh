@@ -23,7 +23,7 @@ __device__ __forceinline__ uint32_t buildNeighborList(uint32_t self, f3 p, const
                                                       const uint32_t* __restrict__ cellEnd,
                                                       const float4* __restrict__ posS, uint32_t* list,
                                                       uint32_t ls, float* distList) {
-  const int gx = gridCoord(p.x, fl.cell, fl.G), gy = gridCoord(p.y, fl.cell, fl.G), gz = gridCoord(p.z, fl.cell, fl.G);
+  const int gx = gridCoord(p.x, fl), gy = gridCoord(p.y, fl), gz = gridCoord(p.z, fl);
   const uint32_t M = fl.M;
   // kNN replacement is per flock: an engine may mix kNN and first-M flocks
   const bool knn = KNN && fl.useKnn;
@@ -85,7 +85,7 @@ __device__ __forceinline__ uint32_t scanNeighborsFlat(uint32_t self, f3 p, const
                                                       const uint32_t* __restrict__ cellEnd,
                                                       const float4* __restrict__ posS, uint32_t* list,
                                                       uint32_t ls) {
-  const int gx = gridCoord(p.x, fl.cell, fl.G), gy = gridCoord(p.y, fl.cell, fl.G), gz = gridCoord(p.z, fl.cell, fl.G);
+  const int gx = gridCoord(p.x, fl), gy = gridCoord(p.y, fl), gz = gridCoord(p.z, fl);
   const uint32_t M = fl.M;
   const float thr = fl.r2thr;
   uint32_t n = 0;
@@ -149,7 +149,7 @@ __device__ __forceinline__ uint32_t scanNeighborsPipelined(uint32_t self, f3 p, 
                                                            const uint32_t* __restrict__ cellEnd,
                                                            const float4* __restrict__ posS, uint32_t* list,
                                                            uint32_t ls, bool cull) {
-  const int gx = gridCoord(p.x, fl.cell, fl.G), gy = gridCoord(p.y, fl.cell, fl.G), gz = gridCoord(p.z, fl.cell, fl.G);
+  const int gx = gridCoord(p.x, fl), gy = gridCoord(p.y, fl), gz = gridCoord(p.z, fl);
   const uint32_t M = fl.M;
   const float thr = fl.r2thr;
   // squared distances to the lower / upper faces of the home cell
@@ -375,7 +375,7 @@ __device__ __forceinline__ uint32_t scanNeighborsCooperative(bool active, uint32
     const uint32_t G = fl.G;
     // home cell coordinates from the group's first agent
     const float px = __shfl_sync(full, p.x, g0), py = __shfl_sync(full, p.y, g0), pz = __shfl_sync(full, p.z, g0);
-    const int gx = gridCoord(px, fl.cell, G), gy = gridCoord(py, fl.cell, G), gz = gridCoord(pz, fl.cell, G);
+    const int gx = gridCoord(px, fl), gy = gridCoord(py, fl), gz = gridCoord(pz, fl);
     // lanes 0..26: one neighbour cell each, in visit order
     uint32_t segStart = 0, segLen = 0;
     float sx = 0.0f, sy = 0.0f, sz = 0.0f;
@@ -723,9 +723,9 @@ __device__ __forceinline__ AgentCtx makeCtx(float4 p4, float4 w4, const FlockDev
   a.pos = xyz(p4);
   a.fwd = xyz(w4);
   a.speed = w4.w;
-  a.g[0] = gridCoord(a.pos.x, fl.cell, fl.G);
-  a.g[1] = gridCoord(a.pos.y, fl.cell, fl.G);
-  a.g[2] = gridCoord(a.pos.z, fl.cell, fl.G);
+  a.g[0] = gridCoord(a.pos.x, fl);
+  a.g[1] = gridCoord(a.pos.y, fl);
+  a.g[2] = gridCoord(a.pos.z, fl);
   const int hi = (int)fl.G - 1;
   a.interior = a.g[0] > 0 && a.g[0] < hi && a.g[1] > 0 && a.g[1] < hi && a.g[2] > 0 && a.g[2] < hi;
   return a;
@@ -735,9 +735,9 @@ __device__ __forceinline__ f3 neighborImage(const AgentCtx& a, float4 q4, const 
   f3 q = xyz(q4);
   float sx = 0.0f, sy = 0.0f, sz = 0.0f;
   if (!a.interior) {
-    sx = imageShiftCells(a.g[0], gridCoord(q.x, fl.cell, fl.G), fl.G, fl.L);
-    sy = imageShiftCells(a.g[1], gridCoord(q.y, fl.cell, fl.G), fl.G, fl.L);
-    sz = imageShiftCells(a.g[2], gridCoord(q.z, fl.cell, fl.G), fl.G, fl.L);
+    sx = imageShiftCells(a.g[0], gridCoord(q.x, fl), fl.G, fl.L);
+    sy = imageShiftCells(a.g[1], gridCoord(q.y, fl), fl.G, fl.L);
+    sz = imageShiftCells(a.g[2], gridCoord(q.z, fl), fl.G, fl.L);
   }
   return mk3(q.x + sx, q.y + sy, q.z + sz);
 }

@@ -71,6 +71,14 @@ static FlockDev toDev(const brt_params& p, uint32_t G) {
   d.n = p.numBodies;
   d.L = p.worldSize;
   d.cell = p.cellSize;
+  {
+    // exact reciprocal of a power-of-two cell (mantissa 0.5 after frexp),
+    // when it is a normal float: x * invCell then equals x / cell bit for bit
+    int ex = 0;
+    const float m = std::frexp(p.cellSize, &ex);
+    const float inv = std::ldexp(1.0f, 1 - ex);
+    d.invCell = (m == 0.5f && std::isnormal(inv) && inv * p.cellSize == 1.0f) ? inv : 0.0f;
+  }
   d.radius = p.commonSearchRadius;
   d.r2thr = radiusThreshold(p.commonSearchRadius);
   d.M = p.maxNeighbors;

@@ -237,7 +237,12 @@ __global__ void __launch_bounds__(kFlockMaxThreads, MINB) flockKernel(FusedArgs 
   const float4 p4 = __ldg(&A.posS[i]);
   const f3 p = xyz(p4);
   const uint32_t G = fl.G;
-  const int gx = gridCoord(p.x, fl.cell, G), gy = gridCoord(p.y, fl.cell, G), gz = gridCoord(p.z, fl.cell, G);
+  // The plain quotient here (the same cell as gridCoord's product): measured,
+  // the product at this point changes ptxas's register allocation of the
+  // feature-carrying instantiations (116 against 104 spilled bytes) and costs
+  // 2% on the 1M-agent flock, while the product everywhere else saves 0.6%
+  // there and 2.2% on the batched flocks.
+  const int gx = gridCoordQuotient(p.x, fl), gy = gridCoordQuotient(p.y, fl), gz = gridCoordQuotient(p.z, fl);
   const uint32_t M = fl.M;
   uint32_t* list = sList + threadIdx.x;
   // The cooperative scan stores 32 rows of one agent's column per vote: an
@@ -453,7 +458,7 @@ __global__ void __launch_bounds__(kTileThreads, 4) tileFlockKernel(FusedArgs A) 
       const uint32_t i = active ? i0 : hi - 1;  // inactive lanes mirror the last agent (read-only)
       const float4 p4 = __ldg(&A.posS[i]);
       const f3 p = xyz(p4);
-      const int gx = gridCoord(p.x, fl.cell, G), gy = gridCoord(p.y, fl.cell, G), gz = gridCoord(p.z, fl.cell, G);
+      const int gx = gridCoord(p.x, fl), gy = gridCoord(p.y, fl), gz = gridCoord(p.z, fl);
       uint32_t n = 0;
       if (staged) {
         // an agent outside the tile's cells only follows a corrupted step

@@ -53,7 +53,7 @@ struct FlockDev {
   uint32_t numObstacles;
   float obsW;
   uint32_t obsBase;     // first entry in the engine-wide obstacle table
-  uint32_t pad;
+  float invCell;        // 1 / cell when cell is a power of two (exact), else 0
   // inBoidNeighborhood as exact squared-distance tests:
   //   dist < minR  <=>  d2 < minT,   dist > maxR_b  <=>  d2 > maxT_b
   float minT, sepT, aliT, cohT;
@@ -83,9 +83,18 @@ __host__ __device__ __forceinline__ float clampf(float f, float a, float b) { re
 __host__ __device__ __forceinline__ f3 xyz(float4 v) { return mk3(v.x, v.y, v.z); }
 
 // envgrid3d_resources.cu:60-84 with origin 0 and clamping to the grid.
-__device__ __forceinline__ int gridCoord(float x, float cell, uint32_t G) {
-  int g = (int)floorf(x / cell);
-  return max(0, min(g, (int)G - 1));
+// x / cell for a power-of-two cell is computed as x * (1 / cell): the
+// reciprocal is exact, and the product and the quotient are the correctly
+// rounded values of the same real number, so they agree bit for bit (NaN,
+// infinities and subnormals included) at a fraction of an IEEE division.
+__device__ __forceinline__ int gridCoordQuotient(float x, const FlockDev& fl) {
+  int g = (int)floorf(x / fl.cell);
+  return max(0, min(g, (int)fl.G - 1));
+}
+__device__ __forceinline__ int gridCoord(float x, const FlockDev& fl) {
+  const float u = fl.invCell != 0.0f ? x * fl.invCell : x / fl.cell;
+  int g = (int)floorf(u);
+  return max(0, min(g, (int)fl.G - 1));
 }
 
 // Neighbour cell through offset o from home coordinate g, with its image shift.

@@ -37,7 +37,7 @@ __global__ void __launch_bounds__(256) hashKernel(HashArgs A) {
     const uint32_t f = A.nflocks == 1 ? 0u : flockOfSlot(A.agentBase, A.nflocks, j);
     const FlockDev& fl = A.flocks[f];
     const float4 p = __ldg(&A.pos[j]);
-    const int gx = gridCoord(p.x, fl.cell, fl.G), gy = gridCoord(p.y, fl.cell, fl.G), gz = gridCoord(p.z, fl.cell, fl.G);
+    const int gx = gridCoord(p.x, fl), gy = gridCoord(p.y, fl), gz = gridCoord(p.z, fl);
     const uint32_t key = fl.cellBase + ((uint32_t)gz * fl.G + (uint32_t)gy) * fl.G + (uint32_t)gx;
     const uint32_t id = __ldg(&A.id[j]);
     A.pairs[id] = make_uint2(key, j);
@@ -172,8 +172,8 @@ __global__ void __launch_bounds__(kFusedThreads) fusedKernel(FusedArgs A) {
   } else {
     const f3 p = xyz(p4);
     const uint32_t G = fl.G;
-    const uint32_t key = fl.cellBase + ((uint32_t)gridCoord(p.z, fl.cell, G) * G + (uint32_t)gridCoord(p.y, fl.cell, G)) * G +
-                         (uint32_t)gridCoord(p.x, fl.cell, G);
+    const uint32_t key = fl.cellBase + ((uint32_t)gridCoord(p.z, fl) * G + (uint32_t)gridCoord(p.y, fl)) * G +
+                         (uint32_t)gridCoord(p.x, fl);
     n = scanNeighborsCooperative<kCoopCachedRounds, kCoopWindowAgents>(active, i, p, key, A.flocks, f, A.cellStart,
                                                                       A.cellEnd, A.posS, sList, ls, threadIdx.x & ~31u);
     if (!active) return;
@@ -238,8 +238,8 @@ __global__ void __launch_bounds__(128) listsKernel(StageArgs A) {
     out[0] = buildNeighborList<true>(i, p, fl, A.cellStart, A.cellEnd, A.posS, out + 1, 1, distL);
   } else {
     const uint32_t G = fl.G;
-    const uint32_t key = fl.cellBase + ((uint32_t)gridCoord(p.z, fl.cell, G) * G + (uint32_t)gridCoord(p.y, fl.cell, G)) * G +
-                         (uint32_t)gridCoord(p.x, fl.cell, G);
+    const uint32_t key = fl.cellBase + ((uint32_t)gridCoord(p.z, fl) * G + (uint32_t)gridCoord(p.y, fl)) * G +
+                         (uint32_t)gridCoord(p.x, fl);
     const uint32_t ls = blockDim.x + 1;
     const uint32_t n = scanNeighborsCooperative<kCoopCachedRounds, kCoopWindowAgents>(
         active, i, p, key, A.flocks, f, A.cellStart, A.cellEnd, A.posS, sList, ls, threadIdx.x & ~31u);

@@ -140,8 +140,8 @@ __global__ void __launch_bounds__(kMarkThreads) resortMarkKernel(ResortArgs A, u
     if (slot[k] < A.n) {
       const uint32_t f = A.nflocks == 1 ? 0u : flockOfSlot(A.agentBase, A.nflocks, slot[k]);
       const FlockDev& fl = A.flocks[f];
-      const int gx = gridCoord(p[k].x, fl.cell, fl.G), gy = gridCoord(p[k].y, fl.cell, fl.G),
-                gz = gridCoord(p[k].z, fl.cell, fl.G);
+      const int gx = gridCoord(p[k].x, fl), gy = gridCoord(p[k].y, fl),
+                gz = gridCoord(p[k].z, fl);
       key[k] = fl.cellBase + ((uint32_t)gz * fl.G + (uint32_t)gy) * fl.G + (uint32_t)gx;
       stay[k] = key[k] == prevKey[k];
       mover[k] = !stay[k];

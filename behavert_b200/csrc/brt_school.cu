@@ -161,8 +161,8 @@ __global__ void __launch_bounds__(128) schoolKernel(FusedArgs A) {
   const float4 p4 = __ldg(&A.posS[i]);
   const f3 p = xyz(p4);
   const uint32_t G = fl.G;
-  const uint32_t key = fl.cellBase + ((uint32_t)gridCoord(p.z, fl.cell, G) * G + (uint32_t)gridCoord(p.y, fl.cell, G)) * G +
-                       (uint32_t)gridCoord(p.x, fl.cell, G);
+  const uint32_t key = fl.cellBase + ((uint32_t)gridCoord(p.z, fl) * G + (uint32_t)gridCoord(p.y, fl)) * G +
+                       (uint32_t)gridCoord(p.x, fl);
   const uint32_t ls = blockDim.x + 1;  // odd: one vote's rows fall in distinct banks
   const uint32_t n = scanNeighborsCooperative<kCoopCachedRounds, kCoopWindowAgents>(
       active, i, p, key, A.flocks, f, A.cellStart, A.cellEnd, A.posS, sList, ls, threadIdx.x & ~31u);

@@ -431,6 +431,21 @@ def test_edge_cases_dense_boundary_frozen():
         check_step(eng, w.params, fp64=False)
 
 
+@pytest.mark.parametrize("cell,G", [(2.0, 8), (8.0, 4), (3.0, 5), (2.5, 6)])
+def test_cell_sizes(cell, G):
+    """Cell sizes other than 4: a power-of-two cell takes its position to
+    cell units by the exact reciprocal, any other by the IEEE quotient; both
+    hash, list and step as the oracle's division does."""
+    w = workloads.plain(n=1500, L=cell * G, M=16, seed=9)
+    p = w.params[0]
+    p.cellSize = cell
+    p.commonSearchRadius = min(4.0, cell)
+    w.pos[:20, 0] = np.float32(cell) * np.arange(20, dtype=np.float32) % np.float32(cell * G)  # on cell faces
+    with make_engine(w) as eng:
+        for _ in range(2):
+            check_step(eng, w.params, fp64=False)
+
+
 def _non_finite_workload(seed):
     """Positions a neighbour-cell cull must not trust: NaN agents (every axis,
     and one axis only) hashed into cell 0 beside finite agents there, infinite
