@@ -190,8 +190,10 @@ int brt_engine_set_params(brt_engine* e, uint32_t flock, const brt_params* p);
      "block_size"       32..256, multiple of 32: threads per block of the
                               single-pass flock kernel (default 64)
      "scan_variant"     0..7  neighbour-scan loop: 0 four candidates in flight
-                              with exact cell culling, 1 two in flight with
-                              culling, 2 four without culling, 3 one at a time,
+                              with exact cell culling (skipped for a step whose
+                              state holds a NaN position or one outside the
+                              world), 1 two in flight with the same culling,
+                              2 four without culling, 3 one at a time,
                               4 warp-cooperative (a warp tests 32 candidates of
                               a home cell's neighbourhood per step, the first
                               96 held in registers), 5 as 4, with further
