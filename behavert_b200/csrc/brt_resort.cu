@@ -42,6 +42,8 @@ constexpr uint32_t kStayBit = 0x80000000u;
 // GPU, few enough that the look-back stays short when every tile reaches it
 // at once.  Small grids take 256-thread tiles of 1 to 4 cells a thread, large
 // ones 1024-thread tiles of 8 (measured faster than 256 threads of 32).
+// On the 1M-agent flock (262,144 cells) a target of 2 * 148 tiles measured
+// the same step time and 1 * 148 (8192-cell tiles) 0.7% slower.
 constexpr uint32_t kCellScanTilesTarget = 4 * 148;
 constexpr uint32_t kLookAgg = 1u << 30;
 constexpr uint32_t kLookInc = 2u << 30;
