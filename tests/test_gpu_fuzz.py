@@ -2,7 +2,8 @@
 on the GPU and checked against the FP32 oracle fed the same state (sorted
 hashes, agent order, cell ranges, neighbour lists and the FP32 state, all
 bit-exact).  The draws mix what the hand-written cases cover one at a time:
-1 to 3 flocks of 1 to 3,000 agents in cubes of 3 to 11 cells a side,
+1 to 3 flocks of 1 to 3,000 agents in cubes of 3 to 11 cells a side (and
+batches of 4 to 48 flocks, and flocks with their own cell sizes),
 maxNeighbors from 1 to 40, kNN and first-M flocks side by side, a per-cell
 cap, the 2D projection, features with and without relaxation, sphere
 obstacles, a sensing minimum radius and angle cuts, dense clumps, coincident
@@ -23,19 +24,23 @@ pytestmark = pytest.mark.gpu
 DT = float(np.float32(0.1))
 
 
-def _random_workload(seed: int, flocks=None, max_agents: int = 3000) -> Workload:
+def _random_workload(seed: int, flocks=None, max_agents: int = 3000, cells: bool = False) -> Workload:
     """`flocks`: (low, high) bounds of the flock count, drawn uniformly;
-    1 to 3 (1 twice as likely) otherwise."""
+    1 to 3 (1 twice as likely) otherwise.  `cells`: each flock draws its cell
+    size (powers of two and others) and 3 to 11 cells a side; cell 4
+    otherwise."""
     rng = np.random.default_rng(5000 + seed)
     nflocks = int(rng.choice([1, 1, 2, 3])) if flocks is None else int(rng.integers(flocks[0], flocks[1] + 1))
     F = int(rng.choice([0, 0, 4, 8]))
     relax = float(rng.choice([0.0, 0.05]))
     params, pos, fwd, feat = [], [], [], []
     for _ in range(nflocks):
-        L = 4.0 * int(rng.integers(3, 12))
+        cell = float(rng.choice([2.0, 2.5, 3.0, 4.0, 5.0, 8.0])) if cells else 4.0
+        L = cell * int(rng.integers(3, 12))
         n = int(rng.integers(1, max_agents))
         M = int(rng.choice([1, 4, 16, 32, 40]))
         p = _flock_params(n, L, M, weights=tuple(float(w) for w in rng.uniform(0.2, 2.0, 3)), F=F, relax=relax)
+        p.cellSize = cell
         p.useKnn = int(rng.random() < 0.3)
         if rng.random() < 0.25:
             p.maxBodiesPerCell = int(rng.integers(1, 6))
@@ -77,6 +82,18 @@ def _random_workload(seed: int, flocks=None, max_agents: int = 3000) -> Workload
 @pytest.mark.parametrize("seed", range(80))
 def test_random_configuration_two_steps(seed):
     w = _random_workload(seed)
+    with make_engine(w) as eng:
+        for _ in range(2):
+            check_step(eng, w.params, dt=DT, fp64=False)
+
+
+@pytest.mark.parametrize("seed", range(24))
+def test_random_cell_sizes_two_steps(seed):
+    """1 to 6 flocks, each with its own cell size: a power-of-two cell takes
+    positions to cell units by its exact reciprocal, any other by the IEEE
+    quotient, in one engine; a search radius of 4 may exceed the cell (both
+    sides then scan the same 27 cells)."""
+    w = _random_workload(900 + seed, flocks=(1, 6), max_agents=1500, cells=True)
     with make_engine(w) as eng:
         for _ in range(2):
             check_step(eng, w.params, dt=DT, fp64=False)
