@@ -109,17 +109,19 @@ def test_random_batch_of_many_flocks_two_steps(seed):
             check_step(eng, w.params, dt=DT, fp64=False)
 
 
-def _random_school(seed: int) -> Workload:
+def _random_school(seed: int, cells: bool = False) -> Workload:
     """1 to 3 schools of one mode (an engine's flocks share the steering
     family), random zone radii, turning and blind-angle limits, weights,
-    speed and random deviation."""
+    speed and random deviation; with `cells`, each school its own cell size."""
     rng = np.random.default_rng(7000 + seed)
     mode = int(rng.choice([1, 2]))
     params, pos, fwd = [], [], []
     for _ in range(int(rng.choice([1, 1, 2, 3]))):
-        L = 4.0 * int(rng.integers(3, 10))
+        cell = float(rng.choice([2.0, 2.5, 3.0, 4.0, 5.0, 8.0])) if cells else 4.0
+        L = cell * int(rng.integers(3, 10))
         n = int(rng.integers(2, 2500))
         p = _flock_params(n, L, int(rng.choice([4, 16, 32])))
+        p.cellSize = cell
         sp = p.schooling
         sp.mode = mode
         sp.r_r = float(rng.uniform(0.3, 2.0))
@@ -145,7 +147,15 @@ def _random_school(seed: int) -> Workload:
 
 @pytest.mark.parametrize("seed", range(30))
 def test_random_school_two_steps(seed):
-    w = _random_school(seed)
+    _check_school(_random_school(seed))
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_random_school_cell_sizes_two_steps(seed):
+    _check_school(_random_school(100 + seed, cells=True))
+
+
+def _check_school(w):
     with make_engine(w) as eng:
         p, f, a = w.pos, w.fwd, w.acc
         for step in range(2):
@@ -166,7 +176,15 @@ def test_random_school_two_steps(seed):
 def test_random_crowd_order_one_step(seed):
     """The crowd order, stage by stage (steerAndSlowToAvoidNeighbors, and in
     half the draws the move-away-from-base stage), on random flocks."""
-    w = _random_workload(100 + seed)
+    _check_crowd(_random_workload(100 + seed), seed)
+
+
+@pytest.mark.parametrize("seed", range(10))
+def test_random_crowd_order_cell_sizes_one_step(seed):
+    _check_crowd(_random_workload(1100 + seed, cells=True), 500 + seed)
+
+
+def _check_crowd(w, seed):
     for p in w.params:
         p.useKnn = 0
         p.featuresCount = 0
