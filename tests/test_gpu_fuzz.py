@@ -207,17 +207,23 @@ def _check_crowd(w, seed):
     assert _same_bits(gpos, o["pos"]) and _same_bits(gfwd, o["fwd"]) and _same_bits(gacc, o["acc"])
 
 
-def _random_adjoint(seed: int):
+def _random_adjoint(seed: int, cells: bool = False):
     """1 to 3 flocks of 200 to 3,000 agents, random weights, sometimes
     obstacles, a sensing minimum radius and angle cuts, low speeds (the
     deviation-limited branch), horizons of 4 to 12 steps with a random
-    checkpoint interval, and targets near the start."""
+    checkpoint interval, and targets near the start; with `cells`, each
+    flock its own cell size."""
     rng = np.random.default_rng(11000 + seed)
     params, pos, fwd = [], [], []
     for _ in range(int(rng.choice([1, 1, 2, 3]))):
         n = int(rng.integers(200, 3000))
-        L = 4.0 * int(rng.integers(4, 10))
+        cell = float(rng.choice([2.0, 2.5, 3.0, 4.0, 5.0, 8.0])) if cells else 4.0
+        # the cube side of the cell-4 draws, in whole cells of the drawn
+        # size, so that the density (and the conditioning of the summed
+        # weight gradient) stays in the same range for every cell size
+        L = cell * max(3, round(4.0 * int(rng.integers(4, 10)) / cell))
         p = _flock_params(n, L, int(rng.choice([4, 16, 32])), weights=tuple(float(w) for w in rng.uniform(0.3, 2.0, 3)))
+        p.cellSize = cell
         if rng.random() < 0.3:
             p.commonSensingMinRadius = float(rng.uniform(0.0, 1.0))
             for arr in (p.separationParams, p.alignmentParams, p.cohesionParams):
@@ -250,8 +256,16 @@ def test_random_adjoint_against_fp64_reverse_at_the_gpu_trajectory(seed):
     """The GPU gradients (weights per flock, positions, velocities) against
     the FP64 frozen-neighbour reverse linearised at the GPU's own FP32
     trajectory (the adjoint's arithmetic alone), within 1e-4."""
+    _check_adjoint(*_random_adjoint(seed))
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_random_adjoint_cell_sizes(seed):
+    _check_adjoint(*_random_adjoint(100 + seed, cells=True))
+
+
+def _check_adjoint(w, target, T, k):
     from tests.test_gpu_adjoint import _counts_per_agent, _L_per_agent, _min_image, _vel_grad
-    w, target, T, k = _random_adjoint(seed)
     with make_engine(w) as eng:
         eng.set_option("adjoint_export", 1)
         eng.set_state(w.pos, w.fwd, w.acc)
